@@ -1,0 +1,349 @@
+"""Benchmark: n = 2^20 H-matvec GB/s on one B200 (the large 1-D H-matvec
+workload: uniform grid on [0,10], Cauchy kernel 1/(1+(x-y)^2), MaxBlock 512,
+MinBlock 64, MaxRank 16, ACA tolerance 1e-8, N(0,1) right-hand side).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One step = one single-RHS H-matvec y = H x through the library.  `value` is
+the algorithmic bytes of a matvec (every stored factor and dense entry once,
+plus x and y) divided by the device time of a step, inputs resident in HBM;
+the factor pool (~100 GB in FP64) is far larger than L2, so no flush is
+needed between steps.  `e2e` is the same metric through hm_matvec with host
+(pinned) buffers, the 8 MB host->device copy of x and device->host copy of y
+inside the timed region.
+
+Multi-GPU: every rank builds and multiplies its own replica (independent
+H-matrices, no exchange), weak scaling; the job time is the max over ranks.
+
+--impl reference times the reference algorithm's CPU path (the C restatement
+of hmat_matvec! in oracle/, FP64, all host threads) on a bounded sample of
+the same workload: the leaves touching a band of rows, built by the same
+restatement of aca2.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "hmatrix.jl_b200"))
+
+METRIC = "n=2^20 H-matvec GB/s"
+UNIT = "GB/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--storage", default="f64", choices=["f64", "f32", "bf16"])
+    ap.add_argument("--extra-precisions", action="store_true",
+                    help="also measure FP32 and BF16 factor storage")
+    ap.add_argument("--cpu-rows", type=int, default=4096, help="rows of the CPU baseline sample")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n):
+    return {"workload": "large 1-D H-matvec, n=%d uniform grid on [0,10]" % n, "n": n,
+            "kernel": "1/(1+(x-y)^2)", "MaxBlock": 512, "MinBlock": 64, "MaxRank": 16,
+            "aca_tol": 1e-8, "cons": "aca2 (Adj=I)", "tree": "median bisection",
+            "rhs": "1 column N(0,1), seed 1",
+            "l2": "no flush: inputs (factor pool) far larger than the 126 MB L2"}
+
+
+# --------------------------------------------------------------------------
+# clocks sampled during the timed region
+# --------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_byte():
+    """DRAM bytes per algorithmic byte of each matvec phase from the committed
+    ncu summary (profiles/matvec_traffic.json), if present."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "matvec_traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+# --------------------------------------------------------------------------
+# CPU baseline: the C restatement of aca2 + hmat_matvec! on a band of rows
+# --------------------------------------------------------------------------
+def cpu_sample_gbs(n, rows, target_s=12.0, max_reps=200):
+    from hmatrix.cluster import construct_cluster
+    from oracle.hm_oracle_c import Sample
+    c = construct_cluster(np.linspace(0, 10, n), 64, "bisect")
+    tree = {"s": c.s, "e": c.e, "left": c.left, "right": c.right}
+    r0 = n // 2 - rows // 2
+    S = Sample(1, 1.0, c.X, tree, 64, 512, 16, 1e-8, r0, r0 + rows)
+    x = np.random.default_rng(1).standard_normal(n)
+    S.matvec(x)
+    t0 = time.perf_counter()
+    reps = 0
+    while reps < max_reps:
+        S.matvec(x)
+        reps += 1
+        if time.perf_counter() - t0 > target_s:
+            break
+    dt = (time.perf_counter() - t0) / reps
+    gbs = S.bytes_per_matvec() / dt / 1e9
+    return gbs, S.threads, ("leaves of the %d rows [%d,%d) of the n=%d matrix (%d leaves, %.2f GB FP64), "
+                            "%d matvecs" % (rows, r0, r0 + rows, n, len(S.lv), 8 * S.stored / 1e9, reps)), dt
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    gbs, thr, sample, dt = cpu_sample_gbs(a.n, a.cpu_rows, target_s=max(2.0, 0.5 * a.steps))
+    # each step: one matvec of the sample (bounded), reported as GB/s
+    line = {"metric": METRIC, "value": gbs, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload(a.n),
+            "impl": "reference",
+            "cpu_baseline": {"value": gbs, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample},
+            "e2e": {"value": gbs, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------
+def build(n, storage):
+    import hmatrix as hm
+    prm = hm.Params(Geom=np.linspace(0, 10, n), Kernel=hm.Cauchy(1.0), MaxBlock=512, MinBlock=64,
+                    MaxRank=16, ConsMethod="aca2", εComp=1e-8, Tree="bisect",
+                    Storage={"f64": hm.F64, "f32": hm.F32, "bf16": hm.BF16}[storage],
+                    Device=int(os.environ.get("LOCAL_RANK", "0")))
+    t0 = time.perf_counter()
+    c, H = hm.NewHmat(prm)
+    return c, H, time.perf_counter() - t0
+
+
+def measure(H, a, torch, dist, world):
+    import ctypes as C
+    from hmatrix import _lib
+    L = _lib.lib()
+    n = H.n
+    dev = torch.cuda.current_device()
+    g = torch.Generator(device="cuda").manual_seed(1)
+    x = torch.randn(n, generator=g, device="cuda", dtype=torch.float64)
+    y = torch.empty_like(x)
+    st = torch.cuda.current_stream()
+    sp = C.c_void_p(st.cuda_stream or 1)   # torch's default stream is cudaStreamLegacy
+    flags = _lib.HM_FLAG_DEVICE_PTRS
+
+    def step():
+        _lib.check(L.hm_matvec(H._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), 1, 0, flags, sp))
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    # per-phase device times (events between the launches)
+    ms3 = (C.c_float * 3)()
+    ph = np.zeros(3)
+    for _ in range(3):
+        _lib.check(L.hm_matvec_profile(H._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), 0, sp, ms3))
+        ph += np.array(ms3[:])
+    ph /= 3
+    clocks = Clocks(dev)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(a.steps):
+        step()
+    e1.record(st)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1) / a.steps
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    # end to end through the C ABI with host pinned buffers
+    xh = x.cpu().pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    for _ in range(2):
+        _lib.check(L.hm_matvec(H._h, C.c_void_p(xh.data_ptr()), C.c_void_p(yh.data_ptr()), 1, 0, 0, None))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ke = max(3, a.steps // 2)
+    for _ in range(ke):
+        _lib.check(L.hm_matvec(H._h, C.c_void_p(xh.data_ptr()), C.c_void_p(yh.data_ptr()), 1, 0, 0, None))
+    e2e_ms = (time.perf_counter() - t0) / ke * 1e3
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    # accuracy: 4096 sampled rows against exact FP64 kernel rows (dense oracle)
+    rows = np.sort(np.random.default_rng(2).choice(n, 4096, replace=False))
+    ex = H.exact_rows(rows, x.cpu().numpy())
+    got = y.cpu().numpy()[rows]
+    rel = float(np.linalg.norm(got - ex) / np.linalg.norm(ex))
+    return ms, ph, ck, e2e_ms, rel
+
+
+def run_ours(a):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    import hmatrix as hm
+    c, H, t_build = build(a.n, a.storage)
+    info = H.info()
+    ms, ph, ck, e2e_ms, rel = measure(H, a, torch, dist, world)
+    eb = {"f64": 8, "f32": 4, "bf16": 2}[a.storage]
+    deb = 8 if a.storage == "f64" else 4
+    bytes_mv = eb * info.rk_entries + deb * info.dense_entries + 16 * a.n
+    value = world * bytes_mv / (ms * 1e-3) / 1e9
+    e2e = world * bytes_mv / (e2e_ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    # dominant kernel: the phase with the larger device time; its algorithmic
+    # bytes: phase 1 streams the B factors (+x segments from L2), phase 2 the
+    # A factors, the dense leaves, and writes y.
+    half_rk = eb * info.rk_entries / 2.0
+    p_bytes = [24.0 * a.n, half_rk, half_rk + deb * info.dense_entries + 8 * a.n]
+    dom = int(np.argmax(ph))
+    dom_name = ["xcopy", "mv_phase1_kernel", "mv_phase2_kernel"][dom]
+    achieved = p_bytes[dom] / (ph[dom] * 1e-3) / 1e9
+    tr = traffic_per_byte()
+    traffic = None
+    if tr and dom_name in tr:
+        traffic = tr[dom_name] * p_bytes[dom]
+    extra = {}
+    if a.extra_precisions and world == 1:
+        for s in ("f32", "bf16"):
+            if s == a.storage:
+                continue
+            del H
+            torch.cuda.empty_cache()
+            _, H2, tb2 = build(a.n, s)
+            i2 = H2.info()
+            ms2, ph2, _, _, rel2 = measure(H2, a, torch, None, 1)
+            eb2 = {"f32": 4, "bf16": 2}[s]
+            b2 = eb2 * i2.rk_entries + 4 * i2.dense_entries + 16 * a.n
+            extra[s] = {"GB/s": b2 / (ms2 * 1e-3) / 1e9, "ms_per_step": ms2, "rel_err_4096_rows": rel2,
+                        "phase_ms": [float(v) for v in ph2], "build_s": tb2}
+            del H2
+            H = None
+            torch.cuda.empty_cache()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if not a.no_cpu and world == 1:
+        gbs, thr, sample, _ = cpu_sample_gbs(a.n, a.cpu_rows)
+        cpu = {"value": gbs, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": a.storage, "data": "synthetic",
+            "config": dict(workload(a.n), storage=a.storage, parallelism="replicas" if world > 1 else "1 GPU"),
+            "clocks": ck,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * a.n, "d2h_bytes_per_step": 8 * a.n,
+                    "ms_per_step": e2e_ms},
+            "gpu_launches": 3 * a.steps,
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "algorithmic_bytes": p_bytes[dom], "ms": float(ph[dom])},
+            "matvec_frac_of_peak": value / world / peak,
+            "phase_ms": [float(v) for v in ph],
+            "cpu_baseline": cpu,
+            "accuracy": {"rel_err_vs_exact_fp64_rows": rel, "rows": 4096},
+            "structure": {"n_rk": info.n_rk, "n_dense": info.n_dense, "rk_entries": info.rk_entries,
+                          "dense_entries": info.dense_entries, "max_rank": info.max_rank,
+                          "algorithmic_bytes": bytes_mv, "build_s": t_build},
+            "extra_precisions": extra or None}
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

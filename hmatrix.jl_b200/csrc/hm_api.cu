@@ -1,0 +1,333 @@
+// C ABI of libhmatb200 (declared in include/hmatrix_b200.h).
+#include "hm_internal.h"
+
+#include <cstring>
+#include <new>
+
+namespace hm {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+int check_params(const hm_params* p) {
+  if (!p) return fail(HM_ERR_ARG, "params is NULL");
+  if (p->dim < 1 || p->dim > 3) return fail(HM_ERR_ARG, "dim must be 1, 2 or 3");
+  if (p->kernel != HM_KERNEL_CAUCHY && p->kernel != HM_KERNEL_INVQUAD && p->kernel != HM_KERNEL_GAUSS)
+    return fail(HM_ERR_ARG, "unknown kernel id " + std::to_string(p->kernel) +
+                                "; Hparams.Kernel must map to HM_KERNEL_*");
+  if (!(p->kparam > 0.0) && p->kernel != HM_KERNEL_INVQUAD) return fail(HM_ERR_ARG, "kernel parameter must be > 0");
+  if (p->max_rank < 1 || p->max_rank > 64) return fail(HM_ERR_ARG, "MaxRank must be in [1, 64]");
+  if (p->min_block < 1) return fail(HM_ERR_ARG, "MinBlock must be >= 1");
+  if (p->cons_method != HM_CONS_ACA2 && p->cons_method != HM_CONS_SVD)
+    return fail(HM_ERR_ARG, "ConsMethod must be aca2 or svd (bbfmm/separate are not on this path)");
+  if (p->storage != HM_F64 && p->storage != HM_F32 && p->storage != HM_BF16)
+    return fail(HM_ERR_ARG, "storage must be HM_F64, HM_F32 or HM_BF16");
+  if (!(p->eps_trunc >= 0.0) || !(p->eps_comp >= 0.0)) return fail(HM_ERR_ARG, "tolerances must be >= 0");
+  return HM_OK;
+}
+
+struct IoBuf {
+  hm_handle* h;
+  double* ptr = nullptr;
+  int get(size_t bytes) {
+    if (h->io_bytes < bytes) {
+      if (h->d_io) cudaFree(h->d_io);
+      h->d_io = nullptr;
+      h->io_bytes = 0;
+      cudaError_t e = cudaMalloc(&h->d_io, bytes);
+      if (e != cudaSuccess) return fail(HM_ERR_OOM, std::string("staging buffer: ") + cudaGetErrorString(e));
+      h->io_bytes = bytes;
+    }
+    ptr = h->d_io;
+    return HM_OK;
+  }
+};
+
+}  // namespace
+}  // namespace hm
+
+using namespace hm;
+
+extern "C" {
+
+int hm_version(void) { return 100; }
+
+int hm_last_error(char* buf, int64_t len) {
+  if (!buf || len <= 0) return HM_ERR_ARG;
+  std::strncpy(buf, g_last_error.c_str(), (size_t)len - 1);
+  buf[len - 1] = 0;
+  return HM_OK;
+}
+
+int hm_default_params(hm_params* p) {
+  if (!p) return fail(HM_ERR_ARG, "params is NULL");
+  std::memset(p, 0, sizeof(*p));
+  p->dim = 1;
+  p->kernel = HM_KERNEL_CAUCHY;
+  p->kparam = 1.0;
+  p->shift = 0.0;
+  p->eps_comp = 1e-10;
+  p->eps_trunc = 1e-10;
+  p->max_rank = 16;
+  p->max_block = -1;
+  p->min_block = 64;
+  p->cons_method = HM_CONS_ACA2;
+  p->aca_force = 0;
+  p->storage = HM_F64;
+  p->device = 0;
+  p->rank_cap = 0;
+  return HM_OK;
+}
+
+int hm_new(const hm_params* p, int64_t n, const double* geom, int64_t ncluster, const int64_t* cl_s,
+           const int64_t* cl_e, const int64_t* cl_left, const int64_t* cl_right, int64_t n_nb,
+           const int64_t* nb_pairs, hm_handle** out) {
+  if (!out) return fail(HM_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  HM_TRY(check_params(p));
+  if (n < 1 || !geom || ncluster < 1 || !cl_s || !cl_e || !cl_left || !cl_right)
+    return fail(HM_ERR_ARG, "invalid geometry or cluster arrays");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(HM_ERR_CUDA, "no CUDA device: the H-matrix path has no CPU fallback");
+  if (p->device < 0 || p->device >= ndev) return fail(HM_ERR_ARG, "invalid device ordinal");
+  DeviceGuard g(p->device);
+  hm_handle* h = new (std::nothrow) hm_handle();
+  if (!h) return fail(HM_ERR_OOM, "host allocation");
+  h->prm = *p;
+  if (h->prm.max_block == -1) h->prm.max_block = (int32_t)(n / 4);   // src/cluster.jl:37-39
+  h->n = n;
+  h->dim = p->dim;
+  h->device = p->device;
+  h->storage = p->storage;
+  h->kd = KernelDesc{p->kernel, p->dim, p->kparam, p->shift};
+  cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete h; return fail(HM_ERR_CUDA, cudaGetErrorString(e)); }
+  int s = build_handle(h, geom, ncluster, cl_s, cl_e, cl_left, cl_right, n_nb, nb_pairs);
+  if (s != HM_OK) {
+    std::string msg = g_last_error;
+    free_handle_data(h);
+    cudaStreamDestroy(h->stream);
+    delete h;
+    return fail(s, msg);
+  }
+  *out = h;
+  return HM_OK;
+}
+
+int hm_destroy(hm_handle* h) {
+  if (!h) return HM_OK;
+  DeviceGuard g(h->device);
+  cudaStreamSynchronize(h->stream);
+  free_handle_data(h);
+  cudaStreamDestroy(h->stream);
+  delete h;
+  return HM_OK;
+}
+
+int hm_info(const hm_handle* h, hm_info_t* o) {
+  if (!h || !o) return fail(HM_ERR_ARG, "NULL argument");
+  std::memset(o, 0, sizeof(*o));
+  o->n = h->n;
+  o->depth = h->depth;
+  double stored = 0.0;
+  for (auto& L : h->leaves) {
+    if (L.type == T_DENSE) {
+      o->n_dense++;
+      o->dense_entries += (int64_t)L.m * L.n;
+      stored += (double)L.m * L.n;
+    } else {
+      o->n_rk++;
+      o->rk_entries += (int64_t)L.k * (L.m + L.n);
+      o->max_rank = std::max<int64_t>(o->max_rank, L.k);
+      stored += (double)L.k * (L.m + L.n);
+    }
+  }
+  o->compress_ratio = stored / (double)h->n / (double)h->n;
+  o->pool_bytes = (int64_t)(h->rk_bytes + h->dense_bytes);
+  const int eb = elem_bytes(h->storage), deb = dense_elem_bytes(h->storage);
+  o->matvec_bytes = (int64_t)eb * o->rk_entries + (int64_t)deb * o->dense_entries + 16 * h->n;
+  o->n_row_groups = h->fwd.nwin;
+  o->factorized = h->factorized ? 1 : 0;
+  return HM_OK;
+}
+
+int hm_leaves(const hm_handle* h, int64_t cap, int64_t* out, int64_t* count) {
+  if (!h || !count) return fail(HM_ERR_ARG, "NULL argument");
+  *count = (int64_t)h->leaves.size();
+  if (!out) return HM_OK;
+  if (cap < *count) return fail(HM_ERR_ARG, "leaf buffer too small");
+  for (size_t i = 0; i < h->leaves.size(); ++i) {
+    const Leaf& L = h->leaves[i];
+    int64_t* o = out + 6 * i;
+    o[0] = L.type == T_DENSE ? 0 : 1;
+    o[1] = L.row0; o[2] = L.col0; o[3] = L.m; o[4] = L.n; o[5] = L.k;
+  }
+  return HM_OK;
+}
+
+int hm_leaf_factors(const hm_handle* h, int64_t leaf, double* A, double* B) {
+  if (!h || !A || !B) return fail(HM_ERR_ARG, "NULL argument");
+  if (leaf < 0 || leaf >= (int64_t)h->leaves.size()) return fail(HM_ERR_ARG, "leaf index out of range");
+  if (h->factorized) return fail(HM_ERR_STATE, "factors of a factorised handle are held by the LU state");
+  DeviceGuard g(h->device);
+  return leaf_factors_f64(h, leaf, A, B);
+}
+
+int hm_to_dense(const hm_handle* h, double* out, uint32_t flags) {
+  if (!h || !out) return fail(HM_ERR_ARG, "NULL argument");
+  DeviceGuard g(h->device);
+  const size_t bytes = sizeof(double) * (size_t)h->n * (size_t)h->n;
+  double* d = out;
+  if (!(flags & HM_FLAG_DEVICE_PTRS)) {
+    cudaError_t e = cudaMalloc(&d, bytes);
+    if (e != cudaSuccess) return fail(HM_ERR_OOM, "to_dense buffer");
+  }
+  int s = h->factorized ? lu_to_dense(h, d) : to_dense(h, d);
+  if (s == HM_OK && !(flags & HM_FLAG_DEVICE_PTRS)) {
+    cudaError_t e = cudaMemcpy(out, d, bytes, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) s = fail(HM_ERR_CUDA, cudaGetErrorString(e));
+  }
+  if (!(flags & HM_FLAG_DEVICE_PTRS)) cudaFree(d);
+  return s;
+}
+
+int hm_matvec(hm_handle* h, const double* X, double* Y, int64_t ncols, int32_t trans, uint32_t flags, void* stream) {
+  if (!h || !X || !Y || ncols < 0) return fail(HM_ERR_ARG, "invalid argument");
+  if (h->factorized) return fail(HM_ERR_STATE, "H is factorised; the matvec reads the unfactorised H");
+  DeviceGuard g(h->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  const int64_t n = h->n;
+  if (flags & HM_FLAG_DEVICE_PTRS) {
+    for (int64_t c = 0; c < ncols; ++c) HM_TRY(matvec_device(h, X + c * n, Y + c * n, trans ? 1 : 0, st));
+    return HM_OK;
+  }
+  IoBuf io{h};
+  HM_TRY(io.get(sizeof(double) * 2 * n));
+  for (int64_t c = 0; c < ncols; ++c) {
+    HM_CUDA_TRY(cudaMemcpyAsync(io.ptr, X + c * n, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    HM_TRY(matvec_device(h, io.ptr, io.ptr + n, trans ? 1 : 0, st));
+    HM_CUDA_TRY(cudaMemcpyAsync(Y + c * n, io.ptr + n, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  }
+  HM_CUDA_TRY(cudaStreamSynchronize(st));
+  return HM_OK;
+}
+
+int hm_matvec_profile(hm_handle* h, const double* X, double* Y, int32_t trans, void* stream, float* ms) {
+  if (!h || !X || !Y || !ms) return fail(HM_ERR_ARG, "invalid argument");
+  if (h->factorized) return fail(HM_ERR_STATE, "H is factorised");
+  DeviceGuard g(h->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  cudaEvent_t ev[4];
+  for (int i = 0; i < 4; ++i) HM_CUDA_TRY(cudaEventCreate(&ev[i]));
+  int s = matvec_device(h, X, Y, trans ? 1 : 0, st, ev);
+  if (s == HM_OK) {
+    HM_CUDA_TRY(cudaEventSynchronize(ev[3]));
+    for (int i = 0; i < 3; ++i) HM_CUDA_TRY(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+  }
+  for (int i = 0; i < 4; ++i) cudaEventDestroy(ev[i]);
+  return s;
+}
+
+int hm_exact_rows(hm_handle* h, const int64_t* rows, int64_t nrows, const double* x, double* y, uint32_t flags,
+                  void* stream) {
+  if (!h || !rows || !x || !y || nrows < 0) return fail(HM_ERR_ARG, "invalid argument");
+  DeviceGuard g(h->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  if (flags & HM_FLAG_DEVICE_PTRS) return exact_rows_device(h, rows, nrows, x, y, st);
+  for (int64_t i = 0; i < nrows; ++i)
+    if (rows[i] < 0 || rows[i] >= h->n) return fail(HM_ERR_ARG, "row index out of range");
+  int64_t* dr = nullptr;
+  double *dx = nullptr, *dy = nullptr;
+  HM_CUDA_TRY(cudaMalloc(&dr, 8 * std::max<int64_t>(nrows, 1)));
+  HM_CUDA_TRY(cudaMalloc(&dx, 8 * h->n));
+  HM_CUDA_TRY(cudaMalloc(&dy, 8 * std::max<int64_t>(nrows, 1)));
+  HM_CUDA_TRY(cudaMemcpyAsync(dr, rows, 8 * nrows, cudaMemcpyHostToDevice, st));
+  HM_CUDA_TRY(cudaMemcpyAsync(dx, x, 8 * h->n, cudaMemcpyHostToDevice, st));
+  int s = exact_rows_device(h, dr, nrows, dx, dy, st);
+  if (s == HM_OK) HM_CUDA_TRY(cudaMemcpyAsync(y, dy, 8 * nrows, cudaMemcpyDeviceToHost, st));
+  HM_CUDA_TRY(cudaStreamSynchronize(st));
+  cudaFree(dr); cudaFree(dx); cudaFree(dy);
+  return s;
+}
+
+int hm_add_identity(hm_handle* h, double lambda) {
+  if (!h) return fail(HM_ERR_ARG, "NULL handle");
+  if (h->factorized) return fail(HM_ERR_STATE, "Hmatrix is frozen after factorization");
+  DeviceGuard g(h->device);
+  return apply_shift(h, lambda);
+}
+
+int hm_scale(hm_handle* h, double u) {
+  if (!h) return fail(HM_ERR_ARG, "NULL handle");
+  if (h->factorized) return fail(HM_ERR_STATE, "Hmatrix is frozen after factorization");
+  DeviceGuard g(h->device);
+  return apply_scale(h, u);
+}
+
+int hm_copy(const hm_handle* h, hm_handle** out) {
+  if (!h || !out) return fail(HM_ERR_ARG, "NULL argument");
+  DeviceGuard g(h->device);
+  return copy_handle(h, out);
+}
+
+int hm_lu(hm_handle* h) {
+  if (!h) return fail(HM_ERR_ARG, "NULL handle");
+  if (h->factorized) return fail(HM_ERR_STATE, "H-matrix H is already factorized; reuse factorization");
+  DeviceGuard g(h->device);
+  return lu_factor(h);
+}
+
+int hm_lu_perm(const hm_handle* h, int64_t* P) {
+  if (!h || !P) return fail(HM_ERR_ARG, "NULL argument");
+  if (!h->factorized) return fail(HM_ERR_STATE, "a has not been factorized");
+  return lu_perm(h, P);
+}
+
+int hm_solve(hm_handle* h, const double* B, double* X, int64_t ncols, uint32_t flags, void* stream) {
+  if (!h || !B || !X || ncols < 0) return fail(HM_ERR_ARG, "invalid argument");
+  if (!h->factorized) return fail(HM_ERR_STATE, "a has not been factorized");
+  DeviceGuard g(h->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  const int64_t n = h->n;
+  if (flags & HM_FLAG_DEVICE_PTRS) return lu_solve_device(h, B, X, ncols, st);
+  IoBuf io{h};
+  HM_TRY(io.get(sizeof(double) * 2 * n * std::max<int64_t>(ncols, 1)));
+  HM_CUDA_TRY(cudaMemcpyAsync(io.ptr, B, sizeof(double) * n * ncols, cudaMemcpyHostToDevice, st));
+  HM_TRY(lu_solve_device(h, io.ptr, io.ptr + n * ncols, ncols, st));
+  HM_CUDA_TRY(cudaMemcpyAsync(X, io.ptr + n * ncols, sizeof(double) * n * ncols, cudaMemcpyDeviceToHost, st));
+  HM_CUDA_TRY(cudaStreamSynchronize(st));
+  return HM_OK;
+}
+
+int aca_wrapper(double* AA, double* UU, double* VV, int m, int n, double epsilon, int rank) {
+  if (!AA || !UU || !VV || m <= 0 || n <= 0 || rank < 0) {
+    fail(HM_ERR_ARG, "aca_wrapper: invalid argument");
+    return -HM_ERR_ARG;
+  }
+  int r = 0;
+  int s = aca_fp_host(AA, UU, VV, m, n, epsilon, rank, &r);
+  return s == HM_OK ? r : -s;
+}
+
+}  // extern "C"

@@ -1,0 +1,709 @@
+// Batched low-rank kernels for sm_100a: aca2, fully pivoted ACA and the
+// QR + one-sided-Jacobi-SVD recompression core.
+#include "hm_lowrank.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace hm {
+
+// ===========================================================================
+// aca2 (src/hlu.jl:59-111), one warp per block.  Deterministic pivots: the
+// first row, then the arg-max of |a_r| over unused rows (the reference draws
+// a random unused row inside its "patience" loop, hlu.jl:72-85).  Up to R
+// terms; stops after the first term with |a_r||b_r|/(|a_1||b_1|) <= eps
+// (kept) or on an exactly zero pivot (dropped).
+// ===========================================================================
+struct AcaJob {
+  int64_t row0, col0;
+  int32_t m, n;
+  int64_t off;      // element offset of the leaf in the low-rank pool
+};
+
+template <typename T>
+__global__ void __launch_bounds__(128) aca2_kernel(
+    KernelDesc kd, const double* __restrict__ geom, int64_t ng, const AcaJob* __restrict__ jobs,
+    int64_t njobs, int R, double eps_comp, double* __restrict__ scratch, int mcap, int ncap,
+    int32_t* __restrict__ ranks, T* __restrict__ pool, int write) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  double* SA = scratch + gwarp * (int64_t)R * (mcap + ncap);   // A: R columns of mcap
+  double* SB = SA + (int64_t)R * mcap;                         // B: R columns of ncap
+
+  for (int64_t job = gwarp; job < njobs; job += nwarps) {
+    const AcaJob J = jobs[job];
+    const int m = J.m, n = J.n;
+    int tau = 0;
+    uint64_t used = 0;          // bit q of lane l: row l + 32q is used
+    double na0 = 1.0, nb0 = 1.0;
+    int rank = R;
+    for (int r = 0; r < R; ++r) {
+      // residual row tau (src/hlu.jl:73-77)
+      double best = -1.0, bval = 0.0, nB = 0.0;
+      int64_t bidx = INT64_MAX;
+      for (int j = lane; j < n; j += 32) {
+        double v = kernel_eval(kd, geom, ng, J.row0 + tau, J.col0 + j);
+        if (r > 0) {
+          double s = 0.0;
+          for (int q = 0; q < r; ++q) s = fma(SB[(int64_t)q * ncap + j], SA[(int64_t)q * mcap + tau], s);
+          v = v - s;
+        }
+        SB[(int64_t)r * ncap + j] = v;
+        nB = fma(v, v, nB);
+        double a = fabs(v);
+        if (a > best) { best = a; bidx = j; bval = v; }
+      }
+      warp_argmax(best, bidx, bval);
+      nB = warp_sum(nB);
+      const int sigma = (int)bidx;
+      const double delta = bval;
+      if (!(delta != 0.0)) { rank = r; break; }      // delta == 0 (src/hlu.jl:87-89)
+      if ((tau & 31) == lane) used |= 1ull << (tau >> 5);
+      __syncwarp();
+      // residual column sigma, new a_r (src/hlu.jl:93-98)
+      double nA = 0.0, best2 = -1.0, v2 = 0.0;
+      int64_t idx2 = INT64_MAX;
+      for (int i = lane; i < m; i += 32) {
+        double v = kernel_eval(kd, geom, ng, J.row0 + i, J.col0 + sigma);
+        if (r > 0) {
+          double s = 0.0;
+          for (int q = 0; q < r; ++q) s = fma(SA[(int64_t)q * mcap + i], SB[(int64_t)q * ncap + sigma], s);
+          v = v - s;
+        }
+        v = v / delta;
+        SA[(int64_t)r * mcap + i] = v;
+        nA = fma(v, v, nA);
+        if (!((used >> (i >> 5)) & 1ull)) {
+          double a = fabs(v);
+          if (a > best2) { best2 = a; idx2 = i; v2 = v; }
+        }
+      }
+      warp_argmax(best2, idx2, v2);
+      nA = warp_sum(nA);
+      __syncwarp();
+      const double na = sqrt(nA), nb = sqrt(nB);
+      if (r == 0) { na0 = na; nb0 = nb; }
+      if (idx2 == INT64_MAX) { rank = r + 1; break; }   // no unused row left
+      tau = (int)idx2;
+      const double eps = na * nb / na0 / nb0;           // src/hlu.jl:104
+      if (eps <= eps_comp) { rank = r + 1; break; }
+    }
+    if (!write) {
+      if (lane == 0) ranks[job] = rank;
+    } else {
+      const int eb = (int)sizeof(T);
+      const int64_t npad = col_pad_dev(n, eb), mpad = col_pad_dev(m, eb);
+      T* Bout = pool + J.off;
+      T* Aout = Bout + npad * rank;
+      for (int q = 0; q < rank; ++q) {
+        for (int j = lane; j < npad; j += 32) Bout[q * npad + j] = to_store<T>(j < n ? SB[(int64_t)q * ncap + j] : 0.0);
+        for (int i = lane; i < mpad; i += 32) Aout[q * mpad + i] = to_store<T>(i < m ? SA[(int64_t)q * mcap + i] : 0.0);
+      }
+      if (lane == 0 && ranks[job] != rank) ranks[job] = -1 - rank;   // must match the rank pass
+    }
+    __syncwarp();
+  }
+}
+
+static int aca2_launch(hm_handle* h, const std::vector<int64_t>& rk_leaf, int write,
+                       std::vector<int32_t>* ranks_out) {
+  const int64_t nj = (int64_t)rk_leaf.size();
+  if (nj == 0) { if (ranks_out) ranks_out->clear(); return HM_OK; }
+  std::vector<AcaJob> jobs(nj);
+  int mcap = 1, ncap = 1;
+  for (int64_t i = 0; i < nj; ++i) {
+    const Leaf& L = h->leaves[rk_leaf[i]];
+    jobs[i] = AcaJob{L.row0, L.col0, L.m, L.n, L.off};
+    mcap = std::max(mcap, L.m);
+    ncap = std::max(ncap, L.n);
+  }
+  if (mcap > ACA_MAX_EXTENT || ncap > ACA_MAX_EXTENT)
+    return fail(HM_ERR_UNSUPPORTED, "aca2 block larger than " + std::to_string(ACA_MAX_EXTENT));
+  const int R = std::max(1, h->prm.max_rank);   // aca2(..., MaxRank-1): up to MaxRank terms
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+  int64_t per_warp = (int64_t)R * (mcap + ncap) * 8;
+  int64_t nwarps = std::min<int64_t>((int64_t)nsm * 32, std::max<int64_t>(4, (int64_t)(1ll << 30) / per_warp));
+  nwarps = std::min<int64_t>(nwarps, (nj + 3) / 4 * 4);
+  nwarps = std::max<int64_t>(4, nwarps / 4 * 4);
+  double* scratch = nullptr;
+  AcaJob* dj = nullptr;
+  int32_t* dr = nullptr;
+  HM_CUDA_TRY(cudaMalloc(&scratch, per_warp * nwarps));
+  HM_CUDA_TRY(cudaMalloc(&dj, sizeof(AcaJob) * nj));
+  HM_CUDA_TRY(cudaMalloc(&dr, sizeof(int32_t) * nj));
+  HM_CUDA_TRY(cudaMemcpyAsync(dj, jobs.data(), sizeof(AcaJob) * nj, cudaMemcpyHostToDevice, h->stream));
+  if (write) {
+    std::vector<int32_t> kk(nj);
+    for (int64_t i = 0; i < nj; ++i) kk[i] = h->leaves[rk_leaf[i]].k;
+    HM_CUDA_TRY(cudaMemcpyAsync(dr, kk.data(), sizeof(int32_t) * nj, cudaMemcpyHostToDevice, h->stream));
+  }
+  unsigned grid = (unsigned)(nwarps / 4);
+  switch (write ? h->storage : HM_F64) {
+    case HM_F64:
+      aca2_kernel<double><<<grid, 128, 0, h->stream>>>(h->kd, h->d_geom, h->n, dj, nj, R, h->prm.eps_comp,
+                                                      scratch, mcap, ncap, dr, (double*)h->d_rk, write);
+      break;
+    case HM_F32:
+      aca2_kernel<float><<<grid, 128, 0, h->stream>>>(h->kd, h->d_geom, h->n, dj, nj, R, h->prm.eps_comp,
+                                                     scratch, mcap, ncap, dr, (float*)h->d_rk, write);
+      break;
+    default:
+      aca2_kernel<__nv_bfloat16><<<grid, 128, 0, h->stream>>>(h->kd, h->d_geom, h->n, dj, nj, R,
+                                                             h->prm.eps_comp, scratch, mcap, ncap, dr,
+                                                             (__nv_bfloat16*)h->d_rk, write);
+  }
+  HM_CUDA_TRY(cudaGetLastError());
+  std::vector<int32_t> ranks(nj);
+  HM_CUDA_TRY(cudaMemcpyAsync(ranks.data(), dr, sizeof(int32_t) * nj, cudaMemcpyDeviceToHost, h->stream));
+  HM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  cudaFree(scratch);
+  cudaFree(dj);
+  cudaFree(dr);
+  if (write) {
+    for (int64_t i = 0; i < nj; ++i)
+      if (ranks[i] < 0) return fail(HM_ERR_CUDA, "aca2 write pass disagrees with the rank pass");
+  } else {
+    for (int64_t i = 0; i < nj; ++i)
+      if (ranks[i] < 0 || ranks[i] > R) return fail(HM_ERR_CUDA, "aca2 produced an invalid rank");
+  }
+  if (ranks_out) ranks_out->swap(ranks);
+  return HM_OK;
+}
+
+int aca2_ranks(hm_handle* h, const std::vector<int64_t>& rk_leaf, std::vector<int32_t>& ranks) {
+  return aca2_launch(h, rk_leaf, 0, &ranks);
+}
+int aca2_write(hm_handle* h, const std::vector<int64_t>& rk_leaf) {
+  return aca2_launch(h, rk_leaf, 1, nullptr);
+}
+
+// ===========================================================================
+// Fully pivoted ACA (deps/src/ACA_FullyPivoted.cpp:9-151), one CTA per
+// block.  R (m x n, ld m) is the residual, updated in place; U/V receive up
+// to `cap` columns.  Pivot: largest |R| with the smallest column-major index
+// (Eigen's per-column then overall maxCoeff).  Loop condition of line 60:
+// (rank < min(m,n) && |R|_F > eps && |R|_F > machine eps) || rank < min_rank.
+// status: 0 converged, 1 stopped at `cap` terms, 2 non-finite norm.
+// ===========================================================================
+struct AcaFpJob {
+  double* R; double* U; double* V;
+  int32_t m, n, cap, min_rank;
+  double eps;
+  int32_t* rank; int32_t* status;
+};
+
+__global__ void __launch_bounds__(512) aca_fp_kernel(const AcaFpJob* __restrict__ jobs) {
+  const AcaFpJob J = jobs[blockIdx.x];
+  __shared__ double red[32];
+  __shared__ double s_a[32];
+  __shared__ int64_t s_i[32];
+  __shared__ double s_v[32];
+  __shared__ int64_t s_sel;
+  __shared__ double s_max;
+  const int m = J.m, n = J.n;
+  const int64_t mn = (int64_t)m * n;
+  const int maxr = min(m, n);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const double meps = 2.220446049250313e-16;
+  int rank = 0, status = 0;
+  double* ucol = nullptr;
+  double* vcol = nullptr;
+
+  for (;;) {
+    // pass over R: update with the previous term, then arg-max and norm
+    double best = -1.0, bval = 0.0, ss = 0.0;
+    int64_t bidx = INT64_MAX;
+    for (int64_t e = threadIdx.x; e < mn; e += blockDim.x) {
+      double v = J.R[e];
+      if (ucol) {
+        const int i = (int)(e % m), j = (int)(e / m);
+        v = v - ucol[i] * vcol[j];
+        J.R[e] = v;
+      }
+      ss = fma(v, v, ss);
+      double a = fabs(v);
+      if (a > best) { best = a; bidx = e; bval = v; }
+    }
+    warp_argmax(best, bidx, bval);
+    __syncthreads();
+    if (lane == 0) { s_a[w] = best; s_i[w] = bidx; s_v[w] = bval; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double b = s_a[0]; int64_t bi = s_i[0]; double bv = s_v[0];
+      for (int q = 1; q < nw; ++q)
+        if (s_a[q] > b || (s_a[q] == b && s_i[q] < bi)) { b = s_a[q]; bi = s_i[q]; bv = s_v[q]; }
+      s_sel = bi; s_max = bv;
+    }
+    const double Rnorm = sqrt(block_sum(ss, red));   // contains a __syncthreads
+    const int64_t sel = s_sel;
+    const double Max = s_max;
+    if (isnan(Rnorm)) { status = 2; break; }
+    if (!((rank < maxr && Rnorm > J.eps && Rnorm > meps) || rank < J.min_rank)) break;
+    if (rank >= J.cap) { status = 1; break; }
+    const int sel_row = (int)(sel % m), sel_col = (int)(sel / m);
+    ucol = J.U + (int64_t)rank * m;
+    vcol = J.V + (int64_t)rank * n;
+    if (fabs(Max) > meps && !isnan(Max)) {
+      const double gamma = 1.0 / Max;
+      for (int i = threadIdx.x; i < m; i += blockDim.x) ucol[i] = gamma * J.R[i + (int64_t)sel_col * m];
+      for (int j = threadIdx.x; j < n; j += blockDim.x) vcol[j] = J.R[sel_row + (int64_t)j * m];
+    } else {
+      for (int i = threadIdx.x; i < m; i += blockDim.x) ucol[i] = (i == rank) ? 1.0 : 0.0;
+      for (int j = threadIdx.x; j < n; j += blockDim.x) vcol[j] = 0.0;
+    }
+    __syncthreads();
+    ++rank;
+  }
+  if (threadIdx.x == 0) { *J.rank = rank; *J.status = status; }
+}
+
+// ===========================================================================
+// Recompression core (K3): CGS2 QR of A and B in place, W = R_A R_B^T, one
+// sided Jacobi SVD of W, truncation k = #{s_i/s_1 > eps_trunc}, and
+// A' = Q_A U_k, B' = Q_B V_k S_k.  One CTA per job; smem 3*rmax^2 doubles.
+// ===========================================================================
+__device__ void cgs2_qr(double* X, int len, int ld, int r, double* Rm /* r x r, col-major */,
+                        double* proj /* r */, double* red) {
+  for (int e = threadIdx.x; e < r * r; e += blockDim.x) Rm[e] = 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j = 0; j < r; ++j) {
+    double* xj = X + (int64_t)j * ld;
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int i = w; i < j; i += nw) {
+        const double* qi = X + (int64_t)i * ld;
+        double s = 0.0;
+        for (int t = lane; t < len; t += 32) s = fma(qi[t], xj[t], s);
+        s = warp_sum(s);
+        if (lane == 0) proj[i] = s;
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < len; t += blockDim.x) {
+        double s = 0.0;
+        for (int i = 0; i < j; ++i) s = fma(X[t + (int64_t)i * ld], proj[i], s);
+        xj[t] -= s;
+      }
+      if (threadIdx.x < j) Rm[threadIdx.x + j * r] += proj[threadIdx.x];
+      __syncthreads();
+    }
+    double ss = 0.0;
+    for (int t = threadIdx.x; t < len; t += blockDim.x) ss = fma(xj[t], xj[t], ss);
+    const double nrm = sqrt(block_sum(ss, red));
+    const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+    for (int t = threadIdx.x; t < len; t += blockDim.x) xj[t] *= inv;
+    if (threadIdx.x == 0) Rm[j + j * r] = nrm;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) core_recompress_kernel(const CoreJob* __restrict__ jobs, int rmax,
+                                                              double eps_trunc, int* __restrict__ flags) {
+  extern __shared__ double sm[];
+  __shared__ double red[32];
+  __shared__ double proj[RCORE_MAX];
+  __shared__ double sig[RCORE_MAX];
+  __shared__ int ord[RCORE_MAX];
+  __shared__ int s_rot;
+  __shared__ int s_k;
+  const CoreJob J = jobs[blockIdx.x];
+  const int r = J.r;
+  double* b0 = sm;                       // R_A, later V (Jacobi right vectors)
+  double* b1 = sm + rmax * rmax;         // R_B, later U-coefficients
+  double* b2 = sm + 2 * rmax * rmax;     // W, later V-coefficients
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+
+  if (r == 0) {
+    if (threadIdx.x == 0) *J.rank = 0;
+    return;
+  }
+  cgs2_qr(J.A, J.m, J.lda, r, b0, proj, red);
+  cgs2_qr(J.B, J.n, J.ldb, r, b1, proj, red);
+  // W = R_A R_B^T  (r x r, column-major, ld r)
+  double sabs = 0.0;
+  for (int e = threadIdx.x; e < r * r; e += blockDim.x) {
+    const int i = e % r, j = e / r;
+    double s = 0.0;
+    for (int q = max(i, j); q < r; ++q) s = fma(b0[i + q * r], b1[j + q * r], s);
+    b2[e] = s;
+    sabs += fabs(s);
+  }
+  sabs = block_sum(sabs, red);
+  bool nonfinite = !isfinite(sabs);
+  if (J.zero_test && sabs < 1e-5) {
+    // compress(): an (absolutely) tiny core becomes rank-1 zeros (src/hlu.jl:163-167)
+    for (int i = threadIdx.x; i < J.m; i += blockDim.x) J.outA[i] = 0.0;
+    for (int j = threadIdx.x; j < J.n; j += blockDim.x) J.outB[j] = 0.0;
+    if (threadIdx.x == 0) *J.rank = 1;
+    return;
+  }
+  // V = I
+  for (int e = threadIdx.x; e < r * r; e += blockDim.x) b0[e] = (e % r == e / r) ? 1.0 : 0.0;
+  __syncthreads();
+  // one-sided Jacobi on the columns of W, round-robin pairing
+  const int rr = (r + 1) & ~1;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    if (threadIdx.x == 0) s_rot = 0;
+    __syncthreads();
+    for (int round = 0; round < rr - 1; ++round) {
+      for (int pidx = w; pidx < rr / 2; pidx += nw) {
+        // tournament pairing: position 0 fixed, others rotate
+        auto posv = [&](int q) { return q == 0 ? 0 : 1 + (q - 1 + round) % (rr - 1); };
+        int p = posv(pidx), q = posv(rr - 1 - pidx);
+        if (p > q) { int t = p; p = q; q = t; }
+        if (q >= r) continue;
+        double* wp = b2 + p * r;
+        double* wq = b2 + q * r;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (int t = lane; t < r; t += 32) {
+          al = fma(wp[t], wp[t], al);
+          be = fma(wq[t], wq[t], be);
+          ga = fma(wp[t], wq[t], ga);
+        }
+        al = warp_sum(al); be = warp_sum(be); ga = warp_sum(ga);
+        if (ga != 0.0 && fabs(ga) > 1e-15 * sqrt(al * be)) {
+          const double zeta = (be - al) / (2.0 * ga);
+          const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+          double* vp = b0 + p * r;
+          double* vq = b0 + q * r;
+          for (int t2 = lane; t2 < r; t2 += 32) {
+            const double x = wp[t2], y = wq[t2];
+            wp[t2] = c * x - s * y;
+            wq[t2] = s * x + c * y;
+            const double u = vp[t2], v = vq[t2];
+            vp[t2] = c * u - s * v;
+            vq[t2] = s * u + c * v;
+          }
+          if (lane == 0) atomicAdd(&s_rot, 1);
+        }
+      }
+      __syncthreads();
+    }
+    if (s_rot == 0) break;
+    __syncthreads();
+  }
+  // singular values = column norms of W; sort descending
+  for (int j = w; j < r; j += nw) {
+    double s = 0.0;
+    for (int t = lane; t < r; t += 32) s = fma(b2[t + j * r], b2[t + j * r], s);
+    s = warp_sum(s);
+    if (lane == 0) sig[j] = sqrt(s);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int j = 0; j < r; ++j) ord[j] = j;
+    for (int a = 0; a < r; ++a) {             // stable selection sort, descending
+      int b = a;
+      for (int c = a + 1; c < r; ++c)
+        if (sig[ord[c]] > sig[ord[b]]) b = c;
+      int t = ord[b];
+      for (int c = b; c > a; --c) ord[c] = ord[c - 1];
+      ord[a] = t;
+    }
+    const double s1 = sig[ord[0]];
+    int k = 0;
+    for (int j = 0; j < r; ++j)
+      if (sig[ord[j]] / s1 > eps_trunc) k = j + 1;   // findlast(S/S[1] .> εTrunc)
+    if (!(s1 > 0.0)) k = 0;
+    s_k = k;
+  }
+  __syncthreads();
+  int k = s_k;
+  if (k > J.kcap) {
+    if (threadIdx.x == 0) atomicOr(flags, 1);
+    k = J.kcap;
+  }
+  if (nonfinite && threadIdx.x == 0) atomicOr(flags, 2);
+  // coefficients: CU[j][c] = W[j, ord c] / s ; CV[j][c] = V[j, ord c] * s
+  for (int e = threadIdx.x; e < r * k; e += blockDim.x) {
+    const int j = e % r, c = e / r;
+    const int o = ord[c];
+    const double s = sig[o];
+    b1[e] = s > 0.0 ? b2[j + o * r] / s : 0.0;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < r * k; e += blockDim.x) {
+    const int j = e % r, c = e / r;
+    const int o = ord[c];
+    b2[e] = b0[j + o * r] * sig[o];
+  }
+  __syncthreads();
+  for (int64_t e = threadIdx.x; e < (int64_t)J.m * k; e += blockDim.x) {
+    const int i = (int)(e % J.m), c = (int)(e / J.m);
+    double s = 0.0;
+    for (int j = 0; j < r; ++j) s = fma(J.A[i + (int64_t)j * J.lda], b1[j + c * r], s);
+    J.outA[i + (int64_t)c * J.ldoa] = s;
+  }
+  for (int64_t e = threadIdx.x; e < (int64_t)J.n * k; e += blockDim.x) {
+    const int i = (int)(e % J.n), c = (int)(e / J.n);
+    double s = 0.0;
+    for (int j = 0; j < r; ++j) s = fma(J.B[i + (int64_t)j * J.ldb], b2[j + c * r], s);
+    J.outB[i + (int64_t)c * J.ldob] = s;
+  }
+  if (threadIdx.x == 0) *J.rank = k;
+}
+
+int launch_core_recompress(const CoreJob* d_jobs, int njobs, int rmax, double eps_trunc, int* d_flags,
+                           cudaStream_t st) {
+  if (njobs == 0) return HM_OK;
+  if (rmax > RCORE_MAX) return fail(HM_ERR_UNSUPPORTED, "recompression core above " + std::to_string(RCORE_MAX));
+  rmax = std::max(rmax, 1);
+  size_t smem = (size_t)3 * rmax * rmax * sizeof(double);
+  static bool attr_set = false;
+  if (!attr_set) {
+    HM_CUDA_TRY(cudaFuncSetAttribute(core_recompress_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)((size_t)3 * RCORE_MAX * RCORE_MAX * sizeof(double))));
+    attr_set = true;
+  }
+  core_recompress_kernel<<<njobs, 256, smem, st>>>(d_jobs, rmax, eps_trunc, d_flags);
+  HM_CUDA_TRY(cudaGetLastError());
+  return HM_OK;
+}
+
+// ===========================================================================
+// "svd" route candidates (src/cluster.jl:99-107): dense block, compress,
+// low-rank iff rank <= MaxRank.  compress (src/hlu.jl:159-190) is realised
+// as a fully pivoted ACA down to a residual far below eps_trunc*s_1 followed
+// by the exact QR+SVD of its core, which yields the truncated SVD of the
+// block up to that residual.
+// ===========================================================================
+__global__ void dense_block_kernel(KernelDesc kd, const double* __restrict__ geom, int64_t ng,
+                                   const int64_t* __restrict__ r0, const int64_t* __restrict__ c0,
+                                   const int32_t* __restrict__ mm, const int32_t* __restrict__ nn,
+                                   const int64_t* __restrict__ off, double* __restrict__ out,
+                                   double* __restrict__ fro2, double* __restrict__ sabs) {
+  __shared__ double red[32];
+  const int b = blockIdx.x;
+  const int m = mm[b], n = nn[b];
+  double* C = out + off[b];
+  double s2 = 0.0, s1 = 0.0;
+  for (int64_t e = threadIdx.x; e < (int64_t)m * n; e += blockDim.x) {
+    const int i = (int)(e % m), j = (int)(e / m);
+    double v = kernel_eval(kd, geom, ng, r0[b] + i, c0[b] + j);
+    C[e] = v;
+    s2 = fma(v, v, s2);
+    s1 += fabs(v);
+  }
+  s2 = block_sum(s2, red);
+  s1 = block_sum(s1, red);
+  if (threadIdx.x == 0) { fro2[b] = s2; sabs[b] = s1; }
+}
+
+int svd_compress_candidates(hm_handle* h, const std::vector<int64_t>& r0, const std::vector<int64_t>& c0,
+                            const std::vector<int32_t>& mm, const std::vector<int32_t>& nn,
+                            std::vector<int32_t>& ranks, SvdCandidateStore& store,
+                            const std::vector<int32_t>& nodes) {
+  const int64_t nc = (int64_t)r0.size();
+  ranks.assign(nc, 0);
+  const int cap = RCORE_MAX;
+  const double eps_trunc = h->prm.eps_trunc;
+  // chunk the candidates so that the dense blocks stay below ~2 GB
+  int64_t b0 = 0;
+  while (b0 < nc) {
+    int64_t b1 = b0, elems = 0;
+    while (b1 < nc && (b1 == b0 || elems + (int64_t)mm[b1] * nn[b1] < (1ll << 28))) {
+      elems += (int64_t)mm[b1] * nn[b1] + (int64_t)(mm[b1] + nn[b1]) * cap * 2;
+      ++b1;
+    }
+    const int64_t nb = b1 - b0;
+    std::vector<int64_t> offC(nb), offU(nb), offV(nb), offA(nb), offB(nb);
+    int64_t tot = 0;
+    for (int64_t i = 0; i < nb; ++i) {
+      const int64_t m = mm[b0 + i], n = nn[b0 + i];
+      offC[i] = tot; tot += pad_to(m * n, 32);
+      offU[i] = tot; tot += pad_to(m * cap, 32);
+      offV[i] = tot; tot += pad_to(n * cap, 32);
+      offA[i] = tot; tot += pad_to(m * cap, 32);
+      offB[i] = tot; tot += pad_to(n * cap, 32);
+    }
+    double* buf = nullptr;
+    HM_CUDA_TRY(cudaMalloc(&buf, sizeof(double) * tot));
+    int64_t *d_r0 = nullptr, *d_c0 = nullptr, *d_off = nullptr;
+    int32_t *d_m = nullptr, *d_n = nullptr, *d_rank = nullptr, *d_stat = nullptr;
+    double *d_f2 = nullptr, *d_sa = nullptr;
+    int* d_flags = nullptr;
+    HM_CUDA_TRY(cudaMalloc(&d_r0, 8 * nb)); HM_CUDA_TRY(cudaMalloc(&d_c0, 8 * nb));
+    HM_CUDA_TRY(cudaMalloc(&d_off, 8 * nb)); HM_CUDA_TRY(cudaMalloc(&d_m, 4 * nb));
+    HM_CUDA_TRY(cudaMalloc(&d_n, 4 * nb)); HM_CUDA_TRY(cudaMalloc(&d_rank, 4 * nb * 2));
+    HM_CUDA_TRY(cudaMalloc(&d_stat, 4 * nb)); HM_CUDA_TRY(cudaMalloc(&d_f2, 8 * nb));
+    HM_CUDA_TRY(cudaMalloc(&d_sa, 8 * nb)); HM_CUDA_TRY(cudaMalloc(&d_flags, 4));
+    HM_CUDA_TRY(cudaMemsetAsync(d_flags, 0, 4, h->stream));
+    cudaStream_t st = h->stream;
+    HM_CUDA_TRY(cudaMemcpyAsync(d_r0, r0.data() + b0, 8 * nb, cudaMemcpyHostToDevice, st));
+    HM_CUDA_TRY(cudaMemcpyAsync(d_c0, c0.data() + b0, 8 * nb, cudaMemcpyHostToDevice, st));
+    HM_CUDA_TRY(cudaMemcpyAsync(d_off, offC.data(), 8 * nb, cudaMemcpyHostToDevice, st));
+    HM_CUDA_TRY(cudaMemcpyAsync(d_m, mm.data() + b0, 4 * nb, cudaMemcpyHostToDevice, st));
+    HM_CUDA_TRY(cudaMemcpyAsync(d_n, nn.data() + b0, 4 * nb, cudaMemcpyHostToDevice, st));
+    dense_block_kernel<<<(unsigned)nb, 256, 0, st>>>(h->kd, h->d_geom, h->n, d_r0, d_c0, d_m, d_n, d_off,
+                                                     buf, d_f2, d_sa);
+    HM_CUDA_TRY(cudaGetLastError());
+    std::vector<double> fro2(nb), sabs(nb);
+    HM_CUDA_TRY(cudaMemcpyAsync(fro2.data(), d_f2, 8 * nb, cudaMemcpyDeviceToHost, st));
+    HM_CUDA_TRY(cudaMemcpyAsync(sabs.data(), d_sa, 8 * nb, cudaMemcpyDeviceToHost, st));
+    HM_CUDA_TRY(cudaStreamSynchronize(st));
+    // fully pivoted ACA to tau = 1e-3 * eps_trunc * |C|_F / sqrt(min(m,n)) (<= 1e-3 eps_trunc s_1)
+    std::vector<AcaFpJob> fj(nb);
+    for (int64_t i = 0; i < nb; ++i) {
+      const int m = mm[b0 + i], n = nn[b0 + i];
+      const double fro = sqrt(fro2[i]);
+      double tau = 1e-3 * eps_trunc * fro / sqrt((double)std::min(m, n));
+      tau = std::max(tau, 64.0 * 2.220446049250313e-16 * fro);
+      fj[i] = AcaFpJob{buf + offC[i], buf + offU[i], buf + offV[i], m, n, cap, 1, tau,
+                       d_rank + i, d_stat + i};
+    }
+    AcaFpJob* d_fj = nullptr;
+    HM_CUDA_TRY(cudaMalloc(&d_fj, sizeof(AcaFpJob) * nb));
+    HM_CUDA_TRY(cudaMemcpyAsync(d_fj, fj.data(), sizeof(AcaFpJob) * nb, cudaMemcpyHostToDevice, st));
+    aca_fp_kernel<<<(unsigned)nb, 512, 0, st>>>(d_fj);
+    HM_CUDA_TRY(cudaGetLastError());
+    std::vector<int32_t> rr(nb), stt(nb);
+    HM_CUDA_TRY(cudaMemcpyAsync(rr.data(), d_rank, 4 * nb, cudaMemcpyDeviceToHost, st));
+    HM_CUDA_TRY(cudaMemcpyAsync(stt.data(), d_stat, 4 * nb, cudaMemcpyDeviceToHost, st));
+    HM_CUDA_TRY(cudaStreamSynchronize(st));
+    // QR + SVD of the ACA cores for the blocks that converged
+    std::vector<CoreJob> cj;
+    std::vector<int64_t> cj_idx;
+    int rmax = 1;
+    for (int64_t i = 0; i < nb; ++i) {
+      if (stt[i] == 2) return fail(HM_ERR_NONFINITE, "non-finite kernel block during compression");
+      const int m = mm[b0 + i], n = nn[b0 + i];
+      if (sabs[i] < 1e-5) { ranks[b0 + i] = 1; continue; }       // compress() zero test
+      if (stt[i] == 1) { ranks[b0 + i] = 1 << 30; continue; }    // not low-rank within the core cap
+      cj.push_back(CoreJob{buf + offU[i], buf + offV[i], buf + offA[i], buf + offB[i], m, n, rr[i], m, n,
+                           m, n, cap, 0, d_rank + nb + (int32_t)cj.size()});
+      cj_idx.push_back(i);
+      rmax = std::max(rmax, (int)rr[i]);
+    }
+    CoreJob* d_cj = nullptr;
+    std::vector<int32_t> kk(cj.size());
+    if (!cj.empty()) {
+      HM_CUDA_TRY(cudaMalloc(&d_cj, sizeof(CoreJob) * cj.size()));
+      HM_CUDA_TRY(cudaMemcpyAsync(d_cj, cj.data(), sizeof(CoreJob) * cj.size(), cudaMemcpyHostToDevice, st));
+      HM_TRY(launch_core_recompress(d_cj, (int)cj.size(), rmax, eps_trunc, d_flags, st));
+      HM_CUDA_TRY(cudaMemcpyAsync(kk.data(), d_rank + nb, 4 * cj.size(), cudaMemcpyDeviceToHost, st));
+      HM_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    for (size_t q = 0; q < cj.size(); ++q) ranks[b0 + cj_idx[q]] = kk[q];
+    // keep the factors of the blocks that become low-rank
+    for (int64_t i = 0; i < nb; ++i) {
+      const int k = ranks[b0 + i];
+      if (k > h->prm.max_rank) continue;
+      const int m = mm[b0 + i], n = nn[b0 + i];
+      SvdCandidateStore::F f;
+      f.m = m; f.n = n; f.k = k;
+      f.A.assign((size_t)m * k, 0.0);
+      f.B.assign((size_t)n * k, 0.0);
+      if (sabs[i] >= 1e-5 && k > 0) {
+        HM_CUDA_TRY(cudaMemcpy(f.A.data(), buf + offA[i], 8 * (size_t)m * k, cudaMemcpyDeviceToHost));
+        HM_CUDA_TRY(cudaMemcpy(f.B.data(), buf + offB[i], 8 * (size_t)n * k, cudaMemcpyDeviceToHost));
+      }
+      store.by_node[nodes[b0 + i]] = std::move(f);
+    }
+    cudaFree(buf); cudaFree(d_r0); cudaFree(d_c0); cudaFree(d_off); cudaFree(d_m); cudaFree(d_n);
+    cudaFree(d_rank); cudaFree(d_stat); cudaFree(d_f2); cudaFree(d_sa); cudaFree(d_flags);
+    cudaFree(d_fj); if (d_cj) cudaFree(d_cj);
+    b0 = b1;
+  }
+  return HM_OK;
+}
+
+// pack FP64 host factors into the pool (storage precision, padded layout)
+__global__ void pack_rk_kernel(const double* __restrict__ A, const double* __restrict__ B, int m, int n, int k,
+                               int64_t npad, int64_t mpad, int storage, void* pool, int64_t off) {
+  const int64_t tot = (npad + mpad) * k;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    double v;
+    if (e < npad * k) {
+      const int64_t j = e % npad, q = e / npad;
+      v = j < n ? B[j + q * n] : 0.0;
+    } else {
+      const int64_t e2 = e - npad * k;
+      const int64_t i = e2 % mpad, q = e2 / mpad;
+      v = i < m ? A[i + q * m] : 0.0;
+    }
+    if (storage == HM_F64) ((double*)pool)[off + e] = v;
+    else if (storage == HM_F32) ((float*)pool)[off + e] = (float)v;
+    else ((__nv_bfloat16*)pool)[off + e] = __double2bfloat16(v);
+  }
+}
+
+int SvdCandidateStore::write_pool(hm_handle* h, const std::vector<int64_t>& rk_leaf) const {
+  const int eb = elem_bytes(h->storage);
+  double* dA = nullptr;
+  size_t cap = 0;
+  for (int64_t li : rk_leaf) {
+    const Leaf& L = h->leaves[li];
+    auto it = by_node.find(L.node);
+    if (it == by_node.end()) return fail(HM_ERR_CUDA, "missing factors of an svd-route leaf");
+    const F& f = it->second;
+    if (f.k == 0) continue;
+    size_t need = (f.A.size() + f.B.size()) * sizeof(double);
+    if (need > cap) {
+      if (dA) cudaFree(dA);
+      HM_CUDA_TRY(cudaMalloc(&dA, need));
+      cap = need;
+    }
+    HM_CUDA_TRY(cudaMemcpyAsync(dA, f.A.data(), f.A.size() * 8, cudaMemcpyHostToDevice, h->stream));
+    HM_CUDA_TRY(cudaMemcpyAsync(dA + f.A.size(), f.B.data(), f.B.size() * 8, cudaMemcpyHostToDevice, h->stream));
+    pack_rk_kernel<<<64, 256, 0, h->stream>>>(dA, dA + f.A.size(), f.m, f.n, f.k, col_pad(f.n, eb),
+                                              col_pad(f.m, eb), h->storage, h->d_rk, L.off);
+    HM_CUDA_TRY(cudaGetLastError());
+    HM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
+  if (dA) cudaFree(dA);
+  return HM_OK;
+}
+
+// ===========================================================================
+// aca_wrapper drop-in: fully pivoted ACA of a host matrix (rank 0 branch).
+// ===========================================================================
+int aca_fp_host(const double* A, double* U, double* V, int m, int n, double eps, int rank, int* out_rank) {
+  if (m <= 0 || n <= 0) return fail(HM_ERR_ARG, "aca_wrapper: empty matrix");
+  const int cap = std::min(m, n);
+  double *dR = nullptr, *dU = nullptr, *dV = nullptr;
+  int32_t* dk = nullptr;
+  AcaFpJob* dj = nullptr;
+  HM_CUDA_TRY(cudaMalloc(&dR, 8ull * m * n));
+  HM_CUDA_TRY(cudaMalloc(&dU, 8ull * m * cap));
+  HM_CUDA_TRY(cudaMalloc(&dV, 8ull * n * cap));
+  HM_CUDA_TRY(cudaMalloc(&dk, 8));
+  HM_CUDA_TRY(cudaMalloc(&dj, sizeof(AcaFpJob)));
+  HM_CUDA_TRY(cudaMemcpy(dR, A, 8ull * m * n, cudaMemcpyHostToDevice));
+  AcaFpJob j{dR, dU, dV, m, n, cap, 1, eps, dk, dk + 1};
+  HM_CUDA_TRY(cudaMemcpy(dj, &j, sizeof(j), cudaMemcpyHostToDevice));
+  aca_fp_kernel<<<1, 512>>>(dj);
+  HM_CUDA_TRY(cudaGetLastError());
+  int32_t res[2];
+  HM_CUDA_TRY(cudaMemcpy(res, dk, 8, cudaMemcpyDeviceToHost));
+  int r = res[0];
+  const int M = std::min(r, rank + 1);
+  if (res[1] == 2) {
+    // NaN residual: identity fallback of ACA_FullyPivoted.cpp:122-147
+    if (m < n) {
+      r = m;
+      std::vector<double> hA(A, A + (size_t)m * n);
+      const int Mf = std::min(r, rank + 1);
+      for (int c = 0; c < Mf; ++c)
+        for (int i = 0; i < m; ++i) U[i + (size_t)c * m] = (i == c) ? 1.0 : 0.0;
+      for (int c = 0; c < Mf; ++c)
+        for (int jx = 0; jx < n; ++jx) V[jx + (size_t)c * n] = hA[c + (size_t)jx * m];
+    } else {
+      r = n;
+      const int Mf = std::min(r, rank + 1);
+      std::memcpy(U, A, sizeof(double) * (size_t)m * Mf);
+      for (int c = 0; c < Mf; ++c)
+        for (int jx = 0; jx < n; ++jx) V[jx + (size_t)c * n] = (jx == c) ? 1.0 : 0.0;
+    }
+  } else if (M > 0) {
+    HM_CUDA_TRY(cudaMemcpy(U, dU, 8ull * m * M, cudaMemcpyDeviceToHost));
+    HM_CUDA_TRY(cudaMemcpy(V, dV, 8ull * n * M, cudaMemcpyDeviceToHost));
+  }
+  cudaFree(dR); cudaFree(dU); cudaFree(dV); cudaFree(dk); cudaFree(dj);
+  *out_rank = r;
+  return HM_OK;
+}
+
+}  // namespace hm

@@ -1,0 +1,617 @@
+// H-matvec on sm_100a (K4): y = H x and y = H' x over the flattened leaf
+// list, the device form of hmat_matvec! (src/harithm.jl:340-354) and
+// transpose_hmat_mat_mul (src/harithm.jl:243-260).
+//
+// Phase 1: one warp per low-rank leaf streams its F1 factor (B for H*x)
+//          with 16-byte loads and writes z = F1' x_seg (k values) to z[].
+// Phase 2: one CTA per window of 512 output rows; each warp owns 32 rows and
+//          accumulates sum_r F2[:,r] z_r over the low-rank leaves and C x_seg
+//          over the dense leaves that cover its rows, in FP64, and stores y.
+// The input is staged as 16-byte aligned shifted copies so that every
+// x-segment load in phase 1 is a vector load, whatever the segment start.
+#include "hm_internal.h"
+#include "hm_lowrank.cuh"
+
+#include <algorithm>
+#include <cstring>
+
+namespace hm {
+
+// ---------------------------------------------------------------------------
+// storage traits: 16-byte vector of factors + matching x vector
+// ---------------------------------------------------------------------------
+template <typename T> struct MvT;
+template <> struct MvT<double> {
+  static constexpr int VW = 2, U = 4;
+  using X = double;
+  using R = double2;
+  struct XV { double2 a; };
+  __device__ static R ld(const double* p) { return __ldcs(reinterpret_cast<const double2*>(p)); }
+  __device__ static XV ldx(const double* p) { return XV{__ldg(reinterpret_cast<const double2*>(p))}; }
+  __device__ static double dot(const R& f, const XV& x, double s) {
+    s = fma(f.x, x.a.x, s);
+    return fma(f.y, x.a.y, s);
+  }
+};
+template <> struct MvT<float> {
+  static constexpr int VW = 4, U = 4;
+  using X = float;
+  using R = float4;
+  struct XV { float4 a; };
+  __device__ static R ld(const float* p) { return __ldcs(reinterpret_cast<const float4*>(p)); }
+  __device__ static XV ldx(const float* p) { return XV{__ldg(reinterpret_cast<const float4*>(p))}; }
+  __device__ static double dot(const R& f, const XV& x, double s) {
+    s = fma((double)f.x, (double)x.a.x, s);
+    s = fma((double)f.y, (double)x.a.y, s);
+    s = fma((double)f.z, (double)x.a.z, s);
+    return fma((double)f.w, (double)x.a.w, s);
+  }
+};
+__device__ __forceinline__ float bf_lo(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf_hi(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
+template <> struct MvT<__nv_bfloat16> {
+  static constexpr int VW = 8, U = 2;
+  using X = float;
+  using R = uint4;
+  struct XV { float4 a, b; };
+  __device__ static R ld(const __nv_bfloat16* p) { return __ldcs(reinterpret_cast<const uint4*>(p)); }
+  __device__ static XV ldx(const float* p) {
+    return XV{__ldg(reinterpret_cast<const float4*>(p)), __ldg(reinterpret_cast<const float4*>(p) + 1)};
+  }
+  __device__ static double dot(const R& f, const XV& x, double s) {
+    s = fma((double)bf_lo(f.x), (double)x.a.x, s);
+    s = fma((double)bf_hi(f.x), (double)x.a.y, s);
+    s = fma((double)bf_lo(f.y), (double)x.a.z, s);
+    s = fma((double)bf_hi(f.y), (double)x.a.w, s);
+    s = fma((double)bf_lo(f.z), (double)x.b.x, s);
+    s = fma((double)bf_hi(f.z), (double)x.b.y, s);
+    s = fma((double)bf_lo(f.w), (double)x.b.z, s);
+    return fma((double)bf_hi(f.w), (double)x.b.w, s);
+  }
+};
+
+// shifted copies: copy q holds x[t - q] at index t (zero outside [q, n+q))
+template <typename TX>
+__global__ void xcopy_kernel(const double* __restrict__ x, int64_t n, TX* __restrict__ xs, int64_t stride, int ncopy) {
+  const int64_t tot = stride * ncopy;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t q = e / stride, t = e % stride;
+    const int64_t s = t - q;
+    xs[e] = (s >= 0 && s < n) ? (TX)x[s] : (TX)0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// phase 1: z = F1' x_seg, one warp per low-rank leaf
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) mv_phase1_kernel(const P1Desc* __restrict__ d, int64_t nd,
+                                                        const T* __restrict__ pool,
+                                                        const typename MvT<T>::X* __restrict__ xs,
+                                                        int64_t xs_stride, double* __restrict__ z) {
+  using Tr = MvT<T>;
+  using TX = typename Tr::X;
+  constexpr int VW = Tr::VW, U = Tr::U;
+  constexpr int XA = 16 / (int)sizeof(TX);
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t b = gw; b < nd; b += nw) {
+    const P1Desc D = d[b];
+    const int q = (XA - (int)(D.seg0 % XA)) % XA;
+    const TX* xb = xs + q * xs_stride + D.seg0 + q;
+    const int nvec = (int)(D.stride / VW);
+    const T* F = pool + D.off;
+    for (int r = 0; r < D.k; r += 2) {
+      const bool two = (r + 1) < D.k;
+      const T* f0 = F + (int64_t)r * D.stride;
+      const T* f1 = two ? f0 + D.stride : f0;
+      double s0 = 0.0, s1 = 0.0;
+      for (int v0 = lane; v0 < nvec; v0 += 32 * U) {
+        typename Tr::R a[U], c[U];
+        typename Tr::XV xv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int v = v0 + 32 * u;
+          if (v < nvec) {
+            a[u] = Tr::ld(f0 + (int64_t)v * VW);
+            c[u] = Tr::ld(f1 + (int64_t)v * VW);
+            xv[u] = Tr::ldx(xb + (int64_t)v * VW);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (v0 + 32 * u < nvec) {
+            s0 = Tr::dot(a[u], xv[u], s0);
+            s1 = Tr::dot(c[u], xv[u], s1);
+          }
+        }
+      }
+      s0 = warp_sum(s0);
+      s1 = warp_sum(s1);
+      if (lane == 0) {
+        z[D.zoff + r] = s0;
+        if (two) z[D.zoff + r + 1] = s1;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// phase 2: y(window) = sum over leaves covering the window
+// ---------------------------------------------------------------------------
+constexpr int P2_NB = 32;      // descriptors staged per round
+constexpr int P2_EMAX = 1024;  // expanded (leaf, column) entries per sub-round
+constexpr uint64_t P2_DENSE_FLAG = 1ull << 63;
+
+template <typename T, typename TD>
+__global__ void __launch_bounds__(512) mv_phase2_kernel(const MvWin* __restrict__ win, const P2Desc* __restrict__ d,
+                                                        const T* __restrict__ rk, const TD* __restrict__ dn,
+                                                        const double* __restrict__ z, const double* __restrict__ x,
+                                                        double* __restrict__ y) {
+  __shared__ P2Desc sd[P2_NB];
+  __shared__ int spre[P2_NB + 1];
+  __shared__ uint64_t e_off[P2_EMAX];
+  __shared__ int32_t e_ro[P2_EMAX];
+  __shared__ uint32_t e_m[P2_EMAX];
+  __shared__ uint32_t e_rs[P2_EMAX];
+  __shared__ double e_z[P2_EMAX];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const MvWin W = win[blockIdx.x];
+  const int lrow = warp * 32 + lane;
+  double acc = 0.0;
+  for (uint32_t b0 = W.begin; b0 < W.end; b0 += P2_NB) {
+    const int nb = (int)min((uint32_t)P2_NB, W.end - b0);
+    __syncthreads();
+    if (warp == 0) {
+      int cnt = 0;
+      if (lane < nb) {
+        sd[lane] = d[b0 + lane];
+        cnt = (int)sd[lane].cnt;
+      }
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      spre[lane + 1] = incl;
+      if (lane == 0) spre[0] = 0;
+    }
+    __syncthreads();
+    const int total = spre[nb];
+    for (int e0 = 0; e0 < total; e0 += P2_EMAX) {
+      const int ne = min(P2_EMAX, total - e0);
+      if (e0 > 0) __syncthreads();
+      for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+        const int ge = e0 + e;
+        int lo = 0, hi = nb - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (spre[mid] <= ge) lo = mid; else hi = mid - 1;
+        }
+        const P2Desc& D = sd[lo];
+        const int c = ge - spre[lo];
+        if (D.type == P2_RK) {
+          e_off[e] = D.off + (uint64_t)c * D.ld;
+          e_rs[e] = 1;
+          e_z[e] = z[D.aux + c];
+        } else if (D.type == P2_DENSE) {
+          e_off[e] = (D.off + (uint64_t)c * D.ld) | P2_DENSE_FLAG;
+          e_rs[e] = 1;
+          e_z[e] = x[D.aux + c];
+        } else {
+          e_off[e] = (D.off + (uint64_t)c) | P2_DENSE_FLAG;
+          e_rs[e] = D.ld;
+          e_z[e] = x[D.aux + c];
+        }
+        e_ro[e] = D.row_off;
+        e_m[e] = D.m;
+      }
+      __syncthreads();
+      if (warp * 32 < (int)W.nrows) {
+        for (int e = 0; e < ne; e += 8) {
+          double v[8];
+          double zz[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            v[u] = 0.0;
+            zz[u] = 0.0;
+            const int ee = e + u;
+            if (ee < ne) {
+              const int lr = lrow - e_ro[ee];
+              if (lr >= 0 && lr < (int)e_m[ee]) {
+                const uint64_t o = e_off[ee];
+                zz[u] = e_z[ee];
+                if (o & P2_DENSE_FLAG)
+                  v[u] = (double)__ldg(dn + (o & ~P2_DENSE_FLAG) + (uint64_t)lr * e_rs[ee]);
+                else
+                  v[u] = from_store<T>(rk[o + (uint64_t)lr]);
+              }
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) acc = fma(v[u], zz[u], acc);
+        }
+      }
+    }
+  }
+  if (lrow < (int)W.nrows) y[W.row0 + lrow] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// plan construction
+// ---------------------------------------------------------------------------
+void free_mv_plan(MvPlan& p) {
+  if (p.d_p1) cudaFree(p.d_p1);
+  if (p.d_p2) cudaFree(p.d_p2);
+  if (p.d_win) cudaFree(p.d_win);
+  p = MvPlan{};
+}
+
+int build_mv_descriptors(hm_handle* h, const std::vector<int64_t>& order, int trans) {
+  const int eb = elem_bytes(h->storage), deb = dense_elem_bytes(h->storage);
+  const int64_t n = h->n;
+  MvPlan& P = trans ? h->bwd : h->fwd;
+  free_mv_plan(P);
+  if (n > (int64_t)UINT32_MAX / 2) return fail(HM_ERR_UNSUPPORTED, "n above 2^31");
+  // z slots in pool order (shared by both directions)
+  std::vector<uint32_t> zoff(h->leaves.size(), 0);
+  int64_t z = 0;
+  for (int64_t li : order)
+    if (h->leaves[li].type == T_RK) { zoff[li] = (uint32_t)z; z += h->leaves[li].k; }
+  if (z > (int64_t)UINT32_MAX) return fail(HM_ERR_UNSUPPORTED, "too many low-rank terms");
+  if (!trans) {
+    if (h->d_z) cudaFree(h->d_z);
+    h->d_z = nullptr;
+    h->zlen = z;
+    if (z) HM_CUDA_TRY(cudaMalloc(&h->d_z, sizeof(double) * z));
+  }
+  std::vector<P1Desc> p1;
+  p1.reserve(order.size());
+  for (int64_t li : order) {
+    const Leaf& L = h->leaves[li];
+    if (L.type != T_RK || L.k == 0) continue;
+    P1Desc D{};
+    const int64_t npad = col_pad(L.n, eb), mpad = col_pad(L.m, eb);
+    if (!trans) { D.off = L.off; D.seg0 = (uint32_t)L.col0; D.len = L.n; D.stride = (uint32_t)npad; }
+    else { D.off = L.off + npad * L.k; D.seg0 = (uint32_t)L.row0; D.len = L.m; D.stride = (uint32_t)mpad; }
+    D.zoff = zoff[li];
+    D.k = (uint16_t)L.k;
+    p1.push_back(D);
+  }
+  const int64_t nwin = (n + MV_WROWS - 1) / MV_WROWS;
+  std::vector<std::vector<P2Desc>> per(nwin);
+  for (int64_t li : order) {
+    const Leaf& L = h->leaves[li];
+    if (L.type == T_RK && L.k == 0) continue;
+    const int64_t npad = col_pad(L.n, eb), mpad = col_pad(L.m, eb);
+    const int64_t o0 = trans ? L.col0 : L.row0;
+    const int64_t oe = o0 + (trans ? L.n : L.m);
+    P2Desc D{};
+    D.m = (uint32_t)(oe - o0);
+    if (L.type == T_RK) {
+      D.type = P2_RK;
+      D.off = trans ? L.off : L.off + npad * L.k;
+      D.ld = (uint32_t)(trans ? npad : mpad);
+      D.aux = zoff[li];
+      D.cnt = (uint32_t)L.k;
+    } else {
+      const int64_t ldc = col_pad(L.m, deb);
+      D.type = trans ? P2_DENSE_T : P2_DENSE;
+      D.off = L.off;
+      D.ld = (uint32_t)ldc;
+      D.aux = (uint32_t)(trans ? L.row0 : L.col0);
+      D.cnt = (uint32_t)(trans ? L.m : L.n);
+    }
+    for (int64_t w = o0 / MV_WROWS; w * MV_WROWS < oe; ++w) {
+      P2Desc E = D;
+      E.row_off = (int32_t)(o0 - w * MV_WROWS);
+      per[w].push_back(E);
+    }
+  }
+  std::vector<P2Desc> p2;
+  std::vector<MvWin> wins(nwin);
+  for (int64_t w = 0; w < nwin; ++w) {
+    wins[w].row0 = (uint32_t)(w * MV_WROWS);
+    wins[w].nrows = (uint32_t)std::min<int64_t>(MV_WROWS, n - w * MV_WROWS);
+    wins[w].begin = (uint32_t)p2.size();
+    p2.insert(p2.end(), per[w].begin(), per[w].end());
+    wins[w].end = (uint32_t)p2.size();
+    std::vector<P2Desc>().swap(per[w]);
+  }
+  if (p2.size() > (size_t)UINT32_MAX) return fail(HM_ERR_UNSUPPORTED, "too many matvec descriptors");
+  P.np1 = (int64_t)p1.size();
+  P.np2 = (int64_t)p2.size();
+  P.nwin = (int32_t)nwin;
+  if (!p1.empty()) {
+    HM_CUDA_TRY(cudaMalloc(&P.d_p1, sizeof(P1Desc) * p1.size()));
+    HM_CUDA_TRY(cudaMemcpy(P.d_p1, p1.data(), sizeof(P1Desc) * p1.size(), cudaMemcpyHostToDevice));
+  }
+  if (!p2.empty()) {
+    HM_CUDA_TRY(cudaMalloc(&P.d_p2, sizeof(P2Desc) * p2.size()));
+    HM_CUDA_TRY(cudaMemcpy(P.d_p2, p2.data(), sizeof(P2Desc) * p2.size(), cudaMemcpyHostToDevice));
+  }
+  HM_CUDA_TRY(cudaMalloc(&P.d_win, sizeof(MvWin) * nwin));
+  HM_CUDA_TRY(cudaMemcpy(P.d_win, wins.data(), sizeof(MvWin) * nwin, cudaMemcpyHostToDevice));
+  return HM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch
+// ---------------------------------------------------------------------------
+static int ensure_xs(hm_handle* h, size_t bytes) {
+  if (h->xs_bytes >= bytes) return HM_OK;
+  if (h->d_xs) cudaFree(h->d_xs);
+  h->d_xs = nullptr;
+  h->xs_bytes = 0;
+  HM_CUDA_TRY(cudaMalloc(&h->d_xs, bytes));
+  h->xs_bytes = bytes;
+  return HM_OK;
+}
+
+template <typename T>
+static int matvec_t(hm_handle* h, const double* d_x, double* d_y, int trans, cudaStream_t st, cudaEvent_t* ev) {
+  using TX = typename MvT<T>::X;
+  constexpr int XA = 16 / (int)sizeof(TX);
+  const MvPlan& P = trans ? h->bwd : h->fwd;
+  const int64_t stride = pad_to(h->n + 64, 64);
+  HM_TRY(ensure_xs(h, sizeof(TX) * stride * XA));
+  TX* xs = (TX*)h->d_xs;
+  if (ev) HM_CUDA_TRY(cudaEventRecord(ev[0], st));
+  {
+    int64_t tot = stride * XA;
+    unsigned g = (unsigned)std::min<int64_t>((tot + 255) / 256, 148 * 16);
+    xcopy_kernel<TX><<<g, 256, 0, st>>>(d_x, h->n, xs, stride, XA);
+  }
+  if (ev) HM_CUDA_TRY(cudaEventRecord(ev[1], st));
+  if (P.np1 > 0) {
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+    int64_t blocks = std::min<int64_t>((P.np1 + 7) / 8, (int64_t)nsm * 8);
+    mv_phase1_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(P.d_p1, P.np1, (const T*)h->d_rk, xs, stride, h->d_z);
+  }
+  if (ev) HM_CUDA_TRY(cudaEventRecord(ev[2], st));
+  if (h->storage == HM_F64)
+    mv_phase2_kernel<T, double><<<P.nwin, 512, 0, st>>>(P.d_win, P.d_p2, (const T*)h->d_rk,
+                                                        (const double*)h->d_dense, h->d_z, d_x, d_y);
+  else
+    mv_phase2_kernel<T, float><<<P.nwin, 512, 0, st>>>(P.d_win, P.d_p2, (const T*)h->d_rk,
+                                                       (const float*)h->d_dense, h->d_z, d_x, d_y);
+  if (ev) HM_CUDA_TRY(cudaEventRecord(ev[3], st));
+  HM_CUDA_TRY(cudaGetLastError());
+  return HM_OK;
+}
+
+int matvec_device(hm_handle* h, const double* d_x, double* d_y, int trans, cudaStream_t st, cudaEvent_t* ev) {
+  switch (h->storage) {
+    case HM_F64: return matvec_t<double>(h, d_x, d_y, trans, st, ev);
+    case HM_F32: return matvec_t<float>(h, d_x, d_y, trans, st, ev);
+    default: return matvec_t<__nv_bfloat16>(h, d_x, d_y, trans, st, ev);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// exact FP64 rows (K14): y_i = sum_j K(x_rows[i], x_j) x_j + shift * x_rows[i]
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) exact_rows_kernel(KernelDesc kd, const double* __restrict__ geom, int64_t n,
+                                                         const int64_t* __restrict__ rows,
+                                                         const double* __restrict__ x, double* __restrict__ y) {
+  __shared__ double red[32];
+  const int64_t i = rows[blockIdx.x];
+  double s = 0.0;
+  for (int64_t j = threadIdx.x; j < n; j += blockDim.x) s = fma(kernel_eval(kd, geom, n, i, j), x[j], s);
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) y[blockIdx.x] = s + kd.shift * x[i];
+}
+
+int exact_rows_device(hm_handle* h, const int64_t* d_rows, int64_t nrows, const double* d_x, double* d_y,
+                      cudaStream_t st) {
+  if (nrows <= 0) return HM_OK;
+  for (int64_t b0 = 0; b0 < nrows; b0 += (1ll << 30)) {
+    unsigned nb = (unsigned)std::min<int64_t>(nrows - b0, 1ll << 30);
+    exact_rows_kernel<<<nb, 512, 0, st>>>(h->kd, h->d_geom, h->n, d_rows + b0, d_x, d_y + b0);
+  }
+  HM_CUDA_TRY(cudaGetLastError());
+  return HM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// densify (to_fmat, src/utils.jl:162-192), leaf factors, shift, scale, copy
+// ---------------------------------------------------------------------------
+struct LeafDev {
+  int64_t row0, col0, off;
+  int32_t m, n, k, type;
+};
+
+template <typename T, typename TD>
+__global__ void to_dense_kernel(const LeafDev* __restrict__ L, const T* __restrict__ rk, const TD* __restrict__ dn,
+                                int64_t n, double* __restrict__ out) {
+  const LeafDev D = L[blockIdx.x];
+  const int eb = (int)sizeof(T), deb = (int)sizeof(TD);
+  const int64_t tot = (int64_t)D.m * D.n;
+  for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
+    const int i = (int)(e % D.m), j = (int)(e / D.m);
+    double v;
+    if (D.type == T_DENSE) {
+      v = (double)dn[D.off + i + (int64_t)j * col_pad_dev(D.m, deb)];
+    } else {
+      const int64_t npad = col_pad_dev(D.n, eb), mpad = col_pad_dev(D.m, eb);
+      const T* B = rk + D.off;
+      const T* A = B + npad * D.k;
+      v = 0.0;
+      for (int q = 0; q < D.k; ++q) v = fma(from_store<T>(A[i + q * mpad]), from_store<T>(B[j + q * npad]), v);
+    }
+    out[(D.row0 + i) + (D.col0 + j) * n] = v;
+  }
+}
+
+int to_dense(const hm_handle* h, double* d_out) {
+  std::vector<LeafDev> L(h->leaves.size());
+  for (size_t i = 0; i < L.size(); ++i) {
+    const Leaf& x = h->leaves[i];
+    L[i] = LeafDev{x.row0, x.col0, x.off, x.m, x.n, x.k, x.type};
+  }
+  if (L.empty()) return HM_OK;
+  LeafDev* dL = nullptr;
+  HM_CUDA_TRY(cudaMalloc(&dL, sizeof(LeafDev) * L.size()));
+  HM_CUDA_TRY(cudaMemcpyAsync(dL, L.data(), sizeof(LeafDev) * L.size(), cudaMemcpyHostToDevice, h->stream));
+  const unsigned nb = (unsigned)L.size();
+  switch (h->storage) {
+    case HM_F64:
+      to_dense_kernel<double, double><<<nb, 256, 0, h->stream>>>(dL, (const double*)h->d_rk, (const double*)h->d_dense, h->n, d_out);
+      break;
+    case HM_F32:
+      to_dense_kernel<float, float><<<nb, 256, 0, h->stream>>>(dL, (const float*)h->d_rk, (const float*)h->d_dense, h->n, d_out);
+      break;
+    default:
+      to_dense_kernel<__nv_bfloat16, float><<<nb, 256, 0, h->stream>>>(dL, (const __nv_bfloat16*)h->d_rk, (const float*)h->d_dense, h->n, d_out);
+  }
+  HM_CUDA_TRY(cudaGetLastError());
+  HM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  cudaFree(dL);
+  return HM_OK;
+}
+
+static inline double bf16_bits_to_double(uint16_t b) {
+  uint32_t w = (uint32_t)b << 16;
+  float f;
+  std::memcpy(&f, &w, 4);
+  return (double)f;
+}
+
+int leaf_factors_f64(const hm_handle* h, int64_t leaf, double* A, double* B) {
+  const Leaf& L = h->leaves[leaf];
+  if (L.type != T_RK) return fail(HM_ERR_ARG, "leaf is not low-rank");
+  const int eb = elem_bytes(h->storage);
+  const int64_t npad = col_pad(L.n, eb), mpad = col_pad(L.m, eb);
+  const int64_t tot = (npad + mpad) * L.k;
+  std::vector<char> buf(tot * eb);
+  if (tot) HM_CUDA_TRY(cudaMemcpy(buf.data(), (const char*)h->d_rk + L.off * eb, tot * eb, cudaMemcpyDeviceToHost));
+  auto get = [&](int64_t e) -> double {
+    if (eb == 8) return ((const double*)buf.data())[e];
+    if (eb == 4) return (double)((const float*)buf.data())[e];
+    return bf16_bits_to_double(((const uint16_t*)buf.data())[e]);
+  };
+  for (int q = 0; q < L.k; ++q) {
+    for (int j = 0; j < L.n; ++j) B[j + (int64_t)q * L.n] = get(j + q * npad);
+    for (int i = 0; i < L.m; ++i) A[i + (int64_t)q * L.m] = get(npad * L.k + i + q * mpad);
+  }
+  return HM_OK;
+}
+
+template <typename TD>
+__global__ void shift_kernel(const int64_t* __restrict__ offs, const int32_t* __restrict__ ms, int nleaf,
+                             const int32_t* __restrict__ lds, TD* dn, double lam) {
+  const int b = blockIdx.x;
+  for (int i = threadIdx.x; i < ms[b]; i += blockDim.x) {
+    TD* p = dn + offs[b] + i + (int64_t)i * lds[b];
+    *p = (TD)((double)*p + lam);
+  }
+}
+
+int apply_shift(hm_handle* h, double lam) {
+  std::vector<int64_t> offs;
+  std::vector<int32_t> ms, lds;
+  const int deb = dense_elem_bytes(h->storage);
+  for (auto& L : h->leaves)
+    if (L.type == T_DENSE && L.row0 == L.col0 && L.m == L.n) {
+      offs.push_back(L.off);
+      ms.push_back(L.m);
+      lds.push_back((int32_t)col_pad(L.m, deb));
+    }
+  if (!offs.empty()) {
+    int64_t* d_o = nullptr;
+    int32_t *d_m = nullptr, *d_l = nullptr;
+    HM_CUDA_TRY(cudaMalloc(&d_o, 8 * offs.size()));
+    HM_CUDA_TRY(cudaMalloc(&d_m, 4 * ms.size()));
+    HM_CUDA_TRY(cudaMalloc(&d_l, 4 * lds.size()));
+    HM_CUDA_TRY(cudaMemcpy(d_o, offs.data(), 8 * offs.size(), cudaMemcpyHostToDevice));
+    HM_CUDA_TRY(cudaMemcpy(d_m, ms.data(), 4 * ms.size(), cudaMemcpyHostToDevice));
+    HM_CUDA_TRY(cudaMemcpy(d_l, lds.data(), 4 * lds.size(), cudaMemcpyHostToDevice));
+    if (h->storage == HM_F64)
+      shift_kernel<double><<<(unsigned)offs.size(), 128, 0, h->stream>>>(d_o, d_m, (int)offs.size(), d_l, (double*)h->d_dense, lam);
+    else
+      shift_kernel<float><<<(unsigned)offs.size(), 128, 0, h->stream>>>(d_o, d_m, (int)offs.size(), d_l, (float*)h->d_dense, lam);
+    HM_CUDA_TRY(cudaGetLastError());
+    HM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    cudaFree(d_o); cudaFree(d_m); cudaFree(d_l);
+  }
+  h->kd.shift += lam;
+  return HM_OK;
+}
+
+template <typename T>
+__global__ void scale_kernel(T* p, int64_t cnt, double u) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x)
+    p[e] = to_store<T>(from_store<T>(p[e]) * u);
+}
+
+int apply_scale(hm_handle* h, double u) {
+  const int eb = elem_bytes(h->storage), deb = dense_elem_bytes(h->storage);
+  // dense pool: every element (padding is zero and stays zero)
+  if (h->dense_bytes) {
+    if (h->storage == HM_F64) scale_kernel<double><<<592, 256, 0, h->stream>>>((double*)h->d_dense, h->dense_bytes / deb, u);
+    else scale_kernel<float><<<592, 256, 0, h->stream>>>((float*)h->d_dense, h->dense_bytes / deb, u);
+  }
+  // low-rank leaves: the A factor only, as u*H scales H.A (src/harithm.jl:487)
+  for (auto& L : h->leaves) {
+    if (L.type != T_RK || L.k == 0) continue;
+    const int64_t npad = col_pad(L.n, eb), mpad = col_pad(L.m, eb);
+    const int64_t o = L.off + npad * L.k, cnt = mpad * L.k;
+    unsigned g = (unsigned)std::min<int64_t>((cnt + 255) / 256, 64);
+    if (h->storage == HM_F64) scale_kernel<double><<<g, 256, 0, h->stream>>>((double*)h->d_rk + o, cnt, u);
+    else if (h->storage == HM_F32) scale_kernel<float><<<g, 256, 0, h->stream>>>((float*)h->d_rk + o, cnt, u);
+    else scale_kernel<__nv_bfloat16><<<g, 256, 0, h->stream>>>((__nv_bfloat16*)h->d_rk + o, cnt, u);
+  }
+  HM_CUDA_TRY(cudaGetLastError());
+  HM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->kd.shift *= u;
+  return HM_OK;
+}
+
+static int dup(void** dst, const void* src, size_t bytes) {
+  *dst = nullptr;
+  if (!bytes || !src) return HM_OK;
+  cudaError_t e = cudaMalloc(dst, bytes);
+  if (e != cudaSuccess) return fail(HM_ERR_OOM, std::string("copy: ") + cudaGetErrorString(e));
+  HM_CUDA_TRY(cudaMemcpy(*dst, src, bytes, cudaMemcpyDeviceToDevice));
+  return HM_OK;
+}
+
+int copy_handle(const hm_handle* h, hm_handle** out) {
+  hm_handle* c = new hm_handle();
+  c->prm = h->prm; c->n = h->n; c->dim = h->dim; c->device = h->device; c->kd = h->kd;
+  c->cl_s = h->cl_s; c->cl_e = h->cl_e; c->cl_left = h->cl_left; c->cl_right = h->cl_right;
+  c->cl_depth = h->cl_depth; c->nodes = h->nodes; c->leaves = h->leaves; c->depth = h->depth;
+  c->storage = h->storage; c->kmax = h->kmax; c->rk_bytes = h->rk_bytes; c->dense_bytes = h->dense_bytes;
+  c->zlen = h->zlen;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete c; return fail(HM_ERR_CUDA, cudaGetErrorString(e)); }
+  int s = HM_OK;
+  auto chk = [&](int st) { if (s == HM_OK) s = st; };
+  chk(dup((void**)&c->d_geom, h->d_geom, sizeof(double) * h->n * h->dim));
+  chk(dup(&c->d_rk, h->d_rk, h->rk_bytes));
+  chk(dup(&c->d_dense, h->d_dense, h->dense_bytes));
+  chk(dup((void**)&c->d_z, h->d_z, sizeof(double) * h->zlen));
+  for (int t = 0; t < 2 && s == HM_OK; ++t) {
+    const MvPlan& a = t ? h->bwd : h->fwd;
+    MvPlan& b = t ? c->bwd : c->fwd;
+    b.np1 = a.np1; b.np2 = a.np2; b.nwin = a.nwin;
+    chk(dup((void**)&b.d_p1, a.d_p1, sizeof(P1Desc) * a.np1));
+    chk(dup((void**)&b.d_p2, a.d_p2, sizeof(P2Desc) * a.np2));
+    chk(dup((void**)&b.d_win, a.d_win, sizeof(MvWin) * a.nwin));
+  }
+  if (s == HM_OK && h->lu) s = lu_copy(h, c);
+  c->factorized = h->factorized;
+  if (s != HM_OK) {
+    free_handle_data(c);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return s;
+  }
+  *out = c;
+  return HM_OK;
+}
+
+}  // namespace hm

@@ -1,0 +1,353 @@
+"""hmatrix -- host-side mirror of Hmatrix.jl's hot path over libhmatb200.
+
+Same names and meaning as the reference API (README.md:22-44,
+src/utils.jl:8-26, src/cluster.jl:36-45, src/harithm.jl:317-329,
+src/hlu.jl:465-562)::
+
+    Hparams.Geom = np.linspace(0, 10, 2000)
+    Hparams.Kernel = Cauchy(1.0)            # (x,y)->1/(1+(x-y)^2)
+    Hparams.MaxBlock, Hparams.MinBlock, Hparams.MaxRank = 500, 64, 5
+    c, H = NewHmat()
+    A = FullMat(Hparams.Kernel, c.X, c.X)
+    H * y ; lu(H) ; H.solve(y)               # H\\y
+
+Vectors live in the cluster-permuted order ``c.X`` exactly as in the
+reference.  All arithmetic runs in the CUDA library; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import HmError, check, lib
+from .cluster import Cluster, construct_cluster, neighbor_pairs
+from .kernels import Cauchy, Gauss, InvQuad, Kernel
+
+__all__ = [
+    "Hparams", "Params", "NewHmat", "FullMat", "Hmat", "lu", "lu_", "getl", "getu", "info",
+    "Cauchy", "InvQuad", "Gauss", "Kernel", "Cluster", "construct_cluster", "HmError",
+    "aca_wrapper", "F64", "F32", "BF16",
+]
+
+F64, F32, BF16 = _lib.HM_F64, _lib.HM_F32, _lib.HM_BF16
+
+
+@dataclass
+class Params:
+    """``Params`` of src/utils.jl:8-24 (plus the device-side choices)."""
+    Geom: Optional[np.ndarray] = None
+    Adj: Optional[object] = None          # None: identity adjacency sparse(I,n,n)
+    εComp: float = 1e-10
+    MaxRank: int = 16
+    MaxBlock: int = -1
+    MinBlock: int = 64
+    Kernel: Optional[Kernel] = None
+    CompMethod: str = "svd"
+    ConsMethod: str = "aca2"
+    εTrunc: float = 1e-10
+    verbose: bool = False
+    aca_force: bool = False
+    Tree: str = "kmeans"                  # "kmeans" (reference) | "bisect"
+    Storage: int = F64                    # precision of the stored factors
+    Shift: float = 0.0                    # lambda of H + lambda*I applied at construction
+    Device: int = 0
+    RankCap: int = 0                      # rank capacity during H-LU (0: automatic)
+
+
+Hparams = Params()
+
+
+def FullMat(f, X, Y):
+    """``FullMat``/``kernel_full`` (src/cluster.jl:45,258-275), evaluated on the host."""
+    X = np.asarray(X, dtype=np.float64)
+    Y = np.asarray(Y, dtype=np.float64)
+    return np.ascontiguousarray(f(X.reshape(len(X), -1), Y.reshape(len(Y), -1)))
+
+
+def _params_struct(prm: Params, dim: int):
+    p = _lib.hm_params()
+    check(lib().hm_default_params(C.byref(p)))
+    if not isinstance(prm.Kernel, Kernel):
+        raise HmError(_lib.HM_ERR_ARG, "Hparams.Kernel must be a device kernel (Cauchy/InvQuad/Gauss); "
+                      "an arbitrary closure cannot run on the GPU")
+    p.dim = dim
+    p.kernel = prm.Kernel.kind
+    p.kparam = prm.Kernel.p
+    p.shift = prm.Shift
+    p.eps_comp = prm.εComp
+    p.eps_trunc = prm.εTrunc
+    p.max_rank = prm.MaxRank
+    p.max_block = prm.MaxBlock
+    p.min_block = prm.MinBlock
+    if prm.ConsMethod == "aca2":
+        p.cons_method = _lib.HM_CONS_ACA2
+    elif prm.ConsMethod == "svd":
+        p.cons_method = _lib.HM_CONS_SVD
+    else:
+        raise HmError(_lib.HM_ERR_ARG, "ConsMethod %r is not on the device path (use 'aca2' or 'svd')"
+                      % prm.ConsMethod)
+    if prm.CompMethod != "svd":
+        raise HmError(_lib.HM_ERR_ARG, "CompMethod %r: only 'svd' works in the reference" % prm.CompMethod)
+    p.aca_force = int(prm.aca_force)
+    p.storage = prm.Storage
+    p.device = prm.Device
+    p.rank_cap = prm.RankCap
+    return p
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+def _torch_stream():
+    """cudaStream_t of torch's current stream; the legacy default stream is
+    handle 0 in torch, passed as cudaStreamLegacy (0x1) so that the library
+    does not fall back to its own stream."""
+    import torch
+    s = torch.cuda.current_stream().cuda_stream
+    return C.c_void_p(s if s else 1)
+
+
+class Hmat:
+    """Opaque H-matrix living on the GPU (mirror of ``Hmat``, src/cluster.jl:21-34)."""
+
+    __array_ufunc__ = None        # ndarray * H defers to H.__rmul__
+
+    def __init__(self, handle, n, cluster=None):
+        self._h = C.c_void_p(handle)
+        self.m = self.n = n
+        self.c = cluster
+
+    def __del__(self):
+        try:
+            if self._h and self._h.value:
+                lib().hm_destroy(self._h)
+                self._h = C.c_void_p(0)
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        return (self.m, self.n)
+
+    # -- structure -----------------------------------------------------------
+    def info(self):
+        o = _lib.hm_info_t()
+        check(lib().hm_info(self._h, C.byref(o)))
+        return o
+
+    def leaves(self):
+        cnt = C.c_int64(0)
+        check(lib().hm_leaves(self._h, 0, None, C.byref(cnt)))
+        out = np.zeros((cnt.value, 6), np.int64)
+        check(lib().hm_leaves(self._h, cnt.value, _ptr(out), C.byref(cnt)))
+        return out
+
+    def leaf_factors(self, i):
+        L = self.leaves()[i]
+        A = np.zeros((L[3], L[5]), order="F")
+        B = np.zeros((L[4], L[5]), order="F")
+        check(lib().hm_leaf_factors(self._h, int(i), _ptr(A), _ptr(B)))
+        return A, B
+
+    def to_dense(self):
+        """``Array(H)`` (src/utils.jl:192); for a factorised H the packed L\\U."""
+        out = np.zeros((self.n, self.n), order="F")
+        check(lib().hm_to_dense(self._h, _ptr(out), 0))
+        return out
+
+    # -- arithmetic ------------------------------------------------------------
+    def matvec(self, x, trans=False):
+        """``H*x`` / ``H'*x`` for a vector or an n x k matrix (src/harithm.jl:317-329)."""
+        try:
+            import torch
+            if isinstance(x, torch.Tensor):
+                return self._matvec_torch(x, trans)
+        except ImportError:
+            pass
+        x = np.asarray(x, dtype=np.float64)
+        X = np.asfortranarray(x.reshape(self.n, -1))
+        Y = np.zeros_like(X, order="F")
+        check(lib().hm_matvec(self._h, _ptr(X), _ptr(Y), X.shape[1], int(bool(trans)), 0, None))
+        return Y.reshape(x.shape)
+
+    def _matvec_torch(self, x, trans):
+        import torch
+        if not x.is_cuda or x.dtype != torch.float64:
+            raise HmError(_lib.HM_ERR_ARG, "torch input must be a CUDA float64 tensor")
+        X = x.reshape(self.n, -1).t().contiguous()      # columns contiguous
+        Y = torch.empty_like(X)
+        check(lib().hm_matvec(self._h, C.c_void_p(X.data_ptr()), C.c_void_p(Y.data_ptr()), X.shape[0],
+                              int(bool(trans)), _lib.HM_FLAG_DEVICE_PTRS, _torch_stream()))
+        return Y.t().reshape(x.shape)
+
+    def __mul__(self, x):
+        if isinstance(x, (int, float)):
+            return self.scaled(float(x))
+        return self.matvec(x)
+
+    __matmul__ = __mul__
+
+    def __rmul__(self, x):
+        if isinstance(x, (int, float)):
+            return self.scaled(float(x))
+        # v*H  (src/harithm.jl:331-337): rows of v times H = (H' v')'
+        v = np.atleast_2d(np.asarray(x, dtype=np.float64))
+        return self.matvec(v.T, trans=True).T
+
+    def exact_rows(self, rows, x):
+        """Exact FP64 rows of (K + shift I) x: the dense FullMat oracle for sampled rows."""
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(len(rows))
+        check(lib().hm_exact_rows(self._h, _ptr(rows), len(rows), _ptr(x), _ptr(y), 0, None))
+        return y
+
+    def copy(self):
+        out = C.c_void_p()
+        check(lib().hm_copy(self._h, C.byref(out)))
+        return Hmat(out.value, self.n, self.c)
+
+    def add_identity(self, lam):
+        """``lam*I + H`` (src/harithm.jl:457-473), returning a new H."""
+        H = self.copy()
+        check(lib().hm_add_identity(H._h, float(lam)))
+        return H
+
+    def scaled(self, u):
+        """``u*H`` (src/harithm.jl:478-498), returning a new H."""
+        H = self.copy()
+        check(lib().hm_scale(H._h, float(u)))
+        return H
+
+    def __add__(self, other):
+        from numbers import Number
+        if isinstance(other, _Identity):
+            return self.add_identity(other.lam)
+        raise TypeError("H + %r is outside the hot path" % type(other))
+
+    __radd__ = __add__
+
+    def __neg__(self):
+        return self.scaled(-1.0)
+
+    # -- LU / solve ------------------------------------------------------------
+    def lu_(self):
+        """``lu!(H)`` (src/hlu.jl:465-515), in place."""
+        check(lib().hm_lu(self._h))
+        return self
+
+    @property
+    def P(self):
+        """Row permutation (0-based) of a factorised H: H[P,:] = L*U."""
+        if not self.info().factorized:
+            return np.zeros(0, np.int64)
+        P = np.zeros(self.n, np.int64)
+        check(lib().hm_lu_perm(self._h, _ptr(P)))
+        return P
+
+    def solve(self, y):
+        """``a\\y`` (src/hlu.jl:553-562) for a factorised H."""
+        try:
+            import torch
+            if isinstance(y, torch.Tensor):
+                Y = y.reshape(self.n, -1).t().contiguous()
+                X = torch.empty_like(Y)
+                check(lib().hm_solve(self._h, C.c_void_p(Y.data_ptr()), C.c_void_p(X.data_ptr()), Y.shape[0],
+                                     _lib.HM_FLAG_DEVICE_PTRS, _torch_stream()))
+                return X.t().reshape(y.shape)
+        except ImportError:
+            pass
+        y = np.asarray(y, dtype=np.float64)
+        B = np.asfortranarray(y.reshape(self.n, -1))
+        X = np.zeros_like(B, order="F")
+        check(lib().hm_solve(self._h, _ptr(B), _ptr(X), B.shape[1], 0, None))
+        return X.reshape(y.shape)
+
+
+class _Identity:
+    def __init__(self, lam=1.0):
+        self.lam = lam
+
+    def __mul__(self, s):
+        return _Identity(self.lam * s)
+
+    __rmul__ = __mul__
+
+
+I = _Identity(1.0)
+
+
+def NewHmat(prm: Params = None):
+    """``c, H = NewHmat()`` (src/cluster.jl:36-43)."""
+    prm = Hparams if prm is None else prm
+    if prm.Geom is None:
+        raise HmError(_lib.HM_ERR_ARG, "Hparams.Geom is not set")
+    X = np.asarray(prm.Geom, dtype=np.float64)
+    if X.ndim == 1:
+        X = X.reshape(-1, 1)
+    n, d = X.shape
+    if prm.MaxBlock == -1:
+        prm.MaxBlock = n // 4                          # src/cluster.jl:37-39
+    c = construct_cluster(X, prm.MinBlock, prm.Tree)
+    p = _params_struct(prm, d)
+    geom = np.asfortranarray(c.X)
+    nb = neighbor_pairs(c, prm.Adj)
+    out = C.c_void_p()
+    check(lib().hm_new(C.byref(p), n, _ptr(geom), c.ncluster, _ptr(c.s), _ptr(c.e), _ptr(c.left),
+                       _ptr(c.right), 0 if nb is None else len(nb),
+                       None if nb is None else _ptr(np.ascontiguousarray(nb)), C.byref(out)))
+    return c, Hmat(out.value, n, c)
+
+
+def lu(H: Hmat):
+    """``lu(H)`` (src/hlu.jl:517-521): a factorised copy."""
+    return H.copy().lu_()
+
+
+def lu_(H: Hmat):
+    return H.lu_()
+
+
+def getl(A, unitdiag=True):
+    """src/hlu.jl:193-199."""
+    L = np.tril(A)
+    if unitdiag:
+        np.fill_diagonal(L, 1.0)
+    return L
+
+
+def getu(A, unitdiag=False):
+    """src/hlu.jl:201-207."""
+    U = np.triu(A)
+    if unitdiag:
+        np.fill_diagonal(U, 1.0)
+    return U
+
+
+def info(H: Hmat):
+    """``info(H)`` (src/utils.jl:83-110): (dense count, Rk count, depth, compression ratio)."""
+    o = H.info()
+    return o.n_dense, o.n_rk, o.depth, o.compress_ratio
+
+
+def aca_wrapper(A, eps, rank):
+    """The reference's native ``aca_wrapper`` (deps/src/ACA_FullyPivoted.cpp:218-236)
+    called as in src/hlu.jl:9-18: returns (U, V) with min(R, rank+1) columns."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    m, n = A.shape
+    U = np.zeros((m, min(m, n, rank + 1)), order="F")
+    V = np.zeros((n, min(m, n, rank + 1)), order="F")
+    Uf = np.zeros((m, max(1, min(m, n))), order="F")
+    Vf = np.zeros((n, max(1, min(m, n))), order="F")
+    pd = C.POINTER(C.c_double)
+    R = lib().aca_wrapper(A.ctypes.data_as(pd), Uf.ctypes.data_as(pd), Vf.ctypes.data_as(pd), m, n,
+                          float(eps), int(rank))
+    if R < 0:
+        raise HmError(-R, _lib.last_error())
+    M = min(R, rank + 1)
+    return Uf[:, :M].copy(), Vf[:, :M].copy(), R

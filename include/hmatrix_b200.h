@@ -1,0 +1,194 @@
+/*
+ * hmatrix_b200.h -- C ABI of the B200 (sm_100a) H-matrix hot path.
+ *
+ * Drop-in boundary for the hot path of Hmatrix.jl: construction with ACA/SVD
+ * compression (NewHmat), H-matvec (H*y, H*V, transposed), H-LU (lu / lu!)
+ * and the triangular H-solve (H\y).  Every entry point takes plain pointers
+ * and sizes, returns an int status (HM_OK == 0) and never aborts; the text of
+ * the last error of the calling thread is available from hm_last_error().
+ *
+ * Index space: exactly as in the reference, vectors live in the
+ * cluster-permuted order c.X = Geom[c.P,:] (src/cluster.jl:248-249,
+ * test/harithm.jl:9-11).  The caller builds the cluster tree (the reference
+ * does it on the host with sklearn, src/cluster.jl:196-256) and passes the
+ * permuted geometry plus the flattened tree; the library builds the block
+ * partition of src/cluster.jl:48-133 and compresses on the GPU.
+ *
+ * Pointers are host pointers unless HM_FLAG_DEVICE_PTRS is given, in which
+ * case they must be device pointers on the handle's device.
+ */
+#ifndef HMATRIX_B200_H
+#define HMATRIX_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define HM_OK              0
+#define HM_ERR_ARG         1   /* invalid argument or configuration          */
+#define HM_ERR_CUDA        2   /* CUDA runtime error                         */
+#define HM_ERR_OOM         3   /* device or host allocation failed           */
+#define HM_ERR_STATE       4   /* frozen (factorised) / not factorised       */
+#define HM_ERR_SINGULAR    5   /* exactly zero pivot in a diagonal leaf      */
+#define HM_ERR_RANK        6   /* a rank exceeded the handle's rank capacity */
+#define HM_ERR_NONFINITE   7   /* NaN/Inf met where a finite value is needed */
+#define HM_ERR_UNSUPPORTED 8   /* valid request outside what is implemented  */
+#define HM_ERR_TIMEOUT     9   /* a bounded device wait gave up              */
+
+/* ---- kernels (Hparams.Kernel has to be one of these on the device) ----- */
+#define HM_KERNEL_CAUCHY   1   /* 1/(1 + |x-y|^2/p^2)      p = kparam (ell)   */
+#define HM_KERNEL_INVQUAD  2   /* 1/(p + |x-y|^2)          p = kparam (c)     */
+#define HM_KERNEL_GAUSS    3   /* exp(-|x-y|^2/(2 p^2))    p = kparam (ell)   */
+
+/* ---- construction methods (Hparams.ConsMethod) --------------------------- */
+#define HM_CONS_ACA2       1   /* partially pivoted ACA, src/hlu.jl:59-111    */
+#define HM_CONS_SVD        2   /* dense block + truncated SVD, cluster.jl:99  */
+
+/* ---- storage precision of the matvec copy of the factors ----------------- */
+#define HM_F64             0
+#define HM_F32             1
+#define HM_BF16            2   /* BF16 low-rank factors, FP32 dense leaves    */
+
+/* ---- flags ------------------------------------------------------------- */
+#define HM_FLAG_DEVICE_PTRS 1u
+
+/* Mirror of the reference's global Params (src/utils.jl:8-24) restricted
+ * to the fields the hot path reads, plus the device kernel description. */
+typedef struct hm_params {
+    int32_t dim;          /* 1..3 spatial dimension of Geom                  */
+    int32_t kernel;       /* HM_KERNEL_*                                      */
+    double  kparam;       /* kernel parameter (ell or c)                      */
+    double  shift;        /* lambda of  H + lambda*I (diagonal of diag. leaves) */
+    double  eps_comp;     /* Hparams.εComp  (ACA stop tolerance)              */
+    double  eps_trunc;    /* Hparams.εTrunc (relative SVD truncation)         */
+    int32_t max_rank;     /* Hparams.MaxRank                                  */
+    int32_t max_block;    /* Hparams.MaxBlock (-1 -> n/4)                     */
+    int32_t min_block;    /* Hparams.MinBlock                                 */
+    int32_t cons_method;  /* HM_CONS_*                                        */
+    int32_t aca_force;    /* Hparams.aca_force                                */
+    int32_t storage;      /* HM_F64 / HM_F32 / HM_BF16                        */
+    int32_t device;       /* CUDA device ordinal                              */
+    int32_t rank_cap;     /* capacity of low-rank blocks during H-LU (0: auto) */
+    int32_t reserved[6];
+} hm_params;
+
+/* info(H) of src/utils.jl:83-110 plus the byte counts used for rooflines. */
+typedef struct hm_info_t {
+    int64_t n;
+    int64_t n_dense;          /* number of dense leaves                        */
+    int64_t n_rk;             /* number of low-rank leaves                     */
+    int64_t depth;            /* depth of the block tree (root = 1)            */
+    double  compress_ratio;   /* stored entries / n^2                          */
+    int64_t dense_entries;    /* sum m*n over dense leaves                     */
+    int64_t rk_entries;       /* sum k*(m+n) over low-rank leaves              */
+    int64_t max_rank;         /* largest rank                                  */
+    int64_t pool_bytes;       /* bytes the matvec streams (padded factors)     */
+    int64_t matvec_bytes;     /* algorithmic bytes of one single-RHS matvec    */
+    int64_t n_row_groups;
+    int64_t factorized;       /* 1 after lu!                                   */
+    int64_t reserved[4];
+} hm_info_t;
+
+typedef struct hm_handle hm_handle;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int hm_version(void);
+
+/* Copy the last error message of the calling thread into buf (NUL-ended). */
+int hm_last_error(char* buf, int64_t len);
+
+/* Fill *p with the reference defaults (src/utils.jl:12-23): εComp=1e-10,
+ * MaxRank=16, MaxBlock=-1, MinBlock=64, ConsMethod aca2, εTrunc=1e-10,
+ * Cauchy kernel with p=1, dim=1, FP64 storage, device 0. */
+int hm_default_params(hm_params* p);
+
+/* c,H = NewHmat()  (src/cluster.jl:36-133).
+ *   geom      n*dim doubles, column-major, ALREADY permuted (c.X).
+ *   cluster tree: ncluster entries in the pre-order of the reference's
+ *   downward pass (ids 1..ncluster -> index 0..ncluster-1):
+ *   cl_s[i] 0-based start, cl_e[i] exclusive end, cl_left/cl_right child
+ *   index or -1 for a leaf (src/cluster.jl:223-240).
+ *   nb_pairs  NULL for the identity adjacency Adj = I (two clusters are
+ *   neighbours iff their ranges intersect), else 2*n_nb int64 (i, j) cluster
+ *   index pairs for which Neighbors[i+1, j+1] != 0 (src/cluster.jl:140-169). */
+int hm_new(const hm_params* p, int64_t n, const double* geom,
+           int64_t ncluster, const int64_t* cl_s, const int64_t* cl_e,
+           const int64_t* cl_left, const int64_t* cl_right,
+           int64_t n_nb, const int64_t* nb_pairs, hm_handle** out);
+
+/* free a handle */
+int hm_destroy(hm_handle* h);
+
+/* info(H) (src/utils.jl:83-110) and roofline byte counts. */
+int hm_info(const hm_handle* h, hm_info_t* out);
+
+/* Leaf list in the order of the reference recursion (children [11 12; 21 22]
+ * visited 11,12,21,22; src/cluster.jl:122-127): for leaf i,
+ * out[6i..6i+5] = (type 0 dense / 1 low-rank, row0, col0, m, n, rank). */
+int hm_leaves(const hm_handle* h, int64_t cap, int64_t* out, int64_t* count);
+
+/* Factors of low-rank leaf `leaf` (index in hm_leaves order) as FP64,
+ * A (m x k) and B (n x k) column-major, H_leaf = A*B' (src/cluster.jl:118-120). */
+int hm_leaf_factors(const hm_handle* h, int64_t leaf, double* A, double* B);
+
+/* Array(H) / to_fmat (src/utils.jl:162-192): n*n doubles column-major.
+ * For a factorised handle this is the packed L\U of lu!. */
+int hm_to_dense(const hm_handle* h, double* out, uint32_t flags);
+
+/* H*V and H'*V (src/harithm.jl:317-329, 243-260): Y = H*X (trans=0) or
+ * Y = H'*X (trans=1); X, Y are n x ncols column-major doubles.  The device
+ * kernel streams the stored factors once per call (single RHS) in the
+ * handle's storage precision and accumulates in FP64.  stream: a
+ * cudaStream_t or NULL for the handle's own stream. */
+int hm_matvec(hm_handle* h, const double* X, double* Y, int64_t ncols,
+              int32_t trans, uint32_t flags, void* stream);
+
+/* One single-RHS matvec on device pointers with CUDA events between its three
+ * launches; ms[0..2] = x staging, phase 1 (z = B'x per low-rank leaf), phase 2
+ * (y = sum A z + dense).  Profiling aid; no counterpart in the reference. */
+int hm_matvec_profile(hm_handle* h, const double* X, double* Y, int32_t trans,
+                      void* stream, float* ms);
+
+/* Exact FP64 rows of the kernel matrix times x: y[i] = sum_j K(c.X[rows[i]],
+ * c.X[j]) x[j] (+ shift*x[rows[i]]), the dense FullMat oracle for sampled rows. */
+int hm_exact_rows(hm_handle* h, const int64_t* rows, int64_t nrows,
+                  const double* x, double* y, uint32_t flags, void* stream);
+
+/* H + lambda*I (src/harithm.jl:457-473), in place on h; refused with
+ * HM_ERR_STATE on a factorised handle (src/harithm.jl:458-460). */
+int hm_add_identity(hm_handle* h, double lambda);
+
+/* u*H (src/harithm.jl:478-498), in place. */
+int hm_scale(hm_handle* h, double u);
+
+/* copy(H) (src/utils.jl:130-159) */
+int hm_copy(const hm_handle* h, hm_handle** out);
+
+/* lu!(H) (src/hlu.jl:465-515): factorise in place with pivoting inside each
+ * diagonal leaf.  HM_ERR_STATE if already factorised (src/hlu.jl:466-468). */
+int hm_lu(hm_handle* h);
+
+/* Row permutation P of a factorised handle (0-based; H[P,:] = L*U). */
+int hm_lu_perm(const hm_handle* h, int64_t* P);
+
+/* a\y (src/hlu.jl:553-562) with a factorised handle: X = H^{-1} B for ncols
+ * right-hand sides (n x ncols column-major). */
+int hm_solve(hm_handle* h, const double* B, double* X, int64_t ncols,
+             uint32_t flags, void* stream);
+
+/* Drop-in for the reference's native entry point
+ * int aca_wrapper(double*, double*, double*, int, int, double, int)
+ * (deps/src/ACA_FullyPivoted.cpp:218-236, called from src/hlu.jl:12-13):
+ * fully pivoted ACA of the column-major m x n host matrix AA; at most
+ * rank+1 columns are written to UU (m x .) and VV (n x .); returns the
+ * untruncated rank, or a negative status on error. */
+int aca_wrapper(double* AA, double* UU, double* VV, int m, int n,
+                double epsilon, int rank);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HMATRIX_B200_H */
