@@ -30,6 +30,7 @@ EXPORTED = [
     "hm_version", "hm_last_error", "hm_default_params", "hm_new", "hm_destroy", "hm_info",
     "hm_leaves", "hm_leaf_factors", "hm_to_dense", "hm_matvec", "hm_matvec_profile", "hm_exact_rows",
     "hm_add_identity", "hm_scale", "hm_copy", "hm_lu", "hm_lu_perm", "hm_solve", "aca_wrapper",
+    "aca_wrapper_noalloc",
 ]
 
 
@@ -93,6 +94,8 @@ def lib():
     L.hm_solve.argtypes = [vp, vp, vp, C.c_int64, C.c_uint32, vp]
     L.aca_wrapper.argtypes = [pd, pd, pd, C.c_int, C.c_int, C.c_double, C.c_int]
     L.aca_wrapper.restype = C.c_int
+    L.aca_wrapper_noalloc.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_double, C.c_int, vp]
+    L.aca_wrapper_noalloc.restype = C.c_int
     for name in EXPORTED:
         f = getattr(L, name)
         if f.restype is None:

@@ -188,6 +188,20 @@ int hm_solve(hm_handle* h, const double* B, double* X, int64_t ncols,
 int aca_wrapper(double* AA, double* UU, double* VV, int m, int n,
                 double epsilon, int rank);
 
+/* Allocation-free aca_wrapper for callers that cannot call cudaMalloc (their
+ * device memory belongs to another allocator's pool, or they cannot afford the
+ * synchronisation an allocation implies).  No counterpart in the reference.
+ * A (m x n), UU (m x min(m,n,rank+1)) and VV (n x min(m,n,rank+1)) are device
+ * pointers on the current device, column-major; the result equals
+ * aca_wrapper's and the untruncated rank is returned (negative status on
+ * error).  The residual lives in a fixed device array of 2^18 - 32 doubles
+ * shared by all calls: m*n + m + n must not exceed that (HM_ERR_ARG
+ * otherwise), calls that overlap on the GPU race, and the first call on a
+ * device (which looks the array up) should come before any stream capture.
+ * stream: a cudaStream_t or NULL for the legacy default stream. */
+int aca_wrapper_noalloc(const double* AA, double* UU, double* VV, int m, int n,
+                        double epsilon, int rank, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
