@@ -310,14 +310,43 @@ int hm_solve(hm_handle* h, const double* B, double* X, int64_t ncols, uint32_t f
   DeviceGuard g(h->device);
   cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
   const int64_t n = h->n;
-  if (flags & HM_FLAG_DEVICE_PTRS) return lu_solve_device(h, B, X, ncols, st);
+  const int trans = (flags & HM_FLAG_TRANS) ? 1 : 0;
+  if (flags & HM_FLAG_DEVICE_PTRS) return lu_solve_device(h, B, X, ncols, trans, st);
   IoBuf io{h};
   HM_TRY(io.get(sizeof(double) * 2 * n * std::max<int64_t>(ncols, 1)));
   HM_CUDA_TRY(cudaMemcpyAsync(io.ptr, B, sizeof(double) * n * ncols, cudaMemcpyHostToDevice, st));
-  HM_TRY(lu_solve_device(h, io.ptr, io.ptr + n * ncols, ncols, st));
+  HM_TRY(lu_solve_device(h, io.ptr, io.ptr + n * ncols, ncols, trans, st));
   HM_CUDA_TRY(cudaMemcpyAsync(X, io.ptr + n * ncols, sizeof(double) * n * ncols, cudaMemcpyDeviceToHost, st));
   HM_CUDA_TRY(cudaStreamSynchronize(st));
   return HM_OK;
+}
+
+int hm_solve_refined(hm_handle* h, const double* B, double* X, int64_t ncols, double tol, int32_t max_iter,
+                     uint32_t flags, void* stream, int32_t* iters, double* relres) {
+  if (!h || !B || !X || ncols < 0 || max_iter < 0) return fail(HM_ERR_ARG, "invalid argument");
+  if (!h->factorized) return fail(HM_ERR_STATE, "a has not been factorized");
+  DeviceGuard g(h->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  const int64_t n = h->n;
+  const int trans = (flags & HM_FLAG_TRANS) ? 1 : 0;
+  int it = 0;
+  double rr = 0.0;
+  int s;
+  if (flags & HM_FLAG_DEVICE_PTRS) {
+    s = lu_solve_refined(h, B, X, ncols, trans, tol, max_iter, st, &it, &rr);
+  } else {
+    double* d = nullptr;
+    HM_CUDA_TRY(cudaMallocAsync(&d, sizeof(double) * 2 * n * std::max<int64_t>(ncols, 1), st));
+    HM_CUDA_TRY(cudaMemcpyAsync(d, B, sizeof(double) * n * ncols, cudaMemcpyHostToDevice, st));
+    s = lu_solve_refined(h, d, d + n * ncols, ncols, trans, tol, max_iter, st, &it, &rr);
+    if (s == HM_OK)
+      HM_CUDA_TRY(cudaMemcpyAsync(X, d + n * ncols, sizeof(double) * n * ncols, cudaMemcpyDeviceToHost, st));
+    cudaFreeAsync(d, st);
+    HM_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  if (iters) *iters = it;
+  if (relres) *relres = rr;
+  return s;
 }
 
 int aca_wrapper(double* AA, double* UU, double* VV, int m, int n, double epsilon, int rank) {

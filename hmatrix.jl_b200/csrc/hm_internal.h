@@ -132,7 +132,7 @@ struct MvWin {
   uint32_t begin, end;     // P2Desc range
 };
 
-constexpr int MV_WROWS = 512;          // rows per phase-2 window (16 warps x 32)
+constexpr int MV_WROWS = 1024;         // rows per phase-2 window (8 warps x 32 lanes x 4 rows)
 
 struct MvPlan {
   P1Desc* d_p1 = nullptr;
@@ -194,9 +194,11 @@ namespace hm {
 inline int elem_bytes(int storage) { return storage == HM_F64 ? 8 : (storage == HM_F32 ? 4 : 2); }
 inline int dense_elem_bytes(int storage) { return storage == HM_F64 ? 8 : 4; }
 __host__ __device__ inline int64_t pad_to(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
-// padded column length: columns start on 16-byte boundaries
-__host__ __device__ inline int64_t col_pad(int64_t len, int ebytes) { return pad_to(len, 16 / ebytes); }
-__host__ __device__ inline int64_t col_pad_dev(int64_t len, int ebytes) { return pad_to(len, 16 / ebytes); }
+// padded column length: a multiple of 16 bytes and of 4 elements, so every
+// column starts on a 16-byte boundary and 4-row groups never leave a column
+__host__ __device__ inline int64_t col_pad_elems(int ebytes) { return 16 / ebytes > 4 ? 16 / ebytes : 4; }
+__host__ __device__ inline int64_t col_pad(int64_t len, int ebytes) { return pad_to(len, col_pad_elems(ebytes)); }
+__host__ __device__ inline int64_t col_pad_dev(int64_t len, int ebytes) { return pad_to(len, col_pad_elems(ebytes)); }
 
 template <typename T> __device__ __forceinline__ T to_store(double v) { return (T)v; }
 template <> __device__ __forceinline__ __nv_bfloat16 to_store<__nv_bfloat16>(double v) {
@@ -233,7 +235,9 @@ int aca_fp_host(const double* A, double* U, double* V, int m, int n, double eps,
 
 // LU (hm_lu.cu)
 int lu_factor(hm_handle* h);
-int lu_solve_device(hm_handle* h, const double* d_b, double* d_x, int64_t ncols, cudaStream_t st);
+int lu_solve_device(hm_handle* h, const double* d_b, double* d_x, int64_t ncols, int trans, cudaStream_t st);
+int lu_solve_refined(hm_handle* h, const double* d_b, double* d_x, int64_t ncols, int trans, double tol,
+                     int max_iter, cudaStream_t st, int* iters, double* relres);
 int lu_perm(const hm_handle* h, int64_t* P);
 int lu_to_dense(const hm_handle* h, double* d_out);
 void lu_free(hm_handle* h);

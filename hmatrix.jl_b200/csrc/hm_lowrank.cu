@@ -188,15 +188,7 @@ int aca2_write(hm_handle* h, const std::vector<int64_t>& rk_leaf) {
 // (rank < min(m,n) && |R|_F > eps && |R|_F > machine eps) || rank < min_rank.
 // status: 0 converged, 1 stopped at `cap` terms, 2 non-finite norm.
 // ===========================================================================
-struct AcaFpJob {
-  double* R; double* U; double* V;
-  int32_t m, n, cap, min_rank;
-  double eps;
-  int32_t* rank; int32_t* status;
-};
-
-__global__ void __launch_bounds__(512) aca_fp_kernel(const AcaFpJob* __restrict__ jobs) {
-  const AcaFpJob J = jobs[blockIdx.x];
+__device__ void aca_fp_body(const AcaFpJob& J) {
   __shared__ double red[32];
   __shared__ double s_a[32];
   __shared__ int64_t s_i[32];
@@ -212,9 +204,10 @@ __global__ void __launch_bounds__(512) aca_fp_kernel(const AcaFpJob* __restrict_
   double* ucol = nullptr;
   double* vcol = nullptr;
 
+  double eps = J.eps;
   for (;;) {
     // pass over R: update with the previous term, then arg-max and norm
-    double best = -1.0, bval = 0.0, ss = 0.0;
+    double best = -1.0, bval = 0.0, ss = 0.0, sa = 0.0;
     int64_t bidx = INT64_MAX;
     for (int64_t e = threadIdx.x; e < mn; e += blockDim.x) {
       double v = J.R[e];
@@ -224,8 +217,17 @@ __global__ void __launch_bounds__(512) aca_fp_kernel(const AcaFpJob* __restrict_
         J.R[e] = v;
       }
       ss = fma(v, v, ss);
+      sa += fabs(v);
       double a = fabs(v);
       if (a > best) { best = a; bidx = e; bval = v; }
+    }
+    if (J.rel_mode && !ucol) {
+      // compress() semantics (src/hlu.jl:163-167): an absolutely tiny block is
+      // rank-1 zeros; otherwise stop far below eps_trunc * s_1
+      const double sabs = block_sum(sa, red);
+      const double fro = sqrt(block_sum(ss, red));
+      if (sabs < 1e-5) { status = 3; break; }
+      eps = fmax(1e-3 * J.eps_trunc * fro / sqrt((double)min(m, n)), 64.0 * meps * fro);
     }
     warp_argmax(best, bidx, bval);
     __syncthreads();
@@ -241,7 +243,7 @@ __global__ void __launch_bounds__(512) aca_fp_kernel(const AcaFpJob* __restrict_
     const int64_t sel = s_sel;
     const double Max = s_max;
     if (isnan(Rnorm)) { status = 2; break; }
-    if (!((rank < maxr && Rnorm > J.eps && Rnorm > meps) || rank < J.min_rank)) break;
+    if (!((rank < maxr && Rnorm > eps && Rnorm > meps) || rank < J.min_rank)) break;
     if (rank >= J.cap) { status = 1; break; }
     const int sel_row = (int)(sel % m), sel_col = (int)(sel / m);
     ucol = J.U + (int64_t)rank * m;
@@ -258,6 +260,18 @@ __global__ void __launch_bounds__(512) aca_fp_kernel(const AcaFpJob* __restrict_
     ++rank;
   }
   if (threadIdx.x == 0) { *J.rank = rank; *J.status = status; }
+}
+
+__global__ void __launch_bounds__(512) aca_fp_kernel(const AcaFpJob* __restrict__ jobs) {
+  aca_fp_body(jobs[blockIdx.x]);
+}
+
+__global__ void __launch_bounds__(512) aca_fp_one_kernel(AcaFpJob J) { aca_fp_body(J); }
+
+int launch_aca_fp_one(const AcaFpJob& J, cudaStream_t st) {
+  aca_fp_one_kernel<<<1, 512, 0, st>>>(J);
+  HM_CUDA_TRY(cudaGetLastError());
+  return HM_OK;
 }
 
 // ===========================================================================
@@ -299,8 +313,12 @@ __device__ void cgs2_qr(double* X, int len, int ld, int r, double* Rm /* r x r, 
   }
 }
 
-__global__ void __launch_bounds__(256) core_recompress_kernel(const CoreJob* __restrict__ jobs, int rmax,
-                                                              double eps_trunc, int* __restrict__ flags) {
+__device__ void zero_cols(double* X, int len, int64_t ld, int c0, int c1) {
+  for (int64_t e = threadIdx.x; e < (int64_t)len * (c1 - c0); e += blockDim.x)
+    X[(e % len) + (int64_t)(c0 + e / len) * ld] = 0.0;
+}
+
+__device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, int* __restrict__ flags) {
   extern __shared__ double sm[];
   __shared__ double red[32];
   __shared__ double proj[RCORE_MAX];
@@ -308,14 +326,26 @@ __global__ void __launch_bounds__(256) core_recompress_kernel(const CoreJob* __r
   __shared__ int ord[RCORE_MAX];
   __shared__ int s_rot;
   __shared__ int s_k;
-  const CoreJob J = jobs[blockIdx.x];
-  const int r = J.r;
+  int r = J.r_dev ? *J.r_dev : J.r;
   double* b0 = sm;                       // R_A, later V (Jacobi right vectors)
   double* b1 = sm + rmax * rmax;         // R_B, later U-coefficients
   double* b2 = sm + 2 * rmax * rmax;     // W, later V-coefficients
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-
+  const int pre = J.pre_status ? *J.pre_status : 0;
+  if (pre != 0 || r > rmax) {
+    // pre == 3: compress() of an absolutely tiny block -> rank-1 zeros;
+    // otherwise the input could not be reduced (not converged / too large)
+    if (threadIdx.x == 0 && pre != 3) atomicOr(flags, pre == 2 ? 2 : 1);
+    zero_cols(J.outA, J.m, J.ldoa, 0, J.kcap);
+    zero_cols(J.outB, J.n, J.ldob, 0, J.kcap);
+    if (threadIdx.x == 0) *J.rank = (pre == 3) ? 1 : 0;
+    return;
+  }
   if (r == 0) {
+    if (J.zero_fill) {
+      zero_cols(J.outA, J.m, J.ldoa, 0, J.kcap);
+      zero_cols(J.outB, J.n, J.ldob, 0, J.kcap);
+    }
     if (threadIdx.x == 0) *J.rank = 0;
     return;
   }
@@ -334,8 +364,9 @@ __global__ void __launch_bounds__(256) core_recompress_kernel(const CoreJob* __r
   bool nonfinite = !isfinite(sabs);
   if (J.zero_test && sabs < 1e-5) {
     // compress(): an (absolutely) tiny core becomes rank-1 zeros (src/hlu.jl:163-167)
-    for (int i = threadIdx.x; i < J.m; i += blockDim.x) J.outA[i] = 0.0;
-    for (int j = threadIdx.x; j < J.n; j += blockDim.x) J.outB[j] = 0.0;
+    const int kz = J.zero_fill ? J.kcap : 1;
+    zero_cols(J.outA, J.m, J.ldoa, 0, kz);
+    zero_cols(J.outB, J.n, J.ldob, 0, kz);
     if (threadIdx.x == 0) *J.rank = 1;
     return;
   }
@@ -443,7 +474,34 @@ __global__ void __launch_bounds__(256) core_recompress_kernel(const CoreJob* __r
     for (int j = 0; j < r; ++j) s = fma(J.B[i + (int64_t)j * J.ldb], b2[j + c * r], s);
     J.outB[i + (int64_t)c * J.ldob] = s;
   }
+  if (J.zero_fill && k < J.kcap) {
+    zero_cols(J.outA, J.m, J.ldoa, k, J.kcap);
+    zero_cols(J.outB, J.n, J.ldob, k, J.kcap);
+  }
   if (threadIdx.x == 0) *J.rank = k;
+}
+
+__global__ void __launch_bounds__(256) core_recompress_kernel(const CoreJob* __restrict__ jobs, int rmax,
+                                                              double eps_trunc, int* __restrict__ flags) {
+  core_body(jobs[blockIdx.x], rmax, eps_trunc, flags);
+}
+
+__global__ void __launch_bounds__(256) core_recompress_one_kernel(CoreJob J, int rmax, double eps_trunc,
+                                                                  int* __restrict__ flags) {
+  core_body(J, rmax, eps_trunc, flags);
+}
+
+int launch_core_one(const CoreJob& J, double eps_trunc, int* d_flags, cudaStream_t st) {
+  static bool attr_set = false;
+  const size_t smem = (size_t)3 * RCORE_MAX * RCORE_MAX * sizeof(double);
+  if (!attr_set) {
+    HM_CUDA_TRY(cudaFuncSetAttribute(core_recompress_one_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    attr_set = true;
+  }
+  core_recompress_one_kernel<<<1, 256, smem, st>>>(J, RCORE_MAX, eps_trunc, d_flags);
+  HM_CUDA_TRY(cudaGetLastError());
+  return HM_OK;
 }
 
 int launch_core_recompress(const CoreJob* d_jobs, int njobs, int rmax, double eps_trunc, int* d_flags,
@@ -551,8 +609,10 @@ int svd_compress_candidates(hm_handle* h, const std::vector<int64_t>& r0, const 
       const double fro = sqrt(fro2[i]);
       double tau = 1e-3 * eps_trunc * fro / sqrt((double)std::min(m, n));
       tau = std::max(tau, 64.0 * 2.220446049250313e-16 * fro);
-      fj[i] = AcaFpJob{buf + offC[i], buf + offU[i], buf + offV[i], m, n, cap, 1, tau,
-                       d_rank + i, d_stat + i};
+      AcaFpJob J{};
+      J.R = buf + offC[i]; J.U = buf + offU[i]; J.V = buf + offV[i]; J.m = m; J.n = n; J.cap = cap;
+      J.min_rank = 1; J.eps = tau; J.rank = d_rank + i; J.status = d_stat + i;
+      fj[i] = J;
     }
     AcaFpJob* d_fj = nullptr;
     HM_CUDA_TRY(cudaMalloc(&d_fj, sizeof(AcaFpJob) * nb));
@@ -572,8 +632,11 @@ int svd_compress_candidates(hm_handle* h, const std::vector<int64_t>& r0, const 
       const int m = mm[b0 + i], n = nn[b0 + i];
       if (sabs[i] < 1e-5) { ranks[b0 + i] = 1; continue; }       // compress() zero test
       if (stt[i] == 1) { ranks[b0 + i] = 1 << 30; continue; }    // not low-rank within the core cap
-      cj.push_back(CoreJob{buf + offU[i], buf + offV[i], buf + offA[i], buf + offB[i], m, n, rr[i], m, n,
-                           m, n, cap, 0, d_rank + nb + (int32_t)cj.size()});
+      CoreJob J{};
+      J.A = buf + offU[i]; J.B = buf + offV[i]; J.outA = buf + offA[i]; J.outB = buf + offB[i];
+      J.m = m; J.n = n; J.r = rr[i]; J.lda = m; J.ldb = n; J.ldoa = m; J.ldob = n; J.kcap = cap;
+      J.zero_test = 0; J.rank = d_rank + nb + (int32_t)cj.size();
+      cj.push_back(J);
       cj_idx.push_back(i);
       rmax = std::max(rmax, (int)rr[i]);
     }
@@ -672,7 +735,9 @@ int aca_fp_host(const double* A, double* U, double* V, int m, int n, double eps,
   HM_CUDA_TRY(cudaMalloc(&dk, 8));
   HM_CUDA_TRY(cudaMalloc(&dj, sizeof(AcaFpJob)));
   HM_CUDA_TRY(cudaMemcpy(dR, A, 8ull * m * n, cudaMemcpyHostToDevice));
-  AcaFpJob j{dR, dU, dV, m, n, cap, 1, eps, dk, dk + 1};
+  AcaFpJob j{};
+  j.R = dR; j.U = dU; j.V = dV; j.m = m; j.n = n; j.cap = cap; j.min_rank = 1; j.eps = eps;
+  j.rank = dk; j.status = dk + 1;
   HM_CUDA_TRY(cudaMemcpy(dj, &j, sizeof(j), cudaMemcpyHostToDevice));
   aca_fp_kernel<<<1, 512>>>(dj);
   HM_CUDA_TRY(cudaGetLastError());

@@ -13,7 +13,7 @@
 namespace hm {
 
 constexpr int ACA_MAX_EXTENT = 2048;   // largest block side for device aca2
-constexpr int RCORE_MAX = 80;          // largest core of the QR+SVD recompression
+constexpr int RCORE_MAX = 96;          // largest core of the QR+SVD recompression
 constexpr int MV_KMAX = 255;           // largest rank a leaf may carry
 
 // ---------------------------------------------------------------------------
@@ -81,7 +81,24 @@ struct CoreJob {
   int32_t m, n, r, lda, ldb, ldoa, ldob, kcap;
   int32_t zero_test;       // apply compress()'s sum|W| < 1e-5 test to the core
   int32_t* rank;
+  const int32_t* r_dev;    // if set: the core size r is read on the device
+  const int32_t* pre_status;  // if set: status of the fully pivoted ACA that made A, B
+  int32_t zero_fill;       // zero the output columns [k, kcap)
 };
+
+// Fully pivoted ACA job (deps/src/ACA_FullyPivoted.cpp:9-151).  rel_mode: the
+// "svd"-compress mode -- status 3 for an absolutely tiny block (sum|R| < 1e-5)
+// and a stop tolerance derived on the device from |R|_F and eps_trunc.
+struct AcaFpJob {
+  double* R; double* U; double* V;
+  int32_t m, n, cap, min_rank;
+  double eps;
+  int32_t* rank; int32_t* status;
+  int32_t rel_mode;
+  double eps_trunc;
+};
+int launch_aca_fp_one(const AcaFpJob& J, cudaStream_t st);
+int launch_core_one(const CoreJob& J, double eps_trunc, int* d_flags, cudaStream_t st);
 // launch the batched recompression; status of rank overflow/nonfinite is
 // OR-ed into *d_flags (bit 0: rank > kcap, bit 1: non-finite).
 int launch_core_recompress(const CoreJob* d_jobs, int njobs, int rmax, double eps_trunc,

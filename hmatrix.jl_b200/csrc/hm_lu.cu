@@ -1,30 +1,1111 @@
-// H-LU and triangular H-solve (src/hlu.jl:227-562).
+// H-LU and triangular H-solve on the device (src/hlu.jl:227-562, with the
+// H-arithmetic of src/harithm.jl:4-420 that the Schur updates use).
+//
+// The host walks the same recursion as the reference -- lu!, permute_hmat!,
+// hmat_trisolve!, mat_full_solve, hmat_sub_mul! = hmul + hmat_add!, and the
+// recompressions of rkmat_add!, rkmat_hmat_add and compress -- and issues one
+// stream-ordered kernel per primitive.  Nothing is read back during the
+// factorisation: ranks live on the device, every low-rank buffer has a fixed
+// capacity `cap` and keeps its columns beyond the current rank at zero, so
+// every product can run with static shapes.  Temporaries are stream-ordered
+// allocations (cudaMallocAsync / cudaFreeAsync).  Pivoting is partial and
+// stays inside each diagonal leaf, exactly as in the reference; the global
+// permutation is one device array P with H[P,:] = L U.
 #include "hm_internal.h"
 #include "hm_lowrank.cuh"
 
+#include <memory>
+#include <stdexcept>
+
 namespace hm {
 
-struct LuState {
-  int dummy = 0;
+// ---------------------------------------------------------------------------
+// strided views: element (i,j) at p[i*rs + j*cs]
+// ---------------------------------------------------------------------------
+struct View {
+  double* p;
+  int64_t rs, cs;
+  int rows, cols;
+};
+static inline View vsub(View v, int r0, int c0, int nr, int nc) {
+  return View{v.p + (int64_t)r0 * v.rs + (int64_t)c0 * v.cs, v.rs, v.cs, nr, nc};
+}
+static inline View vtr(View v) { return View{v.p, v.cs, v.rs, v.cols, v.rows}; }
+static inline View vrev(View v) {
+  return View{v.p + (int64_t)(v.rows - 1) * v.rs + (int64_t)(v.cols - 1) * v.cs, -v.rs, -v.cs, v.rows, v.cols};
+}
+
+struct LuError : std::runtime_error {
+  int code;
+  LuError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
+#define LU_LAUNCH_CHECK()                                                                   \
+  do {                                                                                      \
+    cudaError_t _e = cudaGetLastError();                                                    \
+    if (_e != cudaSuccess) throw LuError(HM_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(_e)); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+// C = alpha * A * B + beta * C   (A: m x k, B: k x n), FP64, 32x32 tiles
+__global__ void __launch_bounds__(256) lu_gemm_kernel(View A, View B, View C, double alpha, double beta) {
+  __shared__ double As[32][33];
+  __shared__ double Bs[32][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+  const int m = C.rows, n = C.cols, kk = A.cols;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int k0 = 0; k0 < kk; k0 += 32) {
+    for (int e = threadIdx.x; e < 1024; e += 256) {
+      const int r = e & 31, c = e >> 5;
+      As[r][c] = (i0 + r < m && k0 + c < kk) ? A.p[(int64_t)(i0 + r) * A.rs + (int64_t)(k0 + c) * A.cs] : 0.0;
+      Bs[r][c] = (k0 + r < kk && j0 + c < n) ? B.p[(int64_t)(k0 + r) * B.rs + (int64_t)(j0 + c) * B.cs] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int q = 0; q < 32; ++q) {
+      const double a = As[tx][q];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) acc[u] = fma(a, Bs[q][ty + 8 * u], acc[u]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int i = i0 + tx, j = j0 + ty + 8 * u;
+    if (i < m && j < n) {
+      double* c = C.p + (int64_t)i * C.rs + (int64_t)j * C.cs;
+      *c = (beta == 0.0) ? alpha * acc[u] : fma(alpha, acc[u], beta * *c);
+    }
+  }
+}
+
+// Y = alpha * X + beta * Y (beta == 0: Y is not read)
+__global__ void lu_axpby_kernel(View Y, View X, double alpha, double beta) {
+  const int64_t tot = (int64_t)Y.rows * Y.cols;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % Y.rows), j = (int)(e / Y.rows);
+    double* y = Y.p + (int64_t)i * Y.rs + (int64_t)j * Y.cs;
+    const double x = X.p ? X.p[(int64_t)i * X.rs + (int64_t)j * X.cs] : 0.0;
+    *y = (beta == 0.0) ? alpha * x : fma(alpha, x, beta * *y);
+  }
+}
+
+// X <- L^{-1} X, L (m x m) lower triangular (strided: upper/transposed/reversed
+// triangles are views of this one), one thread per column of X.
+__global__ void __launch_bounds__(128) lu_trsm_lower_kernel(View L, View X, int unit) {
+  extern __shared__ double Ls[];
+  const int m = L.rows;
+  const bool sm = m <= 96;
+  if (sm) {
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+      const int i = e % m, j = e / m;
+      Ls[e] = (j <= i) ? L.p[(int64_t)i * L.rs + (int64_t)j * L.cs] : 0.0;
+    }
+    __syncthreads();
+  }
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= X.cols) return;
+  double* x = X.p + (int64_t)j * X.cs;
+  for (int i = 0; i < m; ++i) {
+    double s = x[(int64_t)i * X.rs];
+    for (int l = 0; l < i; ++l) {
+      const double lil = sm ? Ls[i + l * m] : L.p[(int64_t)i * L.rs + (int64_t)l * L.cs];
+      s = fma(-lil, x[(int64_t)l * X.rs], s);
+    }
+    if (!unit) s = s / (sm ? Ls[i + i * m] : L.p[(int64_t)i * L.rs + (int64_t)i * L.cs]);
+    x[(int64_t)i * X.rs] = s;
+  }
+}
+
+// getrf with partial pivoting of an m x m dense leaf (LAPACK semantics: first
+// maximum as pivot, full-row swaps); P[goff+i] = goff + p[i] with C[p] = L U.
+__global__ void __launch_bounds__(256) lu_getrf_kernel(View C, int64_t* __restrict__ P, int64_t goff,
+                                                       int* __restrict__ flags) {
+  extern __shared__ double S[];
+  const int m = C.rows;
+  int* perm = reinterpret_cast<int*>(S + (int64_t)m * m);
+  __shared__ int s_piv;
+  for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+    const int i = e % m, j = e / m;
+    S[e] = C.p[(int64_t)i * C.rs + (int64_t)j * C.cs];
+  }
+  for (int i = threadIdx.x; i < m; i += blockDim.x) perm[i] = i;
+  __syncthreads();
+  for (int j = 0; j < m; ++j) {
+    if (threadIdx.x < 32) {
+      double best = -1.0, bv = 0.0;
+      int64_t bi = INT64_MAX;
+      for (int i = j + threadIdx.x; i < m; i += 32) {
+        const double a = fabs(S[i + j * m]);
+        if (a > best) { best = a; bi = i; bv = S[i + j * m]; }
+      }
+      warp_argmax(best, bi, bv);
+      if (threadIdx.x == 0) {
+        s_piv = (int)bi;
+        if (!(bv != 0.0)) atomicOr(flags, 4);        // exactly zero (or NaN) pivot
+      }
+    }
+    __syncthreads();
+    const int p = s_piv;
+    if (p != j) {
+      for (int c = threadIdx.x; c < m; c += blockDim.x) {
+        const double t = S[j + c * m];
+        S[j + c * m] = S[p + c * m];
+        S[p + c * m] = t;
+      }
+      if (threadIdx.x == 0) { const int t = perm[j]; perm[j] = perm[p]; perm[p] = t; }
+    }
+    __syncthreads();
+    const double piv = S[j + j * m];
+    if (piv != 0.0) {
+      for (int i = j + 1 + threadIdx.x; i < m; i += blockDim.x) S[i + j * m] /= piv;
+    }
+    __syncthreads();
+    const int rem = m - j - 1;
+    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
+      const int i = j + 1 + e % rem, c = j + 1 + e / rem;
+      S[i + c * m] = fma(-S[i + j * m], S[j + c * m], S[i + c * m]);
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+    const int i = e % m, j = e / m;
+    C.p[(int64_t)i * C.rs + (int64_t)j * C.cs] = S[e];
+  }
+  for (int i = threadIdx.x; i < m; i += blockDim.x) P[goff + i] = goff + perm[i];
+}
+
+// X <- X[p, :] with p[i] = P[goff+i] - goff, columns in chunks through smem
+__global__ void lu_laswp_kernel(View X, const int64_t* __restrict__ P, int64_t goff, int chunk) {
+  extern __shared__ double T[];
+  const int m = X.rows;
+  const int c0 = blockIdx.x * chunk;
+  const int nc = min(chunk, X.cols - c0);
+  for (int e = threadIdx.x; e < m * nc; e += blockDim.x) {
+    const int i = e % m, c = e / m;
+    const int64_t src = P[goff + i] - goff;
+    T[e] = X.p[src * X.rs + (int64_t)(c0 + c) * X.cs];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < m * nc; e += blockDim.x) {
+    const int i = e % m, c = e / m;
+    X.p[(int64_t)i * X.rs + (int64_t)(c0 + c) * X.cs] = T[e];
+  }
+}
+
+// y[i, c] = b[P[i], c]
+__global__ void lu_gather_rows_kernel(View Y, View Bv, const int64_t* __restrict__ P) {
+  const int64_t tot = (int64_t)Y.rows * Y.cols;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % Y.rows), c = (int)(e / Y.rows);
+    Y.p[(int64_t)i * Y.rs + (int64_t)c * Y.cs] = Bv.p[P[i] * Bv.rs + (int64_t)c * Bv.cs];
+  }
+}
+
+// pieces of a low-rank sum, gathered into contiguous [s_i A_i] / [B_i] with
+// their first k_i columns, rows placed at offsets ro_i / co_i (zeros
+// elsewhere) -- the concatenations of rkmat_add! and rkmat_hmat_add
+struct Piece {
+  const double* A; int64_t lda;
+  const double* B; int64_t ldb;
+  const int32_t* k;
+  int m, n, ro, co;
+  double s;
+};
+constexpr int MAX_PIECES = 4;
+struct GatherArgs {
+  Piece pc[MAX_PIECES];
+  int np;
+  double* SA; double* SB;     // M x rmax, N x rmax
+  int M, N, rmax;
+  int32_t* r_out;
+  int* flags;
+};
+__global__ void __launch_bounds__(256) lu_gather_pieces_kernel(GatherArgs g) {
+  __shared__ int pre[MAX_PIECES + 1];
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int q = 0; q < g.np; ++q) { pre[q] = t; t += *g.pc[q].k; }
+    pre[g.np] = t;
+    if (t > g.rmax) atomicOr(g.flags, 1);
+    *g.r_out = t;
+  }
+  __syncthreads();
+  const int r = min(pre[g.np], g.rmax);
+  for (int64_t e = threadIdx.x; e < (int64_t)g.M * r; e += blockDim.x) {
+    const int i = (int)(e % g.M), c = (int)(e / g.M);
+    int q = 0;
+    while (q + 1 < g.np && pre[q + 1] <= c) ++q;
+    const Piece& P = g.pc[q];
+    const int cc = c - pre[q];
+    const int ii = i - P.ro;
+    g.SA[e] = (ii >= 0 && ii < P.m) ? P.s * P.A[ii + (int64_t)cc * P.lda] : 0.0;
+  }
+  for (int64_t e = threadIdx.x; e < (int64_t)g.N * r; e += blockDim.x) {
+    const int j = (int)(e % g.N), c = (int)(e / g.N);
+    int q = 0;
+    while (q + 1 < g.np && pre[q + 1] <= c) ++q;
+    const Piece& P = g.pc[q];
+    const int cc = c - pre[q];
+    const int jj = j - P.co;
+    g.SB[e] = (jj >= 0 && jj < P.n) ? P.B[jj + (int64_t)cc * P.ldb] : 0.0;
+  }
+}
+
+__global__ void lu_copy_int_kernel(int32_t* dst, const int32_t* src) { *dst = *src; }
+__global__ void lu_set_int_kernel(int32_t* dst, int v) { *dst = v; }
+
+template <typename T>
+__global__ void lu_load_kernel(const T* __restrict__ src, int64_t ld_src, int rows, int cols, double* __restrict__ dst,
+                               int64_t ld_dst, int dst_cols) {
+  const int64_t tot = (int64_t)rows * dst_cols;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % rows), c = (int)(e / rows);
+    dst[i + (int64_t)c * ld_dst] = c < cols ? from_store<T>(src[i + (int64_t)c * ld_src]) : 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host-side block tree of the factorisation and of the temporaries
+// ---------------------------------------------------------------------------
+struct Blk;
+using BP = std::shared_ptr<Blk>;
+
+struct Ctx {
+  cudaStream_t st;
+  int cap;
+  int64_t* P;          // device permutation
+  int* flags;          // device error bits: 1 rank overflow, 2 non-finite, 4 singular
+  double eps_trunc;
+  const hm_handle* h;
+};
+
+struct Blk {
+  int8_t type = T_H;
+  int m = 0, n = 0;
+  int32_t s = -1, t = -1;             // clusters (for the isleaf tests of hmul)
+  int64_t row0 = 0;                   // global first row (persistent blocks)
+  double* C = nullptr;                // dense, column-major, ld = ldc
+  int64_t ldc = 0;
+  double* A = nullptr;                // low-rank: A (m x cap), B (n x cap)
+  double* B = nullptr;
+  int64_t lda = 0, ldb = 0;
+  int32_t* k = nullptr;
+  int cap = 0;
+  BP ch[4];
+  std::vector<void*> own;
+  cudaStream_t st = nullptr;
+  ~Blk() {
+    for (void* p : own) cudaFreeAsync(p, st);
+  }
+  View Cv() const { return View{C, 1, ldc, m, n}; }
+  View Av() const { return View{A, 1, lda, m, cap}; }
+  View Bv() const { return View{B, 1, ldb, n, cap}; }
+};
+
+static void* dmalloc(Ctx& c, Blk& b, size_t bytes) {
+  void* p = nullptr;
+  cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(bytes, 8), c.st);
+  if (e != cudaSuccess) throw LuError(HM_ERR_OOM, std::string("H-LU temporary: ") + cudaGetErrorString(e));
+  b.own.push_back(p);
+  return p;
+}
+
+static BP new_dense(Ctx& c, int m, int n, int32_t s, int32_t t) {
+  BP b = std::make_shared<Blk>();
+  b->st = c.st;
+  b->type = T_DENSE; b->m = m; b->n = n; b->s = s; b->t = t;
+  b->C = (double*)dmalloc(c, *b, sizeof(double) * (size_t)m * n);
+  b->ldc = std::max(m, 1);
+  return b;
+}
+
+static BP new_rk(Ctx& c, int m, int n, int32_t s, int32_t t, bool alloc_a = true, bool alloc_b = true) {
+  BP b = std::make_shared<Blk>();
+  b->st = c.st;
+  b->type = T_RK; b->m = m; b->n = n; b->s = s; b->t = t; b->cap = c.cap;
+  if (alloc_a) { b->A = (double*)dmalloc(c, *b, sizeof(double) * (size_t)m * c.cap); b->lda = std::max(m, 1); }
+  if (alloc_b) { b->B = (double*)dmalloc(c, *b, sizeof(double) * (size_t)n * c.cap); b->ldb = std::max(n, 1); }
+  b->k = (int32_t*)dmalloc(c, *b, sizeof(int32_t));
+  return b;
+}
+
+static bool is_leaf_cluster(const Ctx& c, int32_t cl) { return cl >= 0 && c.h->cl_left[cl] < 0; }
+
+// ---- primitive launches --------------------------------------------------
+static void gemm(Ctx& c, View C, View A, View B, double alpha, double beta) {
+  if (C.rows == 0 || C.cols == 0) return;
+  if (A.cols == 0) {
+    if (beta != 1.0) {
+      lu_axpby_kernel<<<64, 256, 0, c.st>>>(C, View{nullptr, 0, 0, C.rows, C.cols}, 0.0, beta);
+      LU_LAUNCH_CHECK();
+    }
+    return;
+  }
+  dim3 g((C.cols + 31) / 32, (C.rows + 31) / 32);
+  lu_gemm_kernel<<<g, 256, 0, c.st>>>(A, B, C, alpha, beta);
+  LU_LAUNCH_CHECK();
+}
+
+static void axpby(Ctx& c, View Y, View X, double alpha, double beta) {
+  const int64_t tot = (int64_t)Y.rows * Y.cols;
+  if (tot == 0) return;
+  unsigned g = (unsigned)std::min<int64_t>((tot + 255) / 256, 1024);
+  lu_axpby_kernel<<<g, 256, 0, c.st>>>(Y, X, alpha, beta);
+  LU_LAUNCH_CHECK();
+}
+
+static void trsm_lower(Ctx& c, View L, View X, bool unit) {
+  if (X.cols == 0 || L.rows == 0) return;
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(lu_trsm_lower_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             96 * 96 * (int)sizeof(double)) != cudaSuccess)
+      throw LuError(HM_ERR_CUDA, "trsm smem attribute");
+    attr = true;
+  }
+  const size_t smem = L.rows <= 96 ? sizeof(double) * (size_t)L.rows * L.rows : 0;
+  lu_trsm_lower_kernel<<<(X.cols + 127) / 128, 128, smem, c.st>>>(L, X, unit ? 1 : 0);
+  LU_LAUNCH_CHECK();
+}
+
+static void getrf(Ctx& c, View C, int64_t goff) {
+  const int m = C.rows;
+  if (m != C.cols) throw LuError(HM_ERR_UNSUPPORTED, "non-square diagonal leaf");
+  const size_t smem = sizeof(double) * (size_t)m * m + sizeof(int) * m;
+  if (smem > 200 * 1024) throw LuError(HM_ERR_UNSUPPORTED, "diagonal leaf above 150 rows (MinBlock too large)");
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(lu_getrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+      throw LuError(HM_ERR_CUDA, "getrf smem attribute");
+    attr = true;
+  }
+  lu_getrf_kernel<<<1, 256, smem, c.st>>>(C, c.P, goff, c.flags);
+  LU_LAUNCH_CHECK();
+}
+
+static void laswp(Ctx& c, View X, int64_t goff) {
+  if (X.rows == 0 || X.cols == 0) return;
+  int chunk = (int)std::max<int64_t>(1, std::min<int64_t>(X.cols, (48 * 1024 / 8) / X.rows));
+  const size_t smem = sizeof(double) * (size_t)X.rows * chunk;
+  lu_laswp_kernel<<<(X.cols + chunk - 1) / chunk, 256, smem, c.st>>>(X, c.P, goff, chunk);
+  LU_LAUNCH_CHECK();
+}
+
+static void copy_int(Ctx& c, int32_t* dst, const int32_t* src) {
+  lu_copy_int_kernel<<<1, 1, 0, c.st>>>(dst, src);
+  LU_LAUNCH_CHECK();
+}
+
+// ---- recompression --------------------------------------------------------
+// target (low-rank) = truncated sum of pieces: QR of both concatenations and
+// compress() of the core (src/harithm.jl:374-396, 49-56, src/hlu.jl:159-190)
+static void recompress(Ctx& c, Blk& target, const std::vector<Piece>& pcs) {
+  if (pcs.size() > (size_t)MAX_PIECES) throw LuError(HM_ERR_UNSUPPORTED, "too many pieces");
+  Blk tmp;
+  tmp.st = c.st;
+  const int M = target.m, N = target.n;
+  double* SA = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)M * RCORE_MAX);
+  double* SB = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)N * RCORE_MAX);
+  int32_t* r = (int32_t*)dmalloc(c, tmp, sizeof(int32_t));
+  GatherArgs g{};
+  for (size_t q = 0; q < pcs.size(); ++q) g.pc[q] = pcs[q];
+  g.np = (int)pcs.size();
+  g.SA = SA; g.SB = SB; g.M = M; g.N = N; g.rmax = RCORE_MAX; g.r_out = r; g.flags = c.flags;
+  lu_gather_pieces_kernel<<<1, 256, 0, c.st>>>(g);
+  LU_LAUNCH_CHECK();
+  CoreJob J{};
+  J.A = SA; J.B = SB; J.outA = target.A; J.outB = target.B;
+  J.m = M; J.n = N; J.r = 0; J.lda = std::max(M, 1); J.ldb = std::max(N, 1);
+  J.ldoa = (int32_t)target.lda; J.ldob = (int32_t)target.ldb; J.kcap = target.cap;
+  J.zero_test = 1; J.rank = target.k; J.r_dev = r; J.pre_status = nullptr; J.zero_fill = 1;
+  int s = launch_core_one(J, c.eps_trunc, c.flags, c.st);
+  if (s != HM_OK) throw LuError(s, "recompression launch");
+}
+
+// target (low-rank) = compress(D) for a dense D (src/hlu.jl:159-190): fully
+// pivoted ACA far below eps_trunc * s_1, then the exact SVD of its core
+static void compress_dense_into(Ctx& c, Blk& target, View D) {
+  Blk tmp;
+  tmp.st = c.st;
+  const int m = D.rows, n = D.cols;
+  double* R = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)m * n);
+  double* U = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)m * RCORE_MAX);
+  double* V = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)n * RCORE_MAX);
+  int32_t* rk = (int32_t*)dmalloc(c, tmp, sizeof(int32_t) * 2);
+  axpby(c, View{R, 1, std::max(m, 1), m, n}, D, 1.0, 0.0);
+  AcaFpJob J{};
+  J.R = R; J.U = U; J.V = V; J.m = m; J.n = n; J.cap = RCORE_MAX; J.min_rank = 1; J.eps = 0.0;
+  J.rank = rk; J.status = rk + 1; J.rel_mode = 1; J.eps_trunc = c.eps_trunc;
+  int s = launch_aca_fp_one(J, c.st);
+  if (s != HM_OK) throw LuError(s, "compress launch");
+  CoreJob K{};
+  K.A = U; K.B = V; K.outA = target.A; K.outB = target.B; K.m = m; K.n = n; K.r = 0;
+  K.lda = std::max(m, 1); K.ldb = std::max(n, 1); K.ldoa = (int32_t)target.lda; K.ldob = (int32_t)target.ldb;
+  K.kcap = target.cap; K.zero_test = 0; K.rank = target.k; K.r_dev = rk; K.pre_status = rk + 1; K.zero_fill = 1;
+  s = launch_core_one(K, c.eps_trunc, c.flags, c.st);
+  if (s != HM_OK) throw LuError(s, "compress core launch");
+}
+
+// ---- H-matrix products with dense blocks ----------------------------------
+// Y += s H X   (hmat_matvec! with a matrix, src/harithm.jl:340-354)
+static void hmm(Ctx& c, View Y, double s, const Blk& H, View X) {
+  if (H.type == T_DENSE) {
+    gemm(c, Y, H.Cv(), X, s, 1.0);
+  } else if (H.type == T_RK) {
+    Blk tmp;
+    tmp.st = c.st;
+    double* T = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)H.cap * X.cols);
+    View Tv{T, 1, H.cap, H.cap, X.cols};
+    gemm(c, Tv, vtr(H.Bv()), X, 1.0, 0.0);
+    gemm(c, Y, H.Av(), Tv, s, 1.0);
+  } else {
+    const int m = H.ch[0]->m, n = H.ch[0]->n;
+    hmm(c, vsub(Y, 0, 0, m, Y.cols), s, *H.ch[0], vsub(X, 0, 0, n, X.cols));
+    hmm(c, vsub(Y, 0, 0, m, Y.cols), s, *H.ch[1], vsub(X, n, 0, H.n - n, X.cols));
+    hmm(c, vsub(Y, m, 0, H.m - m, Y.cols), s, *H.ch[2], vsub(X, 0, 0, n, X.cols));
+    hmm(c, vsub(Y, m, 0, H.m - m, Y.cols), s, *H.ch[3], vsub(X, n, 0, H.n - n, X.cols));
+  }
+}
+
+// Y += s H' X   (transpose_hmat_mat_mul, src/harithm.jl:243-260)
+static void hmm_t(Ctx& c, View Y, double s, const Blk& H, View X) {
+  if (H.type == T_DENSE) {
+    gemm(c, Y, vtr(H.Cv()), X, s, 1.0);
+  } else if (H.type == T_RK) {
+    Blk tmp;
+    tmp.st = c.st;
+    double* T = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)H.cap * X.cols);
+    View Tv{T, 1, H.cap, H.cap, X.cols};
+    gemm(c, Tv, vtr(H.Av()), X, 1.0, 0.0);
+    gemm(c, Y, H.Bv(), Tv, s, 1.0);
+  } else {
+    const int m = H.ch[0]->m, n = H.ch[0]->n;
+    hmm_t(c, vsub(Y, 0, 0, n, Y.cols), s, *H.ch[0], vsub(X, 0, 0, m, X.cols));
+    hmm_t(c, vsub(Y, 0, 0, n, Y.cols), s, *H.ch[2], vsub(X, m, 0, H.m - m, X.cols));
+    hmm_t(c, vsub(Y, n, 0, H.n - n, Y.cols), s, *H.ch[1], vsub(X, 0, 0, m, X.cols));
+    hmm_t(c, vsub(Y, n, 0, H.n - n, Y.cols), s, *H.ch[3], vsub(X, m, 0, H.m - m, X.cols));
+  }
+}
+
+// Y += s X H   (v*H of src/harithm.jl:331-371 for a matrix v)
+static void xh(Ctx& c, View Y, double s, View X, const Blk& H) {
+  hmm_t(c, vtr(Y), s, H, vtr(X));
+}
+
+// dense copy of H (to_fmat, src/utils.jl:162-192)
+static void densify_into(Ctx& c, View D, const Blk& H) {
+  if (H.type == T_DENSE) {
+    axpby(c, D, H.Cv(), 1.0, 0.0);
+  } else if (H.type == T_RK) {
+    gemm(c, D, H.Av(), vtr(H.Bv()), 1.0, 0.0);
+  } else {
+    const int m = H.ch[0]->m, n = H.ch[0]->n;
+    densify_into(c, vsub(D, 0, 0, m, n), *H.ch[0]);
+    densify_into(c, vsub(D, 0, n, m, H.n - n), *H.ch[1]);
+    densify_into(c, vsub(D, m, 0, H.m - m, n), *H.ch[2]);
+    densify_into(c, vsub(D, m, n, H.m - m, H.n - n), *H.ch[3]);
+  }
+}
+
+static BP dense_of(Ctx& c, const Blk& H) {
+  BP d = new_dense(c, H.m, H.n, H.s, H.t);
+  densify_into(c, d->Cv(), H);
+  return d;
+}
+
+static BP copy_blk(Ctx& c, const Blk& a) {
+  if (a.type == T_DENSE) {
+    BP d = new_dense(c, a.m, a.n, a.s, a.t);
+    d->row0 = a.row0;
+    axpby(c, d->Cv(), a.Cv(), 1.0, 0.0);
+    return d;
+  }
+  if (a.type == T_RK) {
+    BP r = new_rk(c, a.m, a.n, a.s, a.t);
+    r->row0 = a.row0;
+    axpby(c, r->Av(), a.Av(), 1.0, 0.0);
+    axpby(c, r->Bv(), a.Bv(), 1.0, 0.0);
+    copy_int(c, r->k, a.k);
+    return r;
+  }
+  BP h = std::make_shared<Blk>();
+  h->st = c.st;
+  h->type = T_H; h->m = a.m; h->n = a.n; h->s = a.s; h->t = a.t; h->row0 = a.row0;
+  for (int q = 0; q < 4; ++q) h->ch[q] = copy_blk(c, *a.ch[q]);
+  return h;
+}
+
+// ---- H-add (src/harithm.jl:4-151, 374-420) ---------------------------------
+static void hmat_full_add(Ctx& c, Blk& a, View D, double s);
+static void hmat_add(Ctx& c, Blk& a, const Blk& b, double s);
+
+static void hmat_full_add(Ctx& c, Blk& a, View D, double s) {
+  if (a.type == T_DENSE) {
+    axpby(c, a.Cv(), D, s, 1.0);
+  } else if (a.type == T_RK) {
+    // C = A B' + s b; a.A, a.B = compress(C)   (src/harithm.jl:12-15)
+    Blk tmp;
+    tmp.st = c.st;
+    double* T = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)a.m * a.n);
+    View Tv{T, 1, std::max(a.m, 1), a.m, a.n};
+    axpby(c, Tv, D, s, 0.0);
+    gemm(c, Tv, a.Av(), vtr(a.Bv()), 1.0, 1.0);
+    compress_dense_into(c, a, Tv);
+  } else {
+    const int m = a.ch[0]->m, n = a.ch[0]->n;
+    hmat_full_add(c, *a.ch[0], vsub(D, 0, 0, m, n), s);
+    hmat_full_add(c, *a.ch[1], vsub(D, 0, n, m, a.n - n), s);
+    hmat_full_add(c, *a.ch[2], vsub(D, m, 0, a.m - m, n), s);
+    hmat_full_add(c, *a.ch[3], vsub(D, m, n, a.m - m, a.n - n), s);
+  }
+}
+
+// A B' + s H as a new low-rank block (src/harithm.jl:58-91)
+static BP rkmat_hmat_add(Ctx& c, View A, View B, const int32_t* k, double s, const Blk& H) {
+  BP out = new_rk(c, A.rows, B.rows, H.s, H.t);
+  if (H.type == T_DENSE) {
+    Blk tmp;
+    tmp.st = c.st;
+    double* T = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)H.m * H.n);
+    View Tv{T, 1, std::max(H.m, 1), H.m, H.n};
+    axpby(c, Tv, H.Cv(), s, 0.0);
+    gemm(c, Tv, A, vtr(B), 1.0, 1.0);
+    compress_dense_into(c, *out, Tv);
+  } else if (H.type == T_RK) {
+    std::vector<Piece> pcs = {
+        Piece{A.p, A.cs, B.p, B.cs, k, A.rows, B.rows, 0, 0, 1.0},
+        Piece{H.A, H.lda, H.B, H.ldb, H.k, H.m, H.n, 0, 0, s}};
+    recompress(c, *out, pcs);
+  } else {
+    const int m = H.ch[0]->m, n = H.ch[0]->n;
+    BP r11 = rkmat_hmat_add(c, vsub(A, 0, 0, m, A.cols), vsub(B, 0, 0, n, B.cols), k, s, *H.ch[0]);
+    BP r12 = rkmat_hmat_add(c, vsub(A, 0, 0, m, A.cols), vsub(B, n, 0, H.n - n, B.cols), k, s, *H.ch[1]);
+    BP r21 = rkmat_hmat_add(c, vsub(A, m, 0, H.m - m, A.cols), vsub(B, 0, 0, n, B.cols), k, s, *H.ch[2]);
+    BP r22 = rkmat_hmat_add(c, vsub(A, m, 0, H.m - m, A.cols), vsub(B, n, 0, H.n - n, B.cols), k, s, *H.ch[3]);
+    // A0 = [A11 A12 0 0; 0 0 A21 A22], B0 = [B11 0 B21 0; 0 B12 0 B22]  (src/harithm.jl:82-86)
+    std::vector<Piece> pcs = {
+        Piece{r11->A, r11->lda, r11->B, r11->ldb, r11->k, m, n, 0, 0, 1.0},
+        Piece{r12->A, r12->lda, r12->B, r12->ldb, r12->k, m, H.n - n, 0, n, 1.0},
+        Piece{r21->A, r21->lda, r21->B, r21->ldb, r21->k, H.m - m, n, m, 0, 1.0},
+        Piece{r22->A, r22->lda, r22->B, r22->ldb, r22->k, H.m - m, H.n - n, m, n, 1.0}};
+    recompress(c, *out, pcs);
+  }
+  return out;
+}
+
+static void hmat_add(Ctx& c, Blk& a, const Blk& b, double s) {
+  if (b.type == T_DENSE) {
+    hmat_full_add(c, a, b.Cv(), s);
+  } else if (a.type == T_DENSE && b.type == T_RK) {
+    gemm(c, a.Cv(), b.Av(), vtr(b.Bv()), s, 1.0);
+  } else if (a.type == T_DENSE && b.type == T_H) {
+    // a.C += s * (a.C + dense(b))  as written in src/harithm.jl:112; not
+    // reached from lu! (a dense target has a leaf cluster, so b is never H)
+    BP d = dense_of(c, b);
+    axpby(c, d->Cv(), a.Cv(), 1.0, 1.0);
+    axpby(c, a.Cv(), d->Cv(), s, 1.0);
+  } else if (a.type == T_RK && b.type == T_RK) {
+    std::vector<Piece> pcs = {
+        Piece{a.A, a.lda, a.B, a.ldb, a.k, a.m, a.n, 0, 0, 1.0},
+        Piece{b.A, b.lda, b.B, b.ldb, b.k, b.m, b.n, 0, 0, s}};
+    recompress(c, a, pcs);
+  } else if (a.type == T_RK && b.type == T_H) {
+    BP r = rkmat_hmat_add(c, a.Av(), a.Bv(), a.k, s, b);
+    axpby(c, a.Av(), r->Av(), 1.0, 0.0);
+    axpby(c, a.Bv(), r->Bv(), 1.0, 0.0);
+    copy_int(c, a.k, r->k);
+  } else if (a.type == T_H && b.type == T_RK) {
+    const int m = a.ch[0]->m, n = a.ch[0]->n;
+    auto part = [&](int r0, int mr, int c0, int nc) {
+      Blk v;
+      v.st = c.st;
+      v.type = T_RK; v.m = mr; v.n = nc; v.cap = b.cap; v.k = b.k;
+      v.A = b.A + r0; v.lda = b.lda; v.B = b.B + c0; v.ldb = b.ldb;
+      return v;
+    };
+    Blk c11 = part(0, m, 0, n), c21 = part(m, a.m - m, 0, n);
+    Blk c12 = part(0, m, n, a.n - n), c22 = part(m, a.m - m, n, a.n - n);
+    hmat_add(c, *a.ch[0], c11, s);
+    hmat_add(c, *a.ch[2], c21, s);
+    hmat_add(c, *a.ch[1], c12, s);
+    hmat_add(c, *a.ch[3], c22, s);
+  } else if (a.type == T_H && b.type == T_H) {
+    for (int q = 0; q < 4; ++q) hmat_add(c, *a.ch[q], *b.ch[q], s);
+  }
+}
+
+static BP hadd(Ctx& c, const Blk& a, const Blk& b) {
+  BP r = copy_blk(c, a);
+  hmat_add(c, *r, b, 1.0);
+  return r;
+}
+
+// ---- H x H (src/harithm.jl:162-314) -----------------------------------------
+static BP hmul(Ctx& c, const Blk& a, const Blk& b) {
+  BP M;
+  if (a.type == T_DENSE) {
+    if (b.type == T_H && !is_leaf_cluster(c, a.s) && !is_leaf_cluster(c, a.t))
+      throw LuError(HM_ERR_UNSUPPORTED, "full_mat_mul branch that has no method in the reference");
+    if (b.type == T_H) {
+      BP db = dense_of(c, b);
+      M = new_dense(c, a.m, b.n, a.s, b.t);
+      gemm(c, M->Cv(), a.Cv(), db->Cv(), 1.0, 0.0);
+    } else if (b.type == T_DENSE) {
+      M = new_dense(c, a.m, b.n, a.s, b.t);
+      gemm(c, M->Cv(), a.Cv(), b.Cv(), 1.0, 0.0);
+    } else {
+      M = new_rk(c, a.m, b.n, a.s, b.t, true, false);
+      M->B = b.B; M->ldb = b.ldb;
+      gemm(c, M->Av(), a.Cv(), b.Av(), 1.0, 0.0);
+      copy_int(c, M->k, b.k);
+    }
+  } else if (b.type == T_DENSE) {
+    if (a.type == T_H && !is_leaf_cluster(c, b.s) && !is_leaf_cluster(c, b.t))
+      throw LuError(HM_ERR_UNSUPPORTED, "mat_full_mul branch that has no method in the reference");
+    if (a.type == T_H) {
+      M = new_dense(c, a.m, b.n, a.s, b.t);
+      axpby(c, M->Cv(), View{nullptr, 0, 0, a.m, b.n}, 0.0, 0.0);
+      hmm(c, M->Cv(), 1.0, a, b.Cv());
+    } else {
+      M = new_rk(c, a.m, b.n, a.s, b.t, false, true);
+      M->A = a.A; M->lda = a.lda;
+      gemm(c, M->Bv(), vtr(b.Cv()), a.Bv(), 1.0, 0.0);
+      copy_int(c, M->k, a.k);
+    }
+  } else if (a.type == T_RK && b.type == T_RK) {
+    M = new_rk(c, a.m, b.n, a.s, b.t, false, true);
+    M->A = a.A; M->lda = a.lda;
+    Blk tmp;
+    tmp.st = c.st;
+    double* W = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)b.cap * a.cap);
+    View Wv{W, 1, b.cap, b.cap, a.cap};
+    gemm(c, Wv, vtr(b.Av()), a.Bv(), 1.0, 0.0);
+    gemm(c, M->Bv(), b.Bv(), Wv, 1.0, 0.0);
+    copy_int(c, M->k, a.k);
+  } else if (a.type == T_RK && b.type == T_H) {
+    M = new_rk(c, a.m, b.n, a.s, b.t, false, true);
+    M->A = a.A; M->lda = a.lda;
+    axpby(c, M->Bv(), View{nullptr, 0, 0, b.n, M->cap}, 0.0, 0.0);
+    hmm_t(c, M->Bv(), 1.0, b, a.Bv());
+    copy_int(c, M->k, a.k);
+  } else if (a.type == T_H && b.type == T_RK) {
+    M = new_rk(c, a.m, b.n, a.s, b.t, true, false);
+    M->B = b.B; M->ldb = b.ldb;
+    axpby(c, M->Av(), View{nullptr, 0, 0, a.m, M->cap}, 0.0, 0.0);
+    hmm(c, M->Av(), 1.0, a, b.Av());
+    copy_int(c, M->k, b.k);
+  } else {
+    M = std::make_shared<Blk>();
+    M->st = c.st;
+    M->type = T_H; M->m = a.m; M->n = b.n; M->s = a.s; M->t = b.t;
+    for (int i = 0; i < 2; ++i)
+      for (int j = 0; j < 2; ++j) {
+        BP H1 = hmul(c, *a.ch[2 * i + 0], *b.ch[0 + j]);
+        BP H2 = hmul(c, *a.ch[2 * i + 1], *b.ch[2 + j]);
+        M->ch[2 * i + j] = hadd(c, *H1, *H2);
+      }
+  }
+  M->s = a.s;
+  M->t = b.t;
+  return M;
+}
+
+static void sub_mul(Ctx& c, Blk& cc, const Blk& a, const Blk& b) {
+  BP M = hmul(c, a, b);
+  hmat_add(c, cc, *M, -1.0);
+}
+
+// ---- triangular solves (src/hlu.jl:236-442) ----------------------------------
+static void mfs(Ctx& c, const Blk& a, View X, bool unit, bool lower) {
+  if (a.type == T_RK) throw LuError(HM_ERR_UNSUPPORTED, "A should not be a low-rank matrix");
+  if (lower) {
+    if (a.type == T_DENSE) {
+      trsm_lower(c, a.Cv(), X, unit);
+    } else {
+      const int n = a.ch[0]->m;
+      View X1 = vsub(X, 0, 0, n, X.cols), X2 = vsub(X, n, 0, X.rows - n, X.cols);
+      mfs(c, *a.ch[0], X1, unit, true);
+      hmm(c, X2, -1.0, *a.ch[2], X1);
+      mfs(c, *a.ch[3], X2, unit, true);
+    }
+  } else {
+    if (a.type == T_DENSE) {
+      // X <- X U^{-1}  ==  X' <- U'^{-1} X'
+      trsm_lower(c, vtr(a.Cv()), vtr(X), unit);
+    } else {
+      const int n = a.ch[0]->m;
+      View X1 = vsub(X, 0, 0, X.rows, n), X2 = vsub(X, 0, n, X.rows, X.cols - n);
+      mfs(c, *a.ch[0], X1, unit, false);
+      xh(c, X2, -1.0, X1, *a.ch[1]);
+      mfs(c, *a.ch[3], X2, unit, false);
+    }
+  }
+}
+
+static void trisolve(Ctx& c, const Blk& a, Blk& b, bool lower, bool unit) {
+  if (a.type == T_RK) throw LuError(HM_ERR_UNSUPPORTED, "A should not be a low-rank matrix");
+  if (lower) {
+    if (a.type == T_DENSE && b.type == T_DENSE) trsm_lower(c, a.Cv(), b.Cv(), unit);
+    else if (a.type == T_DENSE && b.type == T_RK) trsm_lower(c, a.Cv(), b.Av(), unit);
+    else if (a.type == T_DENSE && b.type == T_H) throw LuError(HM_ERR_UNSUPPORTED, "This is never used");
+    else if (a.type == T_H && b.type == T_H) {
+      trisolve(c, *a.ch[0], *b.ch[0], lower, unit);
+      trisolve(c, *a.ch[0], *b.ch[1], lower, unit);
+      sub_mul(c, *b.ch[2], *a.ch[2], *b.ch[0]);
+      sub_mul(c, *b.ch[3], *a.ch[2], *b.ch[1]);
+      trisolve(c, *a.ch[3], *b.ch[2], lower, unit);
+      trisolve(c, *a.ch[3], *b.ch[3], lower, unit);
+    } else if (a.type == T_H && b.type == T_DENSE) mfs(c, a, b.Cv(), unit, true);
+    else if (a.type == T_H && b.type == T_RK) mfs(c, a, b.Av(), unit, true);
+  } else {
+    if (a.type == T_DENSE && b.type == T_DENSE) trsm_lower(c, vtr(a.Cv()), vtr(b.Cv()), unit);
+    else if (a.type == T_DENSE && b.type == T_RK) trsm_lower(c, vtr(a.Cv()), b.Bv(), unit);
+    else if (a.type == T_H && b.type == T_DENSE) mfs(c, a, b.Cv(), unit, false);
+    else if (a.type == T_H && b.type == T_RK) mfs(c, a, vtr(b.Bv()), unit, false);
+    else if (a.type == T_H && b.type == T_H) {
+      trisolve(c, *a.ch[0], *b.ch[0], lower, unit);
+      trisolve(c, *a.ch[0], *b.ch[2], lower, unit);
+      sub_mul(c, *b.ch[1], *b.ch[0], *a.ch[1]);
+      sub_mul(c, *b.ch[3], *b.ch[2], *a.ch[1]);
+      trisolve(c, *a.ch[3], *b.ch[1], lower, unit);
+      trisolve(c, *a.ch[3], *b.ch[3], lower, unit);
+    } else throw LuError(HM_ERR_UNSUPPORTED, "Invalid");
+  }
+}
+
+// ---- LU (src/hlu.jl:446-515) --------------------------------------------------
+static void permute(Ctx& c, Blk& H) {
+  if (H.type == T_DENSE) laswp(c, H.Cv(), H.row0);
+  else if (H.type == T_RK) laswp(c, H.Av(), H.row0);
+  else
+    for (int q = 0; q < 4; ++q) permute(c, *H.ch[q]);
+}
+
+static void lu_rec(Ctx& c, Blk& H) {
+  if (H.type == T_RK) throw LuError(HM_ERR_UNSUPPORTED, "H should not be a low-rank matrix");
+  if (H.type == T_DENSE) {
+    getrf(c, H.Cv(), H.row0);
+    return;
+  }
+  lu_rec(c, *H.ch[0]);
+  permute(c, *H.ch[1]);
+  trisolve(c, *H.ch[0], *H.ch[1], true, true);
+  trisolve(c, *H.ch[0], *H.ch[2], false, false);
+  sub_mul(c, *H.ch[3], *H.ch[2], *H.ch[1]);
+  lu_rec(c, *H.ch[3]);
+  permute(c, *H.ch[2]);
+}
+
+// ---- solve (src/hlu.jl:524-562) -----------------------------------------------
+static void solve_rec(Ctx& c, const Blk& a, View y, bool lower) {
+  if (a.type == T_RK) throw LuError(HM_ERR_UNSUPPORTED, "a cannot be a low-rank matrix");
+  const int m = a.type == T_H ? a.ch[0]->m : a.m;
+  if (lower) {
+    if (a.type == T_DENSE) {
+      trsm_lower(c, a.Cv(), y, true);
+    } else {
+      solve_rec(c, *a.ch[0], vsub(y, 0, 0, m, y.cols), true);
+      hmm(c, vsub(y, m, 0, y.rows - m, y.cols), -1.0, *a.ch[2], vsub(y, 0, 0, m, y.cols));
+      solve_rec(c, *a.ch[3], vsub(y, m, 0, y.rows - m, y.cols), true);
+    }
+  } else {
+    if (a.type == T_DENSE) {
+      trsm_lower(c, vrev(a.Cv()), vrev(y), false);       // U^{-1} y as a reversed lower solve
+    } else {
+      solve_rec(c, *a.ch[3], vsub(y, m, 0, y.rows - m, y.cols), false);
+      hmm(c, vsub(y, 0, 0, m, y.cols), -1.0, *a.ch[1], vsub(y, m, 0, y.rows - m, y.cols));
+      solve_rec(c, *a.ch[0], vsub(y, 0, 0, m, y.cols), false);
+    }
+  }
+}
+
+// transposed solve H' x = b with H[P,:] = L U: U' z = b (lower, non-unit),
+// L' w = z (upper, unit), x[P] = w.  No counterpart in the reference (the
+// adjoint of H\y); the same leaf kernels run on transposed/reversed views.
+static void solve_t_rec(Ctx& c, const Blk& a, View y, bool upper_t) {
+  if (a.type == T_RK) throw LuError(HM_ERR_UNSUPPORTED, "a cannot be a low-rank matrix");
+  const int m = a.type == T_H ? a.ch[0]->m : a.m;
+  if (upper_t) {                       // U' is lower triangular
+    if (a.type == T_DENSE) {
+      trsm_lower(c, vtr(a.Cv()), y, false);
+    } else {
+      solve_t_rec(c, *a.ch[0], vsub(y, 0, 0, m, y.cols), true);
+      hmm_t(c, vsub(y, m, 0, y.rows - m, y.cols), -1.0, *a.ch[1], vsub(y, 0, 0, m, y.cols));
+      solve_t_rec(c, *a.ch[3], vsub(y, m, 0, y.rows - m, y.cols), true);
+    }
+  } else {                             // L' is unit upper triangular
+    if (a.type == T_DENSE) {
+      trsm_lower(c, vrev(vtr(a.Cv())), vrev(y), true);
+    } else {
+      solve_t_rec(c, *a.ch[3], vsub(y, m, 0, y.rows - m, y.cols), false);
+      hmm_t(c, vsub(y, 0, 0, m, y.cols), -1.0, *a.ch[2], vsub(y, m, 0, y.rows - m, y.cols));
+      solve_t_rec(c, *a.ch[0], vsub(y, 0, 0, m, y.cols), false);
+    }
+  }
+}
+
+// x[P[i], c] = w[i, c]
+__global__ void lu_scatter_rows_kernel(View Xv, View W, const int64_t* __restrict__ P) {
+  const int64_t tot = (int64_t)W.rows * W.cols;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % W.rows), c = (int)(e / W.rows);
+    Xv.p[P[i] * Xv.rs + (int64_t)c * Xv.cs] = W.p[(int64_t)i * W.rs + (int64_t)c * W.cs];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// state, entry points
+// ---------------------------------------------------------------------------
+struct LuState {
+  BP root;
+  int64_t* P = nullptr;
+  int* flags = nullptr;
+  int cap = 0;
+  cudaStream_t st = nullptr;
+  ~LuState() {
+    root.reset();
+    if (P) cudaFreeAsync(P, st);
+    if (flags) cudaFreeAsync(flags, st);
+    if (st) cudaStreamSynchronize(st);
+  }
+};
+
+static BP build_from_handle(Ctx& c, const hm_handle* h, int32_t node) {
+  const Node& nd = h->nodes[node];
+  const int m = (int)(h->cl_e[nd.s] - h->cl_s[nd.s]), n = (int)(h->cl_e[nd.t] - h->cl_s[nd.t]);
+  if (nd.type == T_H) {
+    BP b = std::make_shared<Blk>();
+    b->st = c.st;
+    b->type = T_H; b->m = m; b->n = n; b->s = nd.s; b->t = nd.t; b->row0 = h->cl_s[nd.s];
+    for (int q = 0; q < 4; ++q) b->ch[q] = build_from_handle(c, h, nd.child[q]);
+    return b;
+  }
+  const Leaf& L = h->leaves[nd.leaf];
+  const int eb = elem_bytes(h->storage), deb = dense_elem_bytes(h->storage);
+  if (nd.type == T_DENSE) {
+    BP d = new_dense(c, m, n, nd.s, nd.t);
+    d->row0 = L.row0;
+    const int64_t ld = col_pad(m, deb);
+    unsigned g = (unsigned)std::min<int64_t>(((int64_t)m * n + 255) / 256, 1024);
+    if (h->storage == HM_F64)
+      lu_load_kernel<double><<<g, 256, 0, c.st>>>((const double*)h->d_dense + L.off, ld, m, n, d->C, d->ldc, n);
+    else
+      lu_load_kernel<float><<<g, 256, 0, c.st>>>((const float*)h->d_dense + L.off, ld, m, n, d->C, d->ldc, n);
+    LU_LAUNCH_CHECK();
+    return d;
+  }
+  if (L.k > c.cap) throw LuError(HM_ERR_RANK, "leaf rank above the H-LU rank capacity");
+  BP r = new_rk(c, m, n, nd.s, nd.t);
+  r->row0 = L.row0;
+  const int64_t npad = col_pad(n, eb), mpad = col_pad(m, eb);
+  auto load = [&](int64_t off, int64_t ld, int rows, double* dst, int64_t ldd) {
+    unsigned g = (unsigned)std::min<int64_t>(((int64_t)rows * c.cap + 255) / 256, 1024);
+    switch (h->storage) {
+      case HM_F64: lu_load_kernel<double><<<g, 256, 0, c.st>>>((const double*)h->d_rk + off, ld, rows, L.k, dst, ldd, c.cap); break;
+      case HM_F32: lu_load_kernel<float><<<g, 256, 0, c.st>>>((const float*)h->d_rk + off, ld, rows, L.k, dst, ldd, c.cap); break;
+      default: lu_load_kernel<__nv_bfloat16><<<g, 256, 0, c.st>>>((const __nv_bfloat16*)h->d_rk + off, ld, rows, L.k, dst, ldd, c.cap);
+    }
+    LU_LAUNCH_CHECK();
+  };
+  load(L.off, npad, n, r->B, r->ldb);
+  load(L.off + npad * L.k, mpad, m, r->A, r->lda);
+  lu_set_int_kernel<<<1, 1, 0, c.st>>>(r->k, L.k);
+  LU_LAUNCH_CHECK();
+  return r;
+}
+
+static int finish(Ctx& c, const char* what) {
+  int flags = 0;
+  HM_CUDA_TRY(cudaMemcpyAsync(&flags, c.flags, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+  HM_CUDA_TRY(cudaStreamSynchronize(c.st));
+  if (flags & 4) return fail(HM_ERR_SINGULAR, std::string(what) + ": exactly zero pivot in a diagonal leaf");
+  if (flags & 2) return fail(HM_ERR_NONFINITE, std::string(what) + ": non-finite values");
+  if (flags & 1) return fail(HM_ERR_RANK, std::string(what) + ": a rank exceeded the capacity " + std::to_string(c.cap));
+  return HM_OK;
+}
+
 int lu_factor(hm_handle* h) {
-  (void)h;
-  return fail(HM_ERR_UNSUPPORTED, "H-LU is not built yet");
+  LuState* S = new LuState();
+  S->st = h->stream;
+  S->cap = h->prm.rank_cap > 0 ? h->prm.rank_cap : std::max(32, 2 * std::max(h->kmax, 1));
+  S->cap = std::min(S->cap, RCORE_MAX / 2);
+  HM_CUDA_TRY(cudaMallocAsync((void**)&S->P, sizeof(int64_t) * h->n, h->stream));
+  HM_CUDA_TRY(cudaMallocAsync((void**)&S->flags, sizeof(int), h->stream));
+  HM_CUDA_TRY(cudaMemsetAsync(S->flags, 0, sizeof(int), h->stream));
+  Ctx c{h->stream, S->cap, S->P, S->flags, h->prm.eps_trunc, h};
+  try {
+    if (h->kmax > S->cap) throw LuError(HM_ERR_RANK, "a leaf rank exceeds the H-LU rank capacity");
+    S->root = build_from_handle(c, h, 0);
+    lu_rec(c, *S->root);
+  } catch (const LuError& e) {
+    cudaStreamSynchronize(h->stream);
+    delete S;
+    return fail(e.code, std::string("lu!: ") + e.what());
+  }
+  int s = finish(c, "lu!");
+  if (s != HM_OK) {
+    delete S;
+    return s;
+  }
+  h->lu = S;
+  h->factorized = true;
+  return HM_OK;
 }
-int lu_solve_device(hm_handle* h, const double*, double*, int64_t, cudaStream_t) {
-  (void)h;
-  return fail(HM_ERR_UNSUPPORTED, "H-solve is not built yet");
+
+int lu_solve_device(hm_handle* h, const double* d_b, double* d_x, int64_t ncols, int trans, cudaStream_t st) {
+  LuState* S = h->lu;
+  if (!S) return fail(HM_ERR_STATE, "a has not been factorized");
+  if (ncols <= 0) return HM_OK;
+  Ctx c{st, S->cap, S->P, S->flags, h->prm.eps_trunc, h};
+  try {
+    View B{const_cast<double*>(d_b), 1, h->n, (int)h->n, (int)ncols};
+    View X{d_x, 1, h->n, (int)h->n, (int)ncols};
+    const int64_t tot = h->n * ncols;
+    const unsigned g = (unsigned)std::min<int64_t>((tot + 255) / 256, 4096);
+    if (!trans) {
+      // a\y (src/hlu.jl:553-562): permute!(w, P), unit-L forward, U backward
+      lu_gather_rows_kernel<<<g, 256, 0, st>>>(X, B, S->P);
+      LU_LAUNCH_CHECK();
+      solve_rec(c, *S->root, X, true);
+      solve_rec(c, *S->root, X, false);
+    } else {
+      Blk tmp;
+      tmp.st = st;
+      double* w = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)tot);
+      View W{w, 1, h->n, (int)h->n, (int)ncols};
+      axpby(c, W, B, 1.0, 0.0);
+      solve_t_rec(c, *S->root, W, true);
+      solve_t_rec(c, *S->root, W, false);
+      lu_scatter_rows_kernel<<<g, 256, 0, st>>>(X, W, S->P);
+      LU_LAUNCH_CHECK();
+    }
+  } catch (const LuError& e) {
+    return fail(e.code, std::string("H\\y: ") + e.what());
+  }
+  HM_CUDA_TRY(cudaGetLastError());
+  return HM_OK;
 }
-int lu_perm(const hm_handle*, int64_t*) { return fail(HM_ERR_UNSUPPORTED, "H-LU is not built yet"); }
-int lu_to_dense(const hm_handle*, double*) { return fail(HM_ERR_UNSUPPORTED, "H-LU is not built yet"); }
+
+__global__ void lu_colnorm2_kernel(View X, double* __restrict__ out) {
+  __shared__ double red[32];
+  const int c = blockIdx.x;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < X.rows; i += blockDim.x) {
+    const double v = X.p[(int64_t)i * X.rs + (int64_t)c * X.cs];
+    s = fma(v, v, s);
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) out[c] = s;
+}
+
+// Iterative refinement: x = (LU)^{-1} b, then r = b - H x with the FP64
+// H-matvec of the unfactorised matrix (the matvec pools stay intact after
+// lu!), x += (LU)^{-1} r, until max_c |r_c|/|b_c| <= tol or max_iter steps.
+int lu_solve_refined(hm_handle* h, const double* d_b, double* d_x, int64_t ncols, int trans, double tol,
+                     int max_iter, cudaStream_t st, int* iters, double* relres) {
+  if (!h->lu) return fail(HM_ERR_STATE, "a has not been factorized");
+  const int64_t n = h->n, tot = n * ncols;
+  double *r = nullptr, *d = nullptr, *nrm = nullptr;
+  HM_CUDA_TRY(cudaMallocAsync(&r, sizeof(double) * tot, st));
+  HM_CUDA_TRY(cudaMallocAsync(&d, sizeof(double) * tot, st));
+  HM_CUDA_TRY(cudaMallocAsync(&nrm, sizeof(double) * 2 * ncols, st));
+  std::vector<double> hb(ncols), hr(ncols);
+  int status = HM_OK, it = 0;
+  double worst = 0.0;
+  View Bv{const_cast<double*>(d_b), 1, n, (int)n, (int)ncols};
+  View Rv{r, 1, n, (int)n, (int)ncols};
+  Ctx c{st, h->lu->cap, h->lu->P, h->lu->flags, h->prm.eps_trunc, h};
+  auto norms = [&](View V, double* dst, std::vector<double>& host) -> int {
+    lu_colnorm2_kernel<<<(unsigned)ncols, 256, 0, st>>>(V, dst);
+    HM_CUDA_TRY(cudaGetLastError());
+    HM_CUDA_TRY(cudaMemcpyAsync(host.data(), dst, sizeof(double) * ncols, cudaMemcpyDeviceToHost, st));
+    HM_CUDA_TRY(cudaStreamSynchronize(st));
+    return HM_OK;
+  };
+  status = norms(Bv, nrm, hb);
+  if (status == HM_OK) status = lu_solve_device(h, d_b, d_x, ncols, trans, st);
+  for (; status == HM_OK; ++it) {
+    for (int64_t q = 0; q < ncols && status == HM_OK; ++q)
+      status = matvec_device(h, d_x + q * n, r + q * n, trans, st);
+    if (status != HM_OK) break;
+    try {
+      axpby(c, Rv, Bv, 1.0, -1.0);                    // r = b - H x
+    } catch (const LuError& e) {
+      status = fail(e.code, e.what());
+      break;
+    }
+    status = norms(Rv, nrm + ncols, hr);
+    if (status != HM_OK) break;
+    worst = 0.0;
+    for (int64_t q = 0; q < ncols; ++q)
+      worst = std::max(worst, hb[q] > 0 ? std::sqrt(hr[q] / hb[q]) : std::sqrt(hr[q]));
+    if (!(worst == worst)) { status = fail(HM_ERR_NONFINITE, "refinement: non-finite residual"); break; }
+    if (worst <= tol || it >= max_iter) break;
+    status = lu_solve_device(h, r, d, ncols, trans, st);
+    if (status != HM_OK) break;
+    try {
+      axpby(c, View{d_x, 1, n, (int)n, (int)ncols}, View{d, 1, n, (int)n, (int)ncols}, 1.0, 1.0);
+    } catch (const LuError& e) {
+      status = fail(e.code, e.what());
+      break;
+    }
+  }
+  cudaFreeAsync(r, st);
+  cudaFreeAsync(d, st);
+  cudaFreeAsync(nrm, st);
+  cudaStreamSynchronize(st);
+  if (iters) *iters = it;
+  if (relres) *relres = worst;
+  return status;
+}
+
+int lu_perm(const hm_handle* h, int64_t* P) {
+  if (!h->lu) return fail(HM_ERR_STATE, "a has not been factorized");
+  HM_CUDA_TRY(cudaMemcpyAsync(P, h->lu->P, sizeof(int64_t) * h->n, cudaMemcpyDeviceToHost, h->stream));
+  HM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return HM_OK;
+}
+
+int lu_to_dense(const hm_handle* h, double* d_out) {
+  if (!h->lu) return fail(HM_ERR_STATE, "a has not been factorized");
+  Ctx c{h->stream, h->lu->cap, h->lu->P, h->lu->flags, h->prm.eps_trunc, h};
+  try {
+    densify_into(c, View{d_out, 1, h->n, (int)h->n, (int)h->n}, *h->lu->root);
+  } catch (const LuError& e) {
+    return fail(e.code, e.what());
+  }
+  HM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return HM_OK;
+}
+
 void lu_free(hm_handle* h) {
   delete h->lu;
   h->lu = nullptr;
 }
+
 int lu_copy(const hm_handle* src, hm_handle* dst) {
-  (void)src;
-  (void)dst;
+  if (!src->lu) return HM_OK;
+  LuState* S = new LuState();
+  S->st = dst->stream;
+  S->cap = src->lu->cap;
+  HM_CUDA_TRY(cudaStreamSynchronize(src->stream));
+  HM_CUDA_TRY(cudaMallocAsync((void**)&S->P, sizeof(int64_t) * src->n, dst->stream));
+  HM_CUDA_TRY(cudaMallocAsync((void**)&S->flags, sizeof(int), dst->stream));
+  HM_CUDA_TRY(cudaMemcpyAsync(S->P, src->lu->P, sizeof(int64_t) * src->n, cudaMemcpyDeviceToDevice, dst->stream));
+  HM_CUDA_TRY(cudaMemsetAsync(S->flags, 0, sizeof(int), dst->stream));
+  Ctx c{dst->stream, S->cap, S->P, S->flags, src->prm.eps_trunc, src};
+  try {
+    S->root = copy_blk(c, *src->lu->root);
+  } catch (const LuError& e) {
+    delete S;
+    return fail(e.code, e.what());
+  }
+  HM_CUDA_TRY(cudaStreamSynchronize(dst->stream));
+  dst->lu = S;
   return HM_OK;
 }
 

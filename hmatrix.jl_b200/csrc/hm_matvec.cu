@@ -4,7 +4,7 @@
 //
 // Phase 1: one warp per low-rank leaf streams its F1 factor (B for H*x)
 //          with 16-byte loads and writes z = F1' x_seg (k values) to z[].
-// Phase 2: one CTA per window of 512 output rows; each warp owns 32 rows and
+// Phase 2: one CTA per window of 1024 output rows; each lane owns 4 rows and
 //          accumulates sum_r F2[:,r] z_r over the low-rank leaves and C x_seg
 //          over the dense leaves that cover its rows, in FP64, and stores y.
 // The input is staged as 16-byte aligned shifted copies so that every
@@ -13,6 +13,7 @@
 #include "hm_lowrank.cuh"
 
 #include <algorithm>
+#include <type_traits>
 #include <cstring>
 
 namespace hm {
@@ -138,17 +139,84 @@ __global__ void __launch_bounds__(256) mv_phase1_kernel(const P1Desc* __restrict
 }
 
 // ---------------------------------------------------------------------------
-// phase 2: y(window) = sum over leaves covering the window
+// phase 2: y(window) = sum over leaves covering the window.  Each lane owns 4
+// consecutive output rows; when a leaf starts on a 4-row boundary of the
+// window its 4 values come in one vector load (columns are padded to a
+// multiple of 4 elements and 16 bytes, padding rows hold zeros).
 // ---------------------------------------------------------------------------
 constexpr int P2_NB = 32;      // descriptors staged per round
 constexpr int P2_EMAX = 1024;  // expanded (leaf, column) entries per sub-round
+constexpr int P2_WARPS = MV_WROWS / 128;
 constexpr uint64_t P2_DENSE_FLAG = 1ull << 63;
 
+// 4 consecutive rows of one column are loaded as raw words and converted to
+// FP64 only when they are multiplied: a conversion next to its load would
+// make the warp wait for that load before issuing the next entry's loads.
+template <typename T> struct Row4;
+template <> struct Row4<double> {               // dense leaves: double as well
+  static constexpr int U = 4;
+  struct Raw { double2 a, b; };
+  __device__ static Raw zero() { return Raw{make_double2(0.0, 0.0), make_double2(0.0, 0.0)}; }
+  __device__ static Raw ld(const double* p) {
+    return Raw{__ldcs(reinterpret_cast<const double2*>(p)), __ldcs(reinterpret_cast<const double2*>(p) + 1)};
+  }
+  __device__ static Raw ldd(const double* p) { return ld(p); }
+  __device__ static void put(Raw& r, int q, double v) {
+    if (q == 0) r.a.x = v; else if (q == 1) r.a.y = v; else if (q == 2) r.b.x = v; else r.b.y = v;
+  }
+  __device__ static void cvt(const Raw& r, bool, double (&v)[4]) { v[0] = r.a.x; v[1] = r.a.y; v[2] = r.b.x; v[3] = r.b.y; }
+};
+template <> struct Row4<float> {                // dense leaves: float
+  static constexpr int U = 8;
+  using Raw = float4;
+  __device__ static Raw zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+  __device__ static Raw ld(const float* p) { return __ldcs(reinterpret_cast<const float4*>(p)); }
+  __device__ static Raw ldd(const float* p) { return ld(p); }
+  __device__ static void put(Raw& r, int q, float v) {
+    if (q == 0) r.x = v; else if (q == 1) r.y = v; else if (q == 2) r.z = v; else r.w = v;
+  }
+  __device__ static void cvt(const Raw& r, bool, double (&v)[4]) { v[0] = r.x; v[1] = r.y; v[2] = r.z; v[3] = r.w; }
+};
+template <> struct Row4<__nv_bfloat16> {        // dense leaves: float (raw float bits)
+  static constexpr int U = 8;
+  using Raw = uint4;
+  __device__ static Raw zero() { return make_uint4(0u, 0u, 0u, 0u); }
+  __device__ static Raw ld(const __nv_bfloat16* p) {
+    const uint2 a = __ldcs(reinterpret_cast<const uint2*>(p));
+    return make_uint4(a.x, a.y, 0u, 0u);
+  }
+  __device__ static Raw ldd(const float* p) {
+    return __ldcs(reinterpret_cast<const uint4*>(p));
+  }
+  __device__ static void put(Raw& r, int q, float v) {
+    const uint32_t b = __float_as_uint(v);
+    if (q == 0) r.x = b; else if (q == 1) r.y = b; else if (q == 2) r.z = b; else r.w = b;
+  }
+  __device__ static void put(Raw& r, int q, __nv_bfloat16 v) {
+    const uint32_t b = (uint32_t)__bfloat16_as_ushort(v);
+    if (q == 0) r.x = (r.x & 0xffff0000u) | b;
+    else if (q == 1) r.x = (r.x & 0x0000ffffu) | (b << 16);
+    else if (q == 2) r.y = (r.y & 0xffff0000u) | b;
+    else r.y = (r.y & 0x0000ffffu) | (b << 16);
+  }
+  __device__ static void cvt(const Raw& r, bool dense, double (&v)[4]) {
+    if (dense) {
+      v[0] = __uint_as_float(r.x); v[1] = __uint_as_float(r.y);
+      v[2] = __uint_as_float(r.z); v[3] = __uint_as_float(r.w);
+    } else {
+      v[0] = bf_lo(r.x); v[1] = bf_hi(r.x); v[2] = bf_lo(r.y); v[3] = bf_hi(r.y);
+    }
+  }
+};
+
 template <typename T, typename TD>
-__global__ void __launch_bounds__(512) mv_phase2_kernel(const MvWin* __restrict__ win, const P2Desc* __restrict__ d,
-                                                        const T* __restrict__ rk, const TD* __restrict__ dn,
-                                                        const double* __restrict__ z, const double* __restrict__ x,
-                                                        double* __restrict__ y) {
+__global__ void __launch_bounds__(P2_WARPS * 32) mv_phase2_kernel(const MvWin* __restrict__ win,
+                                                                  const P2Desc* __restrict__ d,
+                                                                  const T* __restrict__ rk, const TD* __restrict__ dn,
+                                                                  const double* __restrict__ z,
+                                                                  const double* __restrict__ x,
+                                                                  double* __restrict__ y) {
+  constexpr int U = Row4<T>::U;
   __shared__ P2Desc sd[P2_NB];
   __shared__ int spre[P2_NB + 1];
   __shared__ uint64_t e_off[P2_EMAX];
@@ -158,8 +226,8 @@ __global__ void __launch_bounds__(512) mv_phase2_kernel(const MvWin* __restrict_
   __shared__ double e_z[P2_EMAX];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const MvWin W = win[blockIdx.x];
-  const int lrow = warp * 32 + lane;
-  double acc = 0.0;
+  const int base = 4 * (warp * 32 + lane);       // first of this lane's rows in the window
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
   for (uint32_t b0 = W.begin; b0 < W.end; b0 += P2_NB) {
     const int nb = (int)min((uint32_t)P2_NB, W.end - b0);
     __syncthreads();
@@ -209,34 +277,55 @@ __global__ void __launch_bounds__(512) mv_phase2_kernel(const MvWin* __restrict_
         e_m[e] = D.m;
       }
       __syncthreads();
-      if (warp * 32 < (int)W.nrows) {
-        for (int e = 0; e < ne; e += 8) {
-          double v[8];
-          double zz[8];
+      for (int e = 0; e < ne; e += U) {
+        typename Row4<T>::Raw raw[U];
+        double zz[U];
+        bool isd[U];
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            v[u] = 0.0;
-            zz[u] = 0.0;
-            const int ee = e + u;
-            if (ee < ne) {
-              const int lr = lrow - e_ro[ee];
-              if (lr >= 0 && lr < (int)e_m[ee]) {
-                const uint64_t o = e_off[ee];
-                zz[u] = e_z[ee];
-                if (o & P2_DENSE_FLAG)
-                  v[u] = (double)__ldg(dn + (o & ~P2_DENSE_FLAG) + (uint64_t)lr * e_rs[ee]);
-                else
-                  v[u] = from_store<T>(rk[o + (uint64_t)lr]);
+        for (int u = 0; u < U; ++u) {
+          raw[u] = Row4<T>::zero();
+          zz[u] = 0.0;
+          isd[u] = false;
+          const int ee = e + u;
+          if (ee < ne) {
+            const int ro = e_ro[ee];
+            const int mm = (int)e_m[ee];
+            const uint64_t o = e_off[ee];
+            const uint32_t rs = e_rs[ee];
+            const int lr = base - ro;
+            const bool dense = (o & P2_DENSE_FLAG) != 0;
+            zz[u] = e_z[ee];
+            isd[u] = dense;
+            if (((ro & 3) == 0) && rs == 1) {
+              if (lr >= 0 && lr < mm) {
+                if (dense) raw[u] = Row4<T>::ldd(dn + (o & ~P2_DENSE_FLAG) + lr);
+                else raw[u] = Row4<T>::ld(rk + o + lr);
+              }
+            } else {
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                const int r = lr + q;
+                if (r >= 0 && r < mm) {
+                  if (dense) Row4<T>::put(raw[u], q, __ldg(dn + (o & ~P2_DENSE_FLAG) + (uint64_t)r * rs));
+                  else Row4<T>::put(raw[u], q, rk[o + (uint64_t)r]);
+                }
               }
             }
           }
+        }
 #pragma unroll
-          for (int u = 0; u < 8; ++u) acc = fma(v[u], zz[u], acc);
+        for (int u = 0; u < U; ++u) {
+          double v[4];
+          Row4<T>::cvt(raw[u], isd[u], v);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[q] = fma(v[q], zz[u], acc[q]);
         }
       }
     }
   }
-  if (lrow < (int)W.nrows) y[W.row0 + lrow] = acc;
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    if (base + q < (int)W.nrows) y[W.row0 + base + q] = acc[q];
 }
 
 // ---------------------------------------------------------------------------
@@ -372,12 +461,10 @@ static int matvec_t(hm_handle* h, const double* d_x, double* d_y, int trans, cud
     mv_phase1_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(P.d_p1, P.np1, (const T*)h->d_rk, xs, stride, h->d_z);
   }
   if (ev) HM_CUDA_TRY(cudaEventRecord(ev[2], st));
-  if (h->storage == HM_F64)
-    mv_phase2_kernel<T, double><<<P.nwin, 512, 0, st>>>(P.d_win, P.d_p2, (const T*)h->d_rk,
-                                                        (const double*)h->d_dense, h->d_z, d_x, d_y);
-  else
-    mv_phase2_kernel<T, float><<<P.nwin, 512, 0, st>>>(P.d_win, P.d_p2, (const T*)h->d_rk,
-                                                       (const float*)h->d_dense, h->d_z, d_x, d_y);
+  // dense leaves are FP64 with FP64 factors and FP32 otherwise
+  using TD = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
+  mv_phase2_kernel<T, TD><<<P.nwin, P2_WARPS * 32, 0, st>>>(P.d_win, P.d_p2, (const T*)h->d_rk,
+                                                            (const TD*)h->d_dense, h->d_z, d_x, d_y);
   if (ev) HM_CUDA_TRY(cudaEventRecord(ev[3], st));
   HM_CUDA_TRY(cudaGetLastError());
   return HM_OK;

@@ -250,23 +250,36 @@ class Hmat:
         check(lib().hm_lu_perm(self._h, _ptr(P)))
         return P
 
-    def solve(self, y):
-        """``a\\y`` (src/hlu.jl:553-562) for a factorised H."""
+    def solve(self, y, trans=False):
+        """``a\\y`` (src/hlu.jl:553-562) for a factorised H; ``trans`` solves with H'."""
+        tf = _lib.HM_FLAG_TRANS if trans else 0
         try:
             import torch
             if isinstance(y, torch.Tensor):
                 Y = y.reshape(self.n, -1).t().contiguous()
                 X = torch.empty_like(Y)
                 check(lib().hm_solve(self._h, C.c_void_p(Y.data_ptr()), C.c_void_p(X.data_ptr()), Y.shape[0],
-                                     _lib.HM_FLAG_DEVICE_PTRS, _torch_stream()))
+                                     _lib.HM_FLAG_DEVICE_PTRS | tf, _torch_stream()))
                 return X.t().reshape(y.shape)
         except ImportError:
             pass
         y = np.asarray(y, dtype=np.float64)
         B = np.asfortranarray(y.reshape(self.n, -1))
         X = np.zeros_like(B, order="F")
-        check(lib().hm_solve(self._h, _ptr(B), _ptr(X), B.shape[1], 0, None))
+        check(lib().hm_solve(self._h, _ptr(B), _ptr(X), B.shape[1], tf, None))
         return X.reshape(y.shape)
+
+    def solve_refined(self, y, tol=1e-10, max_iter=10, trans=False):
+        """H\\y with FP64 iterative refinement on the unfactorised H's matvec.
+        Returns (x, refinement steps, final max relative residual)."""
+        y = np.asarray(y, dtype=np.float64)
+        B = np.asfortranarray(y.reshape(self.n, -1))
+        X = np.zeros_like(B, order="F")
+        it = C.c_int32(0)
+        rr = C.c_double(0.0)
+        check(lib().hm_solve_refined(self._h, _ptr(B), _ptr(X), B.shape[1], float(tol), int(max_iter),
+                                     _lib.HM_FLAG_TRANS if trans else 0, None, C.byref(it), C.byref(rr)))
+        return X.reshape(y.shape), it.value, rr.value
 
 
 class _Identity:

@@ -19,6 +19,7 @@ HM_KERNEL_CAUCHY, HM_KERNEL_INVQUAD, HM_KERNEL_GAUSS = 1, 2, 3
 HM_CONS_ACA2, HM_CONS_SVD = 1, 2
 HM_F64, HM_F32, HM_BF16 = 0, 1, 2
 HM_FLAG_DEVICE_PTRS = 1
+HM_FLAG_TRANS = 2
 
 STATUS_NAMES = {
     1: "HM_ERR_ARG", 2: "HM_ERR_CUDA", 3: "HM_ERR_OOM", 4: "HM_ERR_STATE", 5: "HM_ERR_SINGULAR",
@@ -29,7 +30,8 @@ STATUS_NAMES = {
 EXPORTED = [
     "hm_version", "hm_last_error", "hm_default_params", "hm_new", "hm_destroy", "hm_info",
     "hm_leaves", "hm_leaf_factors", "hm_to_dense", "hm_matvec", "hm_matvec_profile", "hm_exact_rows",
-    "hm_add_identity", "hm_scale", "hm_copy", "hm_lu", "hm_lu_perm", "hm_solve", "aca_wrapper",
+    "hm_add_identity", "hm_scale", "hm_copy", "hm_lu", "hm_lu_perm", "hm_solve", "hm_solve_refined",
+    "aca_wrapper",
     "aca_wrapper_noalloc",
 ]
 
@@ -92,6 +94,8 @@ def lib():
     L.hm_lu.argtypes = [vp]
     L.hm_lu_perm.argtypes = [vp, vp]
     L.hm_solve.argtypes = [vp, vp, vp, C.c_int64, C.c_uint32, vp]
+    L.hm_solve_refined.argtypes = [vp, vp, vp, C.c_int64, C.c_double, C.c_int32, C.c_uint32, vp,
+                                   C.POINTER(C.c_int32), C.POINTER(C.c_double)]
     L.aca_wrapper.argtypes = [pd, pd, pd, C.c_int, C.c_int, C.c_double, C.c_int]
     L.aca_wrapper.restype = C.c_int
     L.aca_wrapper_noalloc.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_double, C.c_int, vp]

@@ -54,6 +54,7 @@ extern "C" {
 
 /* ---- flags ------------------------------------------------------------- */
 #define HM_FLAG_DEVICE_PTRS 1u
+#define HM_FLAG_TRANS       2u   /* hm_solve / hm_solve_refined: solve with H' */
 
 /* Mirror of the reference's global Params (src/utils.jl:8-24) restricted
  * to the fields the hot path reads, plus the device kernel description. */
@@ -175,9 +176,20 @@ int hm_lu(hm_handle* h);
 int hm_lu_perm(const hm_handle* h, int64_t* P);
 
 /* a\y (src/hlu.jl:553-562) with a factorised handle: X = H^{-1} B for ncols
- * right-hand sides (n x ncols column-major). */
+ * right-hand sides (n x ncols column-major).  With HM_FLAG_TRANS it solves
+ * H' X = B (U' then L', then the inverse row permutation), the adjoint that
+ * the reference does not have. */
 int hm_solve(hm_handle* h, const double* B, double* X, int64_t ncols,
              uint32_t flags, void* stream);
+
+/* H\y with iterative refinement: x = (LU)^{-1} b, then r = b - H x with the
+ * FP64 H-matvec of the unfactorised H (lu! keeps it), x += (LU)^{-1} r, until
+ * max over columns |r|/|b| <= tol or max_iter refinement steps.  *iters and
+ * *relres (may be NULL) report the steps taken and the final residual.
+ * No counterpart in the reference (its \ has no refinement). */
+int hm_solve_refined(hm_handle* h, const double* B, double* X, int64_t ncols,
+                     double tol, int32_t max_iter, uint32_t flags, void* stream,
+                     int32_t* iters, double* relres);
 
 /* Drop-in for the reference's native entry point
  * int aca_wrapper(double*, double*, double*, int, int, double, int)
