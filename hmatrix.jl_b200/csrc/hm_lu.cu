@@ -14,6 +14,7 @@
 #include "hm_internal.h"
 #include "hm_lowrank.cuh"
 
+#include <algorithm>
 #include <memory>
 #include <stdexcept>
 
@@ -50,11 +51,11 @@ struct LuError : std::runtime_error {
 // kernels
 // ---------------------------------------------------------------------------
 // C = alpha * A * B + beta * C   (A: m x k, B: k x n), FP64, 32x32 tiles
-__global__ void __launch_bounds__(256) lu_gemm_kernel(View A, View B, View C, double alpha, double beta) {
+__device__ __forceinline__ void gemm_tile(const View& A, const View& B, const View& C, double alpha, double beta,
+                                          int i0, int j0) {
   __shared__ double As[32][33];
   __shared__ double Bs[32][33];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
   const int m = C.rows, n = C.cols, kk = A.cols;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   for (int k0 = 0; k0 < kk; k0 += 32) {
@@ -80,6 +81,22 @@ __global__ void __launch_bounds__(256) lu_gemm_kernel(View A, View B, View C, do
       *c = (beta == 0.0) ? alpha * acc[u] : fma(alpha, acc[u], beta * *c);
     }
   }
+}
+
+__global__ void __launch_bounds__(256) lu_gemm_kernel(View A, View B, View C, double alpha, double beta) {
+  gemm_tile(A, B, C, alpha, beta, blockIdx.y * 32, blockIdx.x * 32);
+}
+
+// a batch of independent products, one job per blockIdx.z
+struct GemmJob {
+  View A, B, C;
+  double alpha, beta;
+};
+__global__ void __launch_bounds__(256) lu_gemm_batch_kernel(const GemmJob* __restrict__ jobs) {
+  const GemmJob& J = jobs[blockIdx.z];
+  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+  if (i0 >= J.C.rows || j0 >= J.C.cols) return;
+  gemm_tile(J.A, J.B, J.C, J.alpha, J.beta, i0, j0);
 }
 
 // Y = alpha * X + beta * Y (beta == 0: Y is not read)
@@ -224,7 +241,13 @@ struct GatherArgs {
   int32_t* r_out;
   int* flags;
 };
-__global__ void __launch_bounds__(256) lu_gather_pieces_kernel(GatherArgs g) {
+__device__ void gather_pieces(const GatherArgs& g);
+__global__ void __launch_bounds__(256) lu_gather_pieces_kernel(GatherArgs g) { gather_pieces(g); }
+__global__ void __launch_bounds__(256) lu_gather_pieces_batch_kernel(const GatherArgs* __restrict__ jobs) {
+  gather_pieces(jobs[blockIdx.x]);
+}
+
+__device__ void gather_pieces(const GatherArgs& g) {
   __shared__ int pre[MAX_PIECES + 1];
   if (threadIdx.x == 0) {
     int t = 0;
@@ -857,17 +880,382 @@ __global__ void lu_scatter_rows_kernel(View Xv, View W, const int64_t* __restric
   }
 }
 
+static BP build_from_handle(Ctx& c, const hm_handle* h, int32_t node);
+
+// ---------------------------------------------------------------------------
+// batched helpers
+// ---------------------------------------------------------------------------
+template <typename J>
+static J* upload_jobs(Ctx& c, Blk& owner, const std::vector<J>& v) {
+  J* d = (J*)dmalloc(c, owner, sizeof(J) * v.size());
+  if (cudaMemcpyAsync(d, v.data(), sizeof(J) * v.size(), cudaMemcpyHostToDevice, c.st) != cudaSuccess)
+    throw LuError(HM_ERR_CUDA, "job upload");
+  return d;
+}
+
+static void gemm_batch(Ctx& c, const std::vector<GemmJob>& jobs) {
+  if (jobs.empty()) return;
+  int gx = 1, gy = 1;
+  for (auto& j : jobs) {
+    gx = std::max(gx, (j.C.cols + 31) / 32);
+    gy = std::max(gy, (j.C.rows + 31) / 32);
+  }
+  for (size_t b = 0; b < jobs.size(); b += 65535) {
+    const size_t nb = std::min<size_t>(65535, jobs.size() - b);
+    Blk tmp;
+    tmp.st = c.st;
+    std::vector<GemmJob> part(jobs.begin() + b, jobs.begin() + b + nb);
+    GemmJob* d = upload_jobs(c, tmp, part);
+    lu_gemm_batch_kernel<<<dim3(gx, gy, (unsigned)nb), 256, 0, c.st>>>(d);
+    LU_LAUNCH_CHECK();
+  }
+}
+
+// one low-rank target = truncated sum of its pieces
+struct RcReq {
+  Piece pc[2];
+  int np;
+  double* outA; int64_t ldoa;
+  double* outB; int64_t ldob;
+  int32_t* k;
+  int m, n, kcap;
+};
+
+static void recompress_batch(Ctx& c, const std::vector<RcReq>& reqs, int rmax) {
+  if (reqs.empty()) return;
+  rmax = std::min(std::max(rmax, 1), RCORE_MAX);
+  size_t b = 0;
+  while (b < reqs.size()) {
+    size_t e = b, elems = 0;
+    while (e < reqs.size() && (e == b || elems + (size_t)(reqs[e].m + reqs[e].n) * rmax < (size_t)1 << 27)) {
+      elems += (size_t)(reqs[e].m + reqs[e].n) * rmax;
+      ++e;
+    }
+    Blk tmp;
+    tmp.st = c.st;
+    double* scratch = (double*)dmalloc(c, tmp, sizeof(double) * elems);
+    int32_t* rr = (int32_t*)dmalloc(c, tmp, sizeof(int32_t) * (e - b));
+    std::vector<GatherArgs> ga(e - b);
+    std::vector<CoreJob> cj(e - b);
+    size_t off = 0;
+    for (size_t q = b; q < e; ++q) {
+      const RcReq& R = reqs[q];
+      GatherArgs& g = ga[q - b];
+      g = GatherArgs{};
+      for (int p = 0; p < R.np; ++p) g.pc[p] = R.pc[p];
+      g.np = R.np;
+      g.SA = scratch + off;
+      g.SB = scratch + off + (size_t)R.m * rmax;
+      g.M = R.m; g.N = R.n; g.rmax = rmax; g.r_out = rr + (q - b); g.flags = c.flags;
+      CoreJob& J = cj[q - b];
+      J = CoreJob{};
+      J.A = g.SA; J.B = g.SB; J.outA = R.outA; J.outB = R.outB;
+      J.m = R.m; J.n = R.n; J.lda = std::max(R.m, 1); J.ldb = std::max(R.n, 1);
+      J.ldoa = (int32_t)R.ldoa; J.ldob = (int32_t)R.ldob; J.kcap = R.kcap;
+      J.zero_test = 1; J.rank = R.k; J.r_dev = g.r_out; J.zero_fill = 1;
+      off += (size_t)(R.m + R.n) * rmax;
+    }
+    GatherArgs* dg = upload_jobs(c, tmp, ga);
+    CoreJob* dc = upload_jobs(c, tmp, cj);
+    lu_gather_pieces_batch_kernel<<<(unsigned)(e - b), 256, 0, c.st>>>(dg);
+    LU_LAUNCH_CHECK();
+    int s = launch_core_recompress(dc, (int)(e - b), rmax, c.eps_trunc, c.flags, c.st);
+    if (s != HM_OK) throw LuError(s, "batched recompression launch");
+    b = e;
+  }
+}
+
+// H_tile += s * A B' for an H-structured diagonal tile, as jobs: dense leaves
+// get a product, low-rank leaves a recompression (hmat_add! of H += Rk splits
+// the low-rank term over the children, src/harithm.jl:129-142)
+static void tile_add_lowrank(const Blk& H, int r0, int c0, const double* A, int64_t lda, const double* B,
+                             int64_t ldb, const int32_t* k, int cap, double s, std::vector<GemmJob>& gj,
+                             std::vector<RcReq>& rj) {
+  if (H.type == T_DENSE) {
+    GemmJob g{};
+    g.A = View{const_cast<double*>(A) + r0, 1, lda, H.m, cap};
+    g.B = vtr(View{const_cast<double*>(B) + c0, 1, ldb, H.n, cap});
+    g.C = H.Cv();
+    g.alpha = s;
+    g.beta = 1.0;
+    gj.push_back(g);
+  } else if (H.type == T_RK) {
+    RcReq R{};
+    R.pc[0] = Piece{H.A, H.lda, H.B, H.ldb, H.k, H.m, H.n, 0, 0, 1.0};
+    R.pc[1] = Piece{A + r0, lda, B + c0, ldb, k, H.m, H.n, 0, 0, s};
+    R.np = 2;
+    R.outA = H.A; R.ldoa = H.lda; R.outB = H.B; R.ldob = H.ldb; R.k = H.k;
+    R.m = H.m; R.n = H.n; R.kcap = H.cap;
+    rj.push_back(R);
+  } else {
+    const int m = H.ch[0]->m, n = H.ch[0]->n;
+    tile_add_lowrank(*H.ch[0], r0, c0, A, lda, B, ldb, k, cap, s, gj, rj);
+    tile_add_lowrank(*H.ch[1], r0, c0 + n, A, lda, B, ldb, k, cap, s, gj, rj);
+    tile_add_lowrank(*H.ch[2], r0 + m, c0, A, lda, B, ldb, k, cap, s, gj, rj);
+    tile_add_lowrank(*H.ch[3], r0 + m, c0 + n, A, lda, B, ldb, k, cap, s, gj, rj);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tile LU.  When every leaf outside the diagonal tiles (row group x column
+// group blocks) is one low-rank block covering its whole tile -- the
+// partition of the aca2 route with the identity adjacency -- the recursion of
+// lu! is carried out tile by tile (right-looking), which performs the same
+// operations with leaf-local pivoting but batches them: per step k the
+// diagonal tile is factorised by the recursion above, the whole row panel
+// (A factors of tiles (k, j>k)) and column panel (B factors of tiles (i>k, k))
+// are solved as one wide triangular solve each, every core B_ik' A_kj comes
+// out of one GEMM, and all updates of the trailing tiles run as one batched
+// product + one batched recompression.  Updates are truncated per step (the
+// recursion sums some products before truncating); both stay within
+// eps_trunc of the exact Schur complement.
+// ---------------------------------------------------------------------------
+struct TileLU {
+  int T = 0;
+  std::vector<int64_t> start, size;      // tile ranges
+  std::vector<BP> diag;                  // diagonal tiles (H or dense)
+  std::vector<double*> Ap, Bp;           // row panels (m_i x T*cap), column panels (n_j x T*cap)
+  int32_t* kmat = nullptr;               // ranks of the off-diagonal tiles, T x T
+  BP hold;                               // owns the panel memory
+  double* Ai(int i, int j, int cap) const { return Ap[i] + (int64_t)j * cap * size[i]; }
+  double* Bj(int i, int j, int cap) const { return Bp[j] + (int64_t)i * cap * size[j]; }
+};
+
+// tile structure of the handle, or false when the partition has no such level
+static bool tile_structure(const hm_handle* h, std::vector<int32_t>& gcl, std::vector<int32_t>& diag_node) {
+  const int64_t ncl = (int64_t)h->cl_s.size();
+  std::vector<char> is_row(ncl, 0);
+  for (auto& L : h->leaves) is_row[L.s] = 1;
+  std::vector<char> covered(ncl, 0);
+  gcl.clear();
+  for (int64_t c = 0; c < ncl; ++c) {
+    if (!covered[c] && is_row[c]) gcl.push_back((int32_t)c);
+    if (h->cl_left[c] >= 0) {
+      const char cv = covered[c] || is_row[c];
+      covered[h->cl_left[c]] = cv;
+      covered[h->cl_right[c]] = cv;
+    }
+  }
+  std::sort(gcl.begin(), gcl.end(), [&](int32_t a, int32_t b) { return h->cl_s[a] < h->cl_s[b]; });
+  const int T = (int)gcl.size();
+  if (T < 2) return false;
+  std::vector<int64_t> st(T);
+  for (int i = 0; i < T; ++i) st[i] = h->cl_s[gcl[i]];
+  auto tile_of = [&](int64_t r) { return (int)(std::upper_bound(st.begin(), st.end(), r) - st.begin()) - 1; };
+  for (auto& L : h->leaves) {
+    const int i = tile_of(L.row0), j = tile_of(L.col0);
+    if (i == j) continue;
+    if (L.type != T_RK || L.s != gcl[i] || L.t != gcl[j]) return false;
+  }
+  diag_node.assign(T, -1);
+  std::vector<int32_t> tile_of_cluster(ncl, -1);
+  for (int i = 0; i < T; ++i) tile_of_cluster[gcl[i]] = i;
+  for (int32_t id = 0; id < (int32_t)h->nodes.size(); ++id) {
+    const Node& nd = h->nodes[id];
+    if (nd.s == nd.t && tile_of_cluster[nd.s] >= 0) diag_node[tile_of_cluster[nd.s]] = id;
+  }
+  for (int i = 0; i < T; ++i)
+    if (diag_node[i] < 0) return false;
+  return true;
+}
+
+static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vector<int32_t>& gcl,
+                        const std::vector<int32_t>& dnode) {
+  const int T = (int)gcl.size(), cap = c.cap;
+  TL.T = T;
+  TL.start.resize(T);
+  TL.size.resize(T);
+  for (int i = 0; i < T; ++i) {
+    TL.start[i] = h->cl_s[gcl[i]];
+    TL.size[i] = h->cl_e[gcl[i]] - h->cl_s[gcl[i]];
+  }
+  TL.hold = std::make_shared<Blk>();
+  TL.hold->st = c.st;
+  TL.Ap.resize(T);
+  TL.Bp.resize(T);
+  for (int i = 0; i < T; ++i) {
+    TL.Ap[i] = (double*)dmalloc(c, *TL.hold, sizeof(double) * TL.size[i] * T * cap);
+    TL.Bp[i] = (double*)dmalloc(c, *TL.hold, sizeof(double) * TL.size[i] * T * cap);
+  }
+  TL.kmat = (int32_t*)dmalloc(c, *TL.hold, sizeof(int32_t) * T * T);
+  if (cudaMemsetAsync(TL.kmat, 0, sizeof(int32_t) * T * T, c.st) != cudaSuccess) throw LuError(HM_ERR_CUDA, "memset");
+  // load the off-diagonal tiles into the panels and the diagonal tiles as trees
+  const int eb = elem_bytes(h->storage);
+  std::vector<int32_t> kh(T * T, 0);
+  auto tile_of = [&](int64_t r) {
+    return (int)(std::upper_bound(TL.start.begin(), TL.start.end(), r) - TL.start.begin()) - 1;
+  };
+  for (auto& L : h->leaves) {
+    const int i = tile_of(L.row0), j = tile_of(L.col0);
+    if (i == j) continue;
+    if (L.k > cap) throw LuError(HM_ERR_RANK, "leaf rank above the H-LU rank capacity");
+    kh[i * T + j] = L.k;
+    const int64_t npad = col_pad(L.n, eb), mpad = col_pad(L.m, eb);
+    auto load = [&](int64_t off, int64_t ld, int rows, double* dst) {
+      unsigned g = (unsigned)std::min<int64_t>(((int64_t)rows * cap + 255) / 256, 1024);
+      switch (h->storage) {
+        case HM_F64: lu_load_kernel<double><<<g, 256, 0, c.st>>>((const double*)h->d_rk + off, ld, rows, L.k, dst, rows, cap); break;
+        case HM_F32: lu_load_kernel<float><<<g, 256, 0, c.st>>>((const float*)h->d_rk + off, ld, rows, L.k, dst, rows, cap); break;
+        default: lu_load_kernel<__nv_bfloat16><<<g, 256, 0, c.st>>>((const __nv_bfloat16*)h->d_rk + off, ld, rows, L.k, dst, rows, cap);
+      }
+      LU_LAUNCH_CHECK();
+    };
+    load(L.off, npad, L.n, TL.Bj(i, j, cap));
+    load(L.off + npad * L.k, mpad, L.m, TL.Ai(i, j, cap));
+  }
+  if (cudaMemcpyAsync(TL.kmat, kh.data(), sizeof(int32_t) * T * T, cudaMemcpyHostToDevice, c.st) != cudaSuccess)
+    throw LuError(HM_ERR_CUDA, "rank upload");
+  cudaStreamSynchronize(c.st);       // kh leaves scope before the async copy otherwise
+  TL.diag.resize(T);
+  for (int i = 0; i < T; ++i) TL.diag[i] = build_from_handle(c, h, dnode[i]);
+
+  for (int k = 0; k < T; ++k) {
+    const int mk = (int)TL.size[k];
+    const int R = (T - k - 1) * cap;
+    lu_rec(c, *TL.diag[k]);
+    if (k > 0) laswp(c, View{TL.Ap[k], 1, mk, mk, k * cap}, TL.start[k]);
+    if (R == 0) break;
+    View Ua{TL.Ai(k, k + 1, cap), 1, mk, mk, R};          // A factors of tiles (k, j>k)
+    View Lb{TL.Bj(k + 1, k, cap), 1, mk, mk, R};          // B factors of tiles (i>k, k)
+    laswp(c, Ua, TL.start[k]);
+    mfs(c, *TL.diag[k], Ua, true, true);                  // L_kk^{-1} P_k A_kj
+    mfs(c, *TL.diag[k], vtr(Lb), false, false);           // B_ik' U_kk^{-1}
+    Blk tmp;
+    tmp.st = c.st;
+    double* W = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)R * R);
+    View Wv{W, 1, R, R, R};
+    gemm(c, Wv, vtr(Lb), Ua, 1.0, 0.0);                   // W_ij = B_ik' A_kj
+    // Q_i = A_ik W_i,:   (m_i x R) for every trailing tile row i
+    std::vector<double*> Q(T, nullptr);
+    std::vector<GemmJob> gq;
+    for (int i = k + 1; i < T; ++i) {
+      const int mi = (int)TL.size[i];
+      Q[i] = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)mi * R);
+      GemmJob g{};
+      g.A = View{TL.Ai(i, k, cap), 1, mi, mi, cap};
+      g.B = vsub(Wv, (i - k - 1) * cap, 0, cap, R);
+      g.C = View{Q[i], 1, mi, mi, R};
+      g.alpha = 1.0; g.beta = 0.0;
+      gq.push_back(g);
+    }
+    gemm_batch(c, gq);
+    std::vector<RcReq> rj;
+    std::vector<GemmJob> gd;
+    for (int i = k + 1; i < T; ++i) {
+      const int mi = (int)TL.size[i];
+      for (int j = k + 1; j < T; ++j) {
+        const int nj = (int)TL.size[j];
+        const double* Qij = Q[i] + (int64_t)(j - k - 1) * cap * mi;
+        const int32_t* kkj = TL.kmat + k * T + j;
+        if (i == j) {
+          tile_add_lowrank(*TL.diag[i], 0, 0, Qij, mi, TL.Bj(k, i, cap), nj, kkj, cap, -1.0, gd, rj);
+        } else {
+          RcReq Rq{};
+          Rq.pc[0] = Piece{TL.Ai(i, j, cap), mi, TL.Bj(i, j, cap), nj, TL.kmat + i * T + j, mi, nj, 0, 0, 1.0};
+          Rq.pc[1] = Piece{Qij, mi, TL.Bj(k, j, cap), nj, kkj, mi, nj, 0, 0, -1.0};
+          Rq.np = 2;
+          Rq.outA = TL.Ai(i, j, cap); Rq.ldoa = mi;
+          Rq.outB = TL.Bj(i, j, cap); Rq.ldob = nj;
+          Rq.k = TL.kmat + i * T + j;
+          Rq.m = mi; Rq.n = nj; Rq.kcap = cap;
+          rj.push_back(Rq);
+        }
+      }
+    }
+    gemm_batch(c, gd);
+    recompress_batch(c, rj, 2 * cap);
+  }
+}
+
+// y = P b, forward (unit L), backward (U) tile by tile; trans: U' then L'
+static void tile_solve(Ctx& c, const TileLU& TL, View X, bool trans) {
+  const int T = TL.T, cap = c.cap, nc = X.cols;
+  auto yv = [&](int i) { return vsub(X, (int)TL.start[i], 0, (int)TL.size[i], nc); };
+  Blk tmp;
+  tmp.st = c.st;
+  double* Z = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)T * cap * nc);
+  if (!trans) {
+    for (int k = 0; k < T; ++k) {                       // L y = b
+      solve_rec(c, *TL.diag[k], yv(k), true);
+      const int R = (T - k - 1) * cap;
+      if (R == 0) break;
+      View Zv{Z, 1, R, R, nc};
+      gemm(c, Zv, vtr(View{TL.Bj(k + 1, k, cap), 1, TL.size[k], (int)TL.size[k], R}), yv(k), 1.0, 0.0);
+      std::vector<GemmJob> g;
+      for (int i = k + 1; i < T; ++i)
+        g.push_back(GemmJob{View{TL.Ai(i, k, cap), 1, TL.size[i], (int)TL.size[i], cap},
+                            vsub(Zv, (i - k - 1) * cap, 0, cap, nc), yv(i), -1.0, 1.0});
+      gemm_batch(c, g);
+    }
+    for (int k = T - 1; k >= 0; --k) {                  // U x = y
+      const int R = (T - k - 1) * cap;
+      if (R > 0) {
+        View Zv{Z, 1, R, R, nc};
+        std::vector<GemmJob> g;
+        for (int j = k + 1; j < T; ++j)
+          g.push_back(GemmJob{vtr(View{TL.Bj(k, j, cap), 1, TL.size[j], (int)TL.size[j], cap}), yv(j),
+                              vsub(Zv, (j - k - 1) * cap, 0, cap, nc), 1.0, 0.0});
+        gemm_batch(c, g);
+        gemm(c, yv(k), View{TL.Ai(k, k + 1, cap), 1, TL.size[k], (int)TL.size[k], R}, Zv, -1.0, 1.0);
+      }
+      solve_rec(c, *TL.diag[k], yv(k), false);
+    }
+  } else {
+    for (int k = 0; k < T; ++k) {                       // U' z = b
+      solve_t_rec(c, *TL.diag[k], yv(k), true);
+      const int R = (T - k - 1) * cap;
+      if (R == 0) break;
+      View Zv{Z, 1, R, R, nc};
+      gemm(c, Zv, vtr(View{TL.Ai(k, k + 1, cap), 1, TL.size[k], (int)TL.size[k], R}), yv(k), 1.0, 0.0);
+      std::vector<GemmJob> g;
+      for (int j = k + 1; j < T; ++j)
+        g.push_back(GemmJob{View{TL.Bj(k, j, cap), 1, TL.size[j], (int)TL.size[j], cap},
+                            vsub(Zv, (j - k - 1) * cap, 0, cap, nc), yv(j), -1.0, 1.0});
+      gemm_batch(c, g);
+    }
+    for (int k = T - 1; k >= 0; --k) {                  // L' w = z
+      const int R = (T - k - 1) * cap;
+      if (R > 0) {
+        View Zv{Z, 1, R, R, nc};
+        std::vector<GemmJob> g;
+        for (int i = k + 1; i < T; ++i)
+          g.push_back(GemmJob{vtr(View{TL.Ai(i, k, cap), 1, TL.size[i], (int)TL.size[i], cap}), yv(i),
+                              vsub(Zv, (i - k - 1) * cap, 0, cap, nc), 1.0, 0.0});
+        gemm_batch(c, g);
+        gemm(c, yv(k), View{TL.Bj(k + 1, k, cap), 1, TL.size[k], (int)TL.size[k], R}, Zv, -1.0, 1.0);
+      }
+      solve_t_rec(c, *TL.diag[k], yv(k), false);
+    }
+  }
+}
+
+static void tile_densify(Ctx& c, const TileLU& TL, View D) {
+  const int T = TL.T, cap = c.cap;
+  std::vector<GemmJob> g;
+  for (int i = 0; i < T; ++i)
+    for (int j = 0; j < T; ++j) {
+      View blk = vsub(D, (int)TL.start[i], (int)TL.start[j], (int)TL.size[i], (int)TL.size[j]);
+      if (i == j) densify_into(c, blk, *TL.diag[i]);
+      else
+        g.push_back(GemmJob{View{TL.Ai(i, j, cap), 1, TL.size[i], (int)TL.size[i], cap},
+                            vtr(View{TL.Bj(i, j, cap), 1, TL.size[j], (int)TL.size[j], cap}), blk, 1.0, 0.0});
+    }
+  gemm_batch(c, g);
+}
+
 // ---------------------------------------------------------------------------
 // state, entry points
 // ---------------------------------------------------------------------------
 struct LuState {
-  BP root;
+  BP root;                       // recursive format
+  std::unique_ptr<TileLU> tile;  // tile format
   int64_t* P = nullptr;
   int* flags = nullptr;
   int cap = 0;
   cudaStream_t st = nullptr;
   ~LuState() {
     root.reset();
+    tile.reset();
     if (P) cudaFreeAsync(P, st);
     if (flags) cudaFreeAsync(flags, st);
     if (st) cudaStreamSynchronize(st);
@@ -937,10 +1325,19 @@ int lu_factor(hm_handle* h) {
   HM_CUDA_TRY(cudaMallocAsync((void**)&S->flags, sizeof(int), h->stream));
   HM_CUDA_TRY(cudaMemsetAsync(S->flags, 0, sizeof(int), h->stream));
   Ctx c{h->stream, S->cap, S->P, S->flags, h->prm.eps_trunc, h};
+  const int mode = h->prm.lu_mode;     // 0 auto, 1 recursion, 2 tiles
   try {
     if (h->kmax > S->cap) throw LuError(HM_ERR_RANK, "a leaf rank exceeds the H-LU rank capacity");
-    S->root = build_from_handle(c, h, 0);
-    lu_rec(c, *S->root);
+    std::vector<int32_t> gcl, dnode;
+    const bool tiled = mode != 1 && tile_structure(h, gcl, dnode);
+    if (mode == 2 && !tiled) throw LuError(HM_ERR_UNSUPPORTED, "the partition has no tile level");
+    if (tiled) {
+      S->tile.reset(new TileLU());
+      tile_factor(c, h, *S->tile, gcl, dnode);
+    } else {
+      S->root = build_from_handle(c, h, 0);
+      lu_rec(c, *S->root);
+    }
   } catch (const LuError& e) {
     cudaStreamSynchronize(h->stream);
     delete S;
@@ -970,16 +1367,24 @@ int lu_solve_device(hm_handle* h, const double* d_b, double* d_x, int64_t ncols,
       // a\y (src/hlu.jl:553-562): permute!(w, P), unit-L forward, U backward
       lu_gather_rows_kernel<<<g, 256, 0, st>>>(X, B, S->P);
       LU_LAUNCH_CHECK();
-      solve_rec(c, *S->root, X, true);
-      solve_rec(c, *S->root, X, false);
+      if (S->tile) {
+        tile_solve(c, *S->tile, X, false);
+      } else {
+        solve_rec(c, *S->root, X, true);
+        solve_rec(c, *S->root, X, false);
+      }
     } else {
       Blk tmp;
       tmp.st = st;
       double* w = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)tot);
       View W{w, 1, h->n, (int)h->n, (int)ncols};
       axpby(c, W, B, 1.0, 0.0);
-      solve_t_rec(c, *S->root, W, true);
-      solve_t_rec(c, *S->root, W, false);
+      if (S->tile) {
+        tile_solve(c, *S->tile, W, true);
+      } else {
+        solve_t_rec(c, *S->root, W, true);
+        solve_t_rec(c, *S->root, W, false);
+      }
       lu_scatter_rows_kernel<<<g, 256, 0, st>>>(X, W, S->P);
       LU_LAUNCH_CHECK();
     }
@@ -1074,7 +1479,9 @@ int lu_to_dense(const hm_handle* h, double* d_out) {
   if (!h->lu) return fail(HM_ERR_STATE, "a has not been factorized");
   Ctx c{h->stream, h->lu->cap, h->lu->P, h->lu->flags, h->prm.eps_trunc, h};
   try {
-    densify_into(c, View{d_out, 1, h->n, (int)h->n, (int)h->n}, *h->lu->root);
+    View D{d_out, 1, h->n, (int)h->n, (int)h->n};
+    if (h->lu->tile) tile_densify(c, *h->lu->tile, D);
+    else densify_into(c, D, *h->lu->root);
   } catch (const LuError& e) {
     return fail(e.code, e.what());
   }
@@ -1099,7 +1506,34 @@ int lu_copy(const hm_handle* src, hm_handle* dst) {
   HM_CUDA_TRY(cudaMemsetAsync(S->flags, 0, sizeof(int), dst->stream));
   Ctx c{dst->stream, S->cap, S->P, S->flags, src->prm.eps_trunc, src};
   try {
-    S->root = copy_blk(c, *src->lu->root);
+    if (src->lu->tile) {
+      const TileLU& A = *src->lu->tile;
+      TileLU* B = new TileLU();
+      S->tile.reset(B);
+      B->T = A.T;
+      B->start = A.start;
+      B->size = A.size;
+      B->hold = std::make_shared<Blk>();
+      B->hold->st = c.st;
+      B->Ap.resize(A.T);
+      B->Bp.resize(A.T);
+      for (int i = 0; i < A.T; ++i) {
+        const size_t bytes = sizeof(double) * A.size[i] * A.T * S->cap;
+        B->Ap[i] = (double*)dmalloc(c, *B->hold, bytes);
+        B->Bp[i] = (double*)dmalloc(c, *B->hold, bytes);
+        if (cudaMemcpyAsync(B->Ap[i], A.Ap[i], bytes, cudaMemcpyDeviceToDevice, c.st) != cudaSuccess ||
+            cudaMemcpyAsync(B->Bp[i], A.Bp[i], bytes, cudaMemcpyDeviceToDevice, c.st) != cudaSuccess)
+          throw LuError(HM_ERR_CUDA, "panel copy");
+      }
+      B->kmat = (int32_t*)dmalloc(c, *B->hold, sizeof(int32_t) * A.T * A.T);
+      if (cudaMemcpyAsync(B->kmat, A.kmat, sizeof(int32_t) * A.T * A.T, cudaMemcpyDeviceToDevice, c.st) !=
+          cudaSuccess)
+        throw LuError(HM_ERR_CUDA, "rank copy");
+      B->diag.resize(A.T);
+      for (int i = 0; i < A.T; ++i) B->diag[i] = copy_blk(c, *A.diag[i]);
+    } else {
+      S->root = copy_blk(c, *src->lu->root);
+    }
   } catch (const LuError& e) {
     delete S;
     return fail(e.code, e.what());

@@ -56,6 +56,7 @@ class Params:
     Shift: float = 0.0                    # lambda of H + lambda*I applied at construction
     Device: int = 0
     RankCap: int = 0                      # rank capacity during H-LU (0: automatic)
+    LuMode: str = "auto"                  # "auto" | "recursive" (lu! as written) | "tiles"
 
 
 Hparams = Params()
@@ -96,6 +97,7 @@ def _params_struct(prm: Params, dim: int):
     p.storage = prm.Storage
     p.device = prm.Device
     p.rank_cap = prm.RankCap
+    p.lu_mode = {"auto": 0, "recursive": 1, "tiles": 2}[prm.LuMode]
     return p
 
 

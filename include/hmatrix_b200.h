@@ -73,7 +73,10 @@ typedef struct hm_params {
     int32_t storage;      /* HM_F64 / HM_F32 / HM_BF16                        */
     int32_t device;       /* CUDA device ordinal                              */
     int32_t rank_cap;     /* capacity of low-rank blocks during H-LU (0: auto) */
-    int32_t reserved[6];
+    int32_t lu_mode;      /* H-LU schedule: 0 auto, 1 the recursion of lu!,
+                             2 tile by tile (needs a level where every block
+                             outside the diagonal tiles is one low-rank block) */
+    int32_t reserved[5];
 } hm_params;
 
 /* info(H) of src/utils.jl:83-110 plus the byte counts used for rooflines. */

@@ -19,9 +19,9 @@ def golden():
     return np.load(os.path.join(ROOT, "tests", "golden", "readme_case.npz"))
 
 
-def readme(hm, mr):
+def readme(hm, mr, mode="recursive"):
     return hm.Params(Geom=np.linspace(0, 10, 2000), Kernel=hm.Cauchy(1.0), MaxBlock=500, MinBlock=64,
-                     MaxRank=mr, ConsMethod="svd")
+                     MaxRank=mr, ConsMethod="svd", LuMode=mode)
 
 
 def close(a, b, rtol):
@@ -128,20 +128,45 @@ def test_lu2_2d():
     assert close(L.solve(y), np.linalg.solve(Hs.to_dense(), y), SQRT_EPS)
 
 
-def test_aca2_route_lu_solve_multi_rhs():
-    # aca2 construction (Adj = I) with a diagonal shift, several right-hand sides
+@pytest.mark.parametrize("mode", ["recursive", "tiles"])
+def test_aca2_route_lu_solve_multi_rhs(mode):
+    # aca2 construction (Adj = I) with a diagonal shift, several right-hand sides;
+    # this partition has a tile level, so both schedules apply
     import hmatrix as hm
     n = 4096
     prm = hm.Params(Geom=np.linspace(0, 10, n), Kernel=hm.Cauchy(1.0), MaxBlock=512, MinBlock=64, MaxRank=16,
-                    ConsMethod="aca2", εComp=1e-10, Tree="bisect", Shift=1.0)
+                    ConsMethod="aca2", εComp=1e-10, Tree="bisect", Shift=1.0, LuMode=mode)
     c, H = hm.NewHmat(prm)
     D = H.to_dense()
     L = hm.lu(H)
     F = L.to_dense()
+    assert leaf_local(L.P, H.leaves())
     assert np.abs(hm.getl(F) @ hm.getu(F) - D[L.P]).max() < 1e-8
     B = np.random.default_rng(4).standard_normal((n, 3))
     X = L.solve(B)
     assert close(X, np.linalg.solve(D, B), 1e-9)
+    assert close(L.solve(B, trans=True), np.linalg.solve(D.T, B), 1e-9)
+    Xr, it, rr = L.solve_refined(B, tol=1e-13, max_iter=5)
+    assert rr <= 1e-13 and close(Xr, np.linalg.solve(D, B), 1e-12)
+
+
+def test_tiles_match_recursion_kmeans_tree():
+    # the tile schedule on a KMeans tree (uneven tiles) against the recursion
+    import hmatrix as hm
+    n = 6000
+    out = {}
+    for mode in ("recursive", "tiles"):
+        prm = hm.Params(Geom=np.linspace(0, 10, n), Kernel=hm.Cauchy(1.0), MaxBlock=512, MinBlock=64,
+                        MaxRank=16, ConsMethod="aca2", εComp=1e-10, Tree="kmeans", Shift=1.0, LuMode=mode)
+        c, H = hm.NewHmat(prm)
+        L = hm.lu(H)
+        y = np.random.default_rng(8).standard_normal(n)
+        out[mode] = (L.P, L.solve(y), H.to_dense(), y)
+    P1, x1, D, y = out["recursive"]
+    P2, x2, _, _ = out["tiles"]
+    assert np.array_equal(P1, P2)                  # well conditioned: same pivots
+    assert close(x1, x2, 1e-9)
+    assert close(x2, np.linalg.solve(D, y), 1e-9)
 
 
 def test_lu_state_errors():
