@@ -50,6 +50,8 @@ def parse():
                     help="also measure FP32 and BF16 factor storage")
     ap.add_argument("--cpu-rows", type=int, default=4096, help="rows of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-lu", action="store_true", help="skip the H-LU + solve leg")
+    ap.add_argument("--lu-n", type=int, default=1 << 16, help="size of the H-LU + solve leg")
     return ap.parse_args()
 
 
@@ -187,6 +189,23 @@ def build(n, storage):
     return c, H, time.perf_counter() - t0
 
 
+def job_time(ms_local, dist, device):
+    """Time of the whole job: the max over ranks of each rank's own time (the
+    job ends when the slowest replica does).  `device` is "cuda" under NCCL
+    and "cpu" under gloo."""
+    if dist is None:
+        return ms_local
+    import torch
+    t = torch.tensor([ms_local], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(bytes_per_rank, world, ms):
+    """Whole-job throughput in GB/s: every rank streams its own replica."""
+    return world * bytes_per_rank / (ms * 1e-3) / 1e9
+
+
 def measure(H, a, torch, dist, world):
     import ctypes as C
     from hmatrix import _lib
@@ -226,11 +245,8 @@ def measure(H, a, torch, dist, world):
     e1.record(st)
     torch.cuda.synchronize()
     ck = clocks.stop()
-    ms = e0.elapsed_time(e1) / a.steps
+    ms = job_time(e0.elapsed_time(e1) / a.steps, dist, "cuda")
     if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     # end to end through the C ABI with host pinned buffers
     xh = x.cpu().pin_memory()
@@ -242,17 +258,44 @@ def measure(H, a, torch, dist, world):
     ke = max(3, a.steps // 2)
     for _ in range(ke):
         _lib.check(L.hm_matvec(H._h, C.c_void_p(xh.data_ptr()), C.c_void_p(yh.data_ptr()), 1, 0, 0, None))
-    e2e_ms = (time.perf_counter() - t0) / ke * 1e3
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = job_time((time.perf_counter() - t0) / ke * 1e3, dist, "cuda")
     # accuracy: 4096 sampled rows against exact FP64 kernel rows (dense oracle)
     rows = np.sort(np.random.default_rng(2).choice(n, 4096, replace=False))
     ex = H.exact_rows(rows, x.cpu().numpy())
     got = y.cpu().numpy()[rows]
     rel = float(np.linalg.norm(got - ex) / np.linalg.norm(ex))
     return ms, ph, ck, e2e_ms, rel
+
+
+def lu_solve_leg(n, torch):
+    """H-LU + H\\y on the largest problem of the batched 1-D configuration
+    (n points on [0,10], 1/(1+(x-y)^2) + delta_xy, MaxBlock 256, MinBlock 32,
+    MaxRank 12, one N(0,1) right-hand side): the FP64 factorisation as in the
+    reference (eps_trunc 1e-10) against a cheaper low-accuracy factorisation
+    (eps_trunc 1e-6 inside the LU), both refined with the FP64 H-matvec to a
+    relative residual <= 1e-10."""
+    import hmatrix as hm
+    out = {"config": {"n": n, "kernel": "1/(1+(x-y)^2) + delta_xy", "MaxBlock": 256, "MinBlock": 32,
+                      "MaxRank": 12, "aca_tol": 1e-10, "target_relres": 1e-10, "tree": "median bisection"}}
+    y = np.random.default_rng(3).standard_normal(n)
+    for name, epslu in (("fp64", 0.0), ("mixed", 1e-6)):
+        prm = hm.Params(Geom=np.linspace(0, 10, n), Kernel=hm.Cauchy(1.0), MaxBlock=256, MinBlock=32,
+                        MaxRank=12, ConsMethod="aca2", εComp=1e-10, Tree="bisect", Shift=1.0, εTruncLU=epslu,
+                        Device=torch.cuda.current_device())
+        c, H = hm.NewHmat(prm)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L = hm.lu(H)
+        t1 = time.perf_counter()
+        x, it, rr = L.solve_refined(y, tol=1e-10, max_iter=20)
+        t2 = time.perf_counter()
+        r = H * x - y
+        out[name] = {"lu_s": t1 - t0, "solve_refined_s": t2 - t1, "total_s": t2 - t0, "refine_steps": it,
+                     "relres": float(np.linalg.norm(r) / np.linalg.norm(y)), "eps_trunc_lu": epslu or 1e-10}
+        del L, H
+        torch.cuda.empty_cache()
+    out["mixed_speedup"] = out["fp64"]["total_s"] / out["mixed"]["total_s"]
+    return out
 
 
 def run_ours(a):
@@ -273,8 +316,8 @@ def run_ours(a):
     eb = {"f64": 8, "f32": 4, "bf16": 2}[a.storage]
     deb = 8 if a.storage == "f64" else 4
     bytes_mv = eb * info.rk_entries + deb * info.dense_entries + 16 * a.n
-    value = world * bytes_mv / (ms * 1e-3) / 1e9
-    e2e = world * bytes_mv / (e2e_ms * 1e-3) / 1e9
+    value = job_value(bytes_mv, world, ms)
+    e2e = job_value(bytes_mv, world, e2e_ms)
     peak, peak_kind = peaks()
     # dominant kernel: the phase with the larger device time; its algorithmic
     # bytes: phase 1 streams the B factors (+x segments from L2), phase 2 the
@@ -305,6 +348,11 @@ def run_ours(a):
             del H2
             H = None
             torch.cuda.empty_cache()
+    lu = None
+    if not a.no_lu and world == 1:
+        H = None
+        torch.cuda.empty_cache()
+        lu = lu_solve_leg(a.lu_n, torch)
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -331,7 +379,8 @@ def run_ours(a):
             "structure": {"n_rk": info.n_rk, "n_dense": info.n_dense, "rk_entries": info.rk_entries,
                           "dense_entries": info.dense_entries, "max_rank": info.max_rank,
                           "algorithmic_bytes": bytes_mv, "build_s": t_build},
-            "extra_precisions": extra or None}
+            "extra_precisions": extra or None,
+            "lu_solve": lu}
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

@@ -516,7 +516,8 @@ int launch_core_recompress(const CoreJob* d_jobs, int njobs, int rmax, double ep
                                      (int)((size_t)3 * RCORE_MAX * RCORE_MAX * sizeof(double))));
     attr_set = true;
   }
-  core_recompress_kernel<<<njobs, 256, smem, st>>>(d_jobs, rmax, eps_trunc, d_flags);
+  // small cores: 2 warps per job, so that many jobs share an SM
+  core_recompress_kernel<<<njobs, rmax <= 32 ? 64 : 256, smem, st>>>(d_jobs, rmax, eps_trunc, d_flags);
   HM_CUDA_TRY(cudaGetLastError());
   return HM_OK;
 }

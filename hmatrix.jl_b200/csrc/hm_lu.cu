@@ -14,7 +14,10 @@
 #include "hm_internal.h"
 #include "hm_lowrank.cuh"
 
+#include <cublas_v2.h>
+
 #include <algorithm>
+#include <map>
 #include <memory>
 #include <stdexcept>
 
@@ -135,6 +138,88 @@ __global__ void __launch_bounds__(128) lu_trsm_lower_kernel(View L, View X, int 
     if (!unit) s = s / (sm ? Ls[i + i * m] : L.p[(int64_t)i * L.rs + (int64_t)i * L.cs]);
     x[(int64_t)i * X.rs] = s;
   }
+}
+
+// The same solve for triangles of at most MM rows (diagonal leaves): one warp
+// per 32 columns of X, each column held in registers, loops fully unrolled.
+template <int MM>
+__global__ void __launch_bounds__(32) lu_trsm_small_kernel(View L, View X, int unit) {
+  __shared__ double Ls[MM * MM];
+  const int m = L.rows;
+  for (int e = threadIdx.x; e < m * m; e += 32) {
+    const int i = e % m, j = e / m;
+    Ls[i + j * MM] = (j <= i) ? L.p[(int64_t)i * L.rs + (int64_t)j * L.cs] : 0.0;
+  }
+  __syncwarp();
+  const int j = blockIdx.x * 32 + threadIdx.x;
+  if (j >= X.cols) return;
+  double* xp = X.p + (int64_t)j * X.cs;
+  double x[MM];
+#pragma unroll
+  for (int i = 0; i < MM; ++i) x[i] = (i < m) ? xp[(int64_t)i * X.rs] : 0.0;
+#pragma unroll
+  for (int i = 0; i < MM; ++i) {
+    if (i < m) {
+      double s = x[i];
+#pragma unroll
+      for (int l = 0; l < i; ++l) s = fma(-Ls[i + l * MM], x[l], s);
+      if (!unit) s = s / Ls[i + i * MM];
+      x[i] = s;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < MM; ++i)
+    if (i < m) xp[(int64_t)i * X.rs] = x[i];
+}
+
+// getrf of a leaf of at most 64 rows by one warp (same pivoting and
+// arithmetic as lu_getrf_kernel; padded shared tile, warp barriers only)
+__global__ void __launch_bounds__(32) lu_getrf_small_kernel(View C, int64_t* __restrict__ P, int64_t goff,
+                                                            int* __restrict__ flags) {
+  constexpr int LD = 65;
+  __shared__ double S[64 * LD];
+  __shared__ int perm[64];
+  const int m = C.rows, lane = threadIdx.x;
+  for (int e = lane; e < m * m; e += 32) {
+    const int i = e % m, j = e / m;
+    S[i + j * LD] = C.p[(int64_t)i * C.rs + (int64_t)j * C.cs];
+  }
+  for (int i = lane; i < m; i += 32) perm[i] = i;
+  __syncwarp();
+  for (int j = 0; j < m; ++j) {
+    double best = -1.0, bv = 0.0;
+    int64_t bi = INT64_MAX;
+    for (int i = j + lane; i < m; i += 32) {
+      const double a = fabs(S[i + j * LD]);
+      if (a > best) { best = a; bi = i; bv = S[i + j * LD]; }
+    }
+    warp_argmax(best, bi, bv);
+    if (lane == 0 && !(bv != 0.0)) atomicOr(flags, 4);
+    const int p = (int)bi;
+    if (p != j) {
+      for (int c = lane; c < m; c += 32) {
+        const double t = S[j + c * LD];
+        S[j + c * LD] = S[p + c * LD];
+        S[p + c * LD] = t;
+      }
+      if (lane == 0) { const int t = perm[j]; perm[j] = perm[p]; perm[p] = t; }
+    }
+    __syncwarp();
+    const double piv = S[j + j * LD];
+    if (piv != 0.0)
+      for (int i = j + 1 + lane; i < m; i += 32) S[i + j * LD] /= piv;
+    __syncwarp();
+    for (int c = j + 1 + lane; c < m; c += 32) {
+      const double ujc = S[j + c * LD];
+      for (int i = j + 1; i < m; ++i) S[i + c * LD] = fma(-S[i + j * LD], ujc, S[i + c * LD]);
+    }
+    __syncwarp();
+  }
+  for (int e = lane; e < m * m; e += 32) {
+    const int i = e % m, j = e / m;
+    C.p[(int64_t)i * C.rs + (int64_t)j * C.cs] = S[i + j * LD];
+  }
+  for (int i = lane; i < m; i += 32) P[goff + i] = goff + perm[i];
 }
 
 // getrf with partial pivoting of an m x m dense leaf (LAPACK semantics: first
@@ -279,6 +364,19 @@ __device__ void gather_pieces(const GatherArgs& g) {
 }
 
 __global__ void lu_copy_int_kernel(int32_t* dst, const int32_t* src) { *dst = *src; }
+
+__global__ void lu_max_int_kernel(const int32_t* __restrict__ v, int n, int32_t* __restrict__ out) {
+  __shared__ int32_t red[256];
+  int32_t m = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = max(m, v[i]);
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] = max(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0];
+}
 __global__ void lu_set_int_kernel(int32_t* dst, int v) { *dst = v; }
 
 template <typename T>
@@ -304,6 +402,7 @@ struct Ctx {
   int* flags;          // device error bits: 1 rank overflow, 2 non-finite, 4 singular
   double eps_trunc;
   const hm_handle* h;
+  cublasHandle_t blas = nullptr;   // large plain products go to cuBLAS DGEMM
 };
 
 struct Blk {
@@ -359,8 +458,24 @@ static BP new_rk(Ctx& c, int m, int n, int32_t s, int32_t t, bool alloc_a = true
 static bool is_leaf_cluster(const Ctx& c, int32_t cl) { return cl >= 0 && c.h->cl_left[cl] < 0; }
 
 // ---- primitive launches --------------------------------------------------
+// a view as a column-major cuBLAS operand (op, leading dimension)
+static bool blas_operand(const View& v, cublasOperation_t& op, int& ld) {
+  if (v.rs == 1 && v.cs >= std::max(v.rows, 1) && v.cs < INT32_MAX) { op = CUBLAS_OP_N; ld = (int)v.cs; return true; }
+  if (v.cs == 1 && v.rs >= std::max(v.cols, 1) && v.rs < INT32_MAX) { op = CUBLAS_OP_T; ld = (int)v.rs; return true; }
+  return false;
+}
+
 static void gemm(Ctx& c, View C, View A, View B, double alpha, double beta) {
   if (C.rows == 0 || C.cols == 0) return;
+  cublasOperation_t oa, ob;
+  int lda, ldb;
+  if (c.blas && A.cols > 0 && (double)C.rows * C.cols * A.cols >= 4.0e6 && C.rs == 1 && C.cs >= C.rows &&
+      blas_operand(A, oa, lda) && blas_operand(B, ob, ldb)) {
+    if (cublasDgemm(c.blas, oa, ob, C.rows, C.cols, A.cols, &alpha, A.p, lda, B.p, ldb, &beta, C.p,
+                    (int)C.cs) != CUBLAS_STATUS_SUCCESS)
+      throw LuError(HM_ERR_CUDA, "cublasDgemm");
+    return;
+  }
   if (A.cols == 0) {
     if (beta != 1.0) {
       lu_axpby_kernel<<<64, 256, 0, c.st>>>(C, View{nullptr, 0, 0, C.rows, C.cols}, 0.0, beta);
@@ -383,6 +498,16 @@ static void axpby(Ctx& c, View Y, View X, double alpha, double beta) {
 
 static void trsm_lower(Ctx& c, View L, View X, bool unit) {
   if (X.cols == 0 || L.rows == 0) return;
+  if (L.rows <= 32) {
+    lu_trsm_small_kernel<32><<<(X.cols + 31) / 32, 32, 0, c.st>>>(L, X, unit ? 1 : 0);
+    LU_LAUNCH_CHECK();
+    return;
+  }
+  if (L.rows <= 64) {
+    lu_trsm_small_kernel<64><<<(X.cols + 31) / 32, 32, 0, c.st>>>(L, X, unit ? 1 : 0);
+    LU_LAUNCH_CHECK();
+    return;
+  }
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(lu_trsm_lower_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -398,6 +523,11 @@ static void trsm_lower(Ctx& c, View L, View X, bool unit) {
 static void getrf(Ctx& c, View C, int64_t goff) {
   const int m = C.rows;
   if (m != C.cols) throw LuError(HM_ERR_UNSUPPORTED, "non-square diagonal leaf");
+  if (m <= 64) {
+    lu_getrf_small_kernel<<<1, 32, 0, c.st>>>(C, c.P, goff, c.flags);
+    LU_LAUNCH_CHECK();
+    return;
+  }
   const size_t smem = sizeof(double) * (size_t)m * m + sizeof(int) * m;
   if (smem > 200 * 1024) throw LuError(HM_ERR_UNSUPPORTED, "diagonal leaf above 150 rows (MinBlock too large)");
   static bool attr = false;
@@ -880,8 +1010,6 @@ __global__ void lu_scatter_rows_kernel(View Xv, View W, const int64_t* __restric
   }
 }
 
-static BP build_from_handle(Ctx& c, const hm_handle* h, int32_t node);
-
 // ---------------------------------------------------------------------------
 // batched helpers
 // ---------------------------------------------------------------------------
@@ -892,6 +1020,55 @@ static J* upload_jobs(Ctx& c, Blk& owner, const std::vector<J>& v) {
     throw LuError(HM_ERR_CUDA, "job upload");
   return d;
 }
+
+// copies of stored leaves into the FP64 working buffers of the factorisation,
+// collected and launched as one kernel (one CTA per block)
+struct LoadJob {
+  const void* src;
+  int64_t ld_src;
+  int rows, cols;          // valid source columns; columns [cols, dst_cols) become zero
+  int type;                // HM_F64 / HM_F32 / HM_BF16 element type of src
+  double* dst;
+  int64_t ld_dst;
+  int dst_cols;
+  int32_t* kdst;           // if set: *kdst = kval
+  int kval;
+};
+__global__ void lu_load_batch_kernel(const LoadJob* __restrict__ jobs) {
+  const LoadJob J = jobs[blockIdx.x];
+  const int64_t tot = (int64_t)J.rows * J.dst_cols;
+  for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
+    const int i = (int)(e % J.rows), c = (int)(e / J.rows);
+    double v = 0.0;
+    if (c < J.cols) {
+      const int64_t s = i + (int64_t)c * J.ld_src;
+      if (J.type == HM_F64) v = ((const double*)J.src)[s];
+      else if (J.type == HM_F32) v = (double)((const float*)J.src)[s];
+      else v = (double)__bfloat162float(((const __nv_bfloat16*)J.src)[s]);
+    }
+    J.dst[i + (int64_t)c * J.ld_dst] = v;
+  }
+  if (threadIdx.x == 0 && J.kdst) *J.kdst = J.kval;
+}
+
+struct Loader {
+  std::vector<LoadJob> jobs;
+  void flush(Ctx& c) {
+    for (size_t b = 0; b < jobs.size(); b += 65535) {
+      const size_t nb = std::min<size_t>(65535, jobs.size() - b);
+      Blk tmp;
+      tmp.st = c.st;
+      std::vector<LoadJob> part(jobs.begin() + b, jobs.begin() + b + nb);
+      LoadJob* d = upload_jobs(c, tmp, part);
+      lu_load_batch_kernel<<<(unsigned)nb, 256, 0, c.st>>>(d);
+      LU_LAUNCH_CHECK();
+    }
+    jobs.clear();
+  }
+};
+
+static BP build_tree(Ctx& c, const hm_handle* h, int32_t node, Loader& ld);
+static BP build_from_handle(Ctx& c, const hm_handle* h, int32_t node);
 
 static void gemm_batch(Ctx& c, const std::vector<GemmJob>& jobs) {
   if (jobs.empty()) return;
@@ -959,7 +1136,17 @@ static void recompress_batch(Ctx& c, const std::vector<RcReq>& reqs, int rmax) {
     CoreJob* dc = upload_jobs(c, tmp, cj);
     lu_gather_pieces_batch_kernel<<<(unsigned)(e - b), 256, 0, c.st>>>(dg);
     LU_LAUNCH_CHECK();
-    int s = launch_core_recompress(dc, (int)(e - b), rmax, c.eps_trunc, c.flags, c.st);
+    // size the core launch to the largest core of this batch (ranks are on
+    // the device: one small read-back per batch)
+    int32_t* dmax = (int32_t*)dmalloc(c, tmp, sizeof(int32_t));
+    lu_max_int_kernel<<<1, 256, 0, c.st>>>(rr, (int)(e - b), dmax);
+    LU_LAUNCH_CHECK();
+    int32_t hmax = 0;
+    if (cudaMemcpyAsync(&hmax, dmax, sizeof(int32_t), cudaMemcpyDeviceToHost, c.st) != cudaSuccess ||
+        cudaStreamSynchronize(c.st) != cudaSuccess)
+      throw LuError(HM_ERR_CUDA, "core size read-back");
+    const int rlaunch = std::min(rmax, std::max(8, (hmax + 7) / 8 * 8));
+    int s = launch_core_recompress(dc, (int)(e - b), rlaunch, c.eps_trunc, c.flags, c.st);
     if (s != HM_OK) throw LuError(s, "batched recompression launch");
     b = e;
   }
@@ -1085,29 +1272,25 @@ static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vecto
   auto tile_of = [&](int64_t r) {
     return (int)(std::upper_bound(TL.start.begin(), TL.start.end(), r) - TL.start.begin()) - 1;
   };
+  Loader ld;
+  const char* base = (const char*)h->d_rk;
   for (auto& L : h->leaves) {
     const int i = tile_of(L.row0), j = tile_of(L.col0);
     if (i == j) continue;
     if (L.k > cap) throw LuError(HM_ERR_RANK, "leaf rank above the H-LU rank capacity");
     kh[i * T + j] = L.k;
     const int64_t npad = col_pad(L.n, eb), mpad = col_pad(L.m, eb);
-    auto load = [&](int64_t off, int64_t ld, int rows, double* dst) {
-      unsigned g = (unsigned)std::min<int64_t>(((int64_t)rows * cap + 255) / 256, 1024);
-      switch (h->storage) {
-        case HM_F64: lu_load_kernel<double><<<g, 256, 0, c.st>>>((const double*)h->d_rk + off, ld, rows, L.k, dst, rows, cap); break;
-        case HM_F32: lu_load_kernel<float><<<g, 256, 0, c.st>>>((const float*)h->d_rk + off, ld, rows, L.k, dst, rows, cap); break;
-        default: lu_load_kernel<__nv_bfloat16><<<g, 256, 0, c.st>>>((const __nv_bfloat16*)h->d_rk + off, ld, rows, L.k, dst, rows, cap);
-      }
-      LU_LAUNCH_CHECK();
-    };
-    load(L.off, npad, L.n, TL.Bj(i, j, cap));
-    load(L.off + npad * L.k, mpad, L.m, TL.Ai(i, j, cap));
+    ld.jobs.push_back(LoadJob{base + L.off * eb, npad, L.n, L.k, h->storage, TL.Bj(i, j, cap), L.n, cap,
+                              nullptr, 0});
+    ld.jobs.push_back(LoadJob{base + (L.off + npad * L.k) * eb, mpad, L.m, L.k, h->storage, TL.Ai(i, j, cap),
+                              L.m, cap, nullptr, 0});
   }
   if (cudaMemcpyAsync(TL.kmat, kh.data(), sizeof(int32_t) * T * T, cudaMemcpyHostToDevice, c.st) != cudaSuccess)
     throw LuError(HM_ERR_CUDA, "rank upload");
   cudaStreamSynchronize(c.st);       // kh leaves scope before the async copy otherwise
   TL.diag.resize(T);
-  for (int i = 0; i < T; ++i) TL.diag[i] = build_from_handle(c, h, dnode[i]);
+  for (int i = 0; i < T; ++i) TL.diag[i] = build_tree(c, h, dnode[i], ld);
+  ld.flush(c);
 
   for (int k = 0; k < T; ++k) {
     const int mk = (int)TL.size[k];
@@ -1127,18 +1310,51 @@ static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vecto
     gemm(c, Wv, vtr(Lb), Ua, 1.0, 0.0);                   // W_ij = B_ik' A_kj
     // Q_i = A_ik W_i,:   (m_i x R) for every trailing tile row i
     std::vector<double*> Q(T, nullptr);
-    std::vector<GemmJob> gq;
-    for (int i = k + 1; i < T; ++i) {
-      const int mi = (int)TL.size[i];
-      Q[i] = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)mi * R);
-      GemmJob g{};
-      g.A = View{TL.Ai(i, k, cap), 1, mi, mi, cap};
-      g.B = vsub(Wv, (i - k - 1) * cap, 0, cap, R);
-      g.C = View{Q[i], 1, mi, mi, R};
-      g.alpha = 1.0; g.beta = 0.0;
-      gq.push_back(g);
+    {
+      int64_t qtot = 0;
+      for (int i = k + 1; i < T; ++i) qtot += TL.size[i] * (int64_t)R;
+      double* qbase = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)qtot);
+      int64_t qo = 0;
+      for (int i = k + 1; i < T; ++i) { Q[i] = qbase + qo; qo += TL.size[i] * (int64_t)R; }
+      // tiles of equal height: one batched cuBLAS product per height
+      std::map<int, std::vector<int>> by_m;
+      for (int i = k + 1; i < T; ++i) by_m[(int)TL.size[i]].push_back(i);
+      std::vector<GemmJob> gq;
+      for (auto& kv : by_m) {
+        const int mi = kv.first;
+        const std::vector<int>& rows = kv.second;
+        if (c.blas && (double)mi * R * cap * rows.size() >= 4.0e6) {
+          std::vector<const double*> pa, pb;
+          std::vector<double*> pc;
+          for (int i : rows) {
+            pa.push_back(TL.Ai(i, k, cap));
+            pb.push_back(W + (int64_t)(i - k - 1) * cap);
+            pc.push_back(Q[i]);
+          }
+          const double** da = (const double**)dmalloc(c, tmp, sizeof(void*) * rows.size());
+          const double** db = (const double**)dmalloc(c, tmp, sizeof(void*) * rows.size());
+          double** dc = (double**)dmalloc(c, tmp, sizeof(void*) * rows.size());
+          if (cudaMemcpyAsync(da, pa.data(), sizeof(void*) * rows.size(), cudaMemcpyHostToDevice, c.st) ||
+              cudaMemcpyAsync(db, pb.data(), sizeof(void*) * rows.size(), cudaMemcpyHostToDevice, c.st) ||
+              cudaMemcpyAsync(dc, pc.data(), sizeof(void*) * rows.size(), cudaMemcpyHostToDevice, c.st))
+            throw LuError(HM_ERR_CUDA, "pointer upload");
+          const double one = 1.0, zero = 0.0;
+          if (cublasDgemmBatched(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, mi, R, cap, &one, da, mi, db, R, &zero, dc, mi,
+                                 (int)rows.size()) != CUBLAS_STATUS_SUCCESS)
+            throw LuError(HM_ERR_CUDA, "cublasDgemmBatched");
+        } else {
+          for (int i : rows) {
+            GemmJob g{};
+            g.A = View{TL.Ai(i, k, cap), 1, mi, mi, cap};
+            g.B = vsub(Wv, (i - k - 1) * cap, 0, cap, R);
+            g.C = View{Q[i], 1, mi, mi, R};
+            g.alpha = 1.0; g.beta = 0.0;
+            gq.push_back(g);
+          }
+        }
+      }
+      gemm_batch(c, gq);
     }
-    gemm_batch(c, gq);
     std::vector<RcReq> rj;
     std::vector<GemmJob> gd;
     for (int i = k + 1; i < T; ++i) {
@@ -1253,23 +1469,31 @@ struct LuState {
   int* flags = nullptr;
   int cap = 0;
   cudaStream_t st = nullptr;
+  cublasHandle_t blas = nullptr;
   ~LuState() {
     root.reset();
     tile.reset();
     if (P) cudaFreeAsync(P, st);
     if (flags) cudaFreeAsync(flags, st);
     if (st) cudaStreamSynchronize(st);
+    if (blas) cublasDestroy(blas);
+  }
+  // cuBLAS on the factorisation's stream (created on first use)
+  cublasHandle_t blas_on(cudaStream_t s) {
+    if (!blas && cublasCreate(&blas) != CUBLAS_STATUS_SUCCESS) blas = nullptr;
+    if (blas) cublasSetStream(blas, s);
+    return blas;
   }
 };
 
-static BP build_from_handle(Ctx& c, const hm_handle* h, int32_t node) {
+static BP build_tree(Ctx& c, const hm_handle* h, int32_t node, Loader& ld) {
   const Node& nd = h->nodes[node];
   const int m = (int)(h->cl_e[nd.s] - h->cl_s[nd.s]), n = (int)(h->cl_e[nd.t] - h->cl_s[nd.t]);
   if (nd.type == T_H) {
     BP b = std::make_shared<Blk>();
     b->st = c.st;
     b->type = T_H; b->m = m; b->n = n; b->s = nd.s; b->t = nd.t; b->row0 = h->cl_s[nd.s];
-    for (int q = 0; q < 4; ++q) b->ch[q] = build_from_handle(c, h, nd.child[q]);
+    for (int q = 0; q < 4; ++q) b->ch[q] = build_tree(c, h, nd.child[q], ld);
     return b;
   }
   const Leaf& L = h->leaves[nd.leaf];
@@ -1277,33 +1501,27 @@ static BP build_from_handle(Ctx& c, const hm_handle* h, int32_t node) {
   if (nd.type == T_DENSE) {
     BP d = new_dense(c, m, n, nd.s, nd.t);
     d->row0 = L.row0;
-    const int64_t ld = col_pad(m, deb);
-    unsigned g = (unsigned)std::min<int64_t>(((int64_t)m * n + 255) / 256, 1024);
-    if (h->storage == HM_F64)
-      lu_load_kernel<double><<<g, 256, 0, c.st>>>((const double*)h->d_dense + L.off, ld, m, n, d->C, d->ldc, n);
-    else
-      lu_load_kernel<float><<<g, 256, 0, c.st>>>((const float*)h->d_dense + L.off, ld, m, n, d->C, d->ldc, n);
-    LU_LAUNCH_CHECK();
+    const int dt = h->storage == HM_F64 ? HM_F64 : HM_F32;
+    ld.jobs.push_back(LoadJob{(const char*)h->d_dense + L.off * deb, col_pad(m, deb), m, n, dt, d->C, d->ldc, n,
+                              nullptr, 0});
     return d;
   }
   if (L.k > c.cap) throw LuError(HM_ERR_RANK, "leaf rank above the H-LU rank capacity");
   BP r = new_rk(c, m, n, nd.s, nd.t);
   r->row0 = L.row0;
   const int64_t npad = col_pad(n, eb), mpad = col_pad(m, eb);
-  auto load = [&](int64_t off, int64_t ld, int rows, double* dst, int64_t ldd) {
-    unsigned g = (unsigned)std::min<int64_t>(((int64_t)rows * c.cap + 255) / 256, 1024);
-    switch (h->storage) {
-      case HM_F64: lu_load_kernel<double><<<g, 256, 0, c.st>>>((const double*)h->d_rk + off, ld, rows, L.k, dst, ldd, c.cap); break;
-      case HM_F32: lu_load_kernel<float><<<g, 256, 0, c.st>>>((const float*)h->d_rk + off, ld, rows, L.k, dst, ldd, c.cap); break;
-      default: lu_load_kernel<__nv_bfloat16><<<g, 256, 0, c.st>>>((const __nv_bfloat16*)h->d_rk + off, ld, rows, L.k, dst, ldd, c.cap);
-    }
-    LU_LAUNCH_CHECK();
-  };
-  load(L.off, npad, n, r->B, r->ldb);
-  load(L.off + npad * L.k, mpad, m, r->A, r->lda);
-  lu_set_int_kernel<<<1, 1, 0, c.st>>>(r->k, L.k);
-  LU_LAUNCH_CHECK();
+  const char* base = (const char*)h->d_rk;
+  ld.jobs.push_back(LoadJob{base + L.off * eb, npad, n, L.k, h->storage, r->B, r->ldb, c.cap, nullptr, 0});
+  ld.jobs.push_back(LoadJob{base + (L.off + npad * L.k) * eb, mpad, m, L.k, h->storage, r->A, r->lda, c.cap,
+                            r->k, L.k});
   return r;
+}
+
+static BP build_from_handle(Ctx& c, const hm_handle* h, int32_t node) {
+  Loader ld;
+  BP b = build_tree(c, h, node, ld);
+  ld.flush(c);
+  return b;
 }
 
 static int finish(Ctx& c, const char* what) {
@@ -1317,14 +1535,28 @@ static int finish(Ctx& c, const char* what) {
 }
 
 int lu_factor(hm_handle* h) {
+  // the factorisation allocates and frees many stream-ordered temporaries:
+  // keep freed memory in the device's pool instead of returning it to the
+  // driver at every synchronisation
+  {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, h->device) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
   LuState* S = new LuState();
   S->st = h->stream;
-  S->cap = h->prm.rank_cap > 0 ? h->prm.rank_cap : std::max(32, 2 * std::max(h->kmax, 1));
+  // capacity of low-rank blocks: twice the largest leaf rank (updated blocks
+  // are truncated back after every addition), at least 12; HM_ERR_RANK if a
+  // truncated rank ever exceeds it (raise rank_cap then)
+  S->cap = h->prm.rank_cap > 0 ? h->prm.rank_cap : std::max(12, 2 * std::max(h->kmax, 1));
   S->cap = std::min(S->cap, RCORE_MAX / 2);
   HM_CUDA_TRY(cudaMallocAsync((void**)&S->P, sizeof(int64_t) * h->n, h->stream));
   HM_CUDA_TRY(cudaMallocAsync((void**)&S->flags, sizeof(int), h->stream));
   HM_CUDA_TRY(cudaMemsetAsync(S->flags, 0, sizeof(int), h->stream));
-  Ctx c{h->stream, S->cap, S->P, S->flags, h->prm.eps_trunc, h};
+  const double eps_lu = h->prm.eps_trunc_lu > 0.0 ? h->prm.eps_trunc_lu : h->prm.eps_trunc;
+  Ctx c{h->stream, S->cap, S->P, S->flags, eps_lu, h, S->blas_on(h->stream)};
   const int mode = h->prm.lu_mode;     // 0 auto, 1 recursion, 2 tiles
   try {
     if (h->kmax > S->cap) throw LuError(HM_ERR_RANK, "a leaf rank exceeds the H-LU rank capacity");
@@ -1357,7 +1589,7 @@ int lu_solve_device(hm_handle* h, const double* d_b, double* d_x, int64_t ncols,
   LuState* S = h->lu;
   if (!S) return fail(HM_ERR_STATE, "a has not been factorized");
   if (ncols <= 0) return HM_OK;
-  Ctx c{st, S->cap, S->P, S->flags, h->prm.eps_trunc, h};
+  Ctx c{st, S->cap, S->P, S->flags, h->prm.eps_trunc, h, S->blas_on(st)};
   try {
     View B{const_cast<double*>(d_b), 1, h->n, (int)h->n, (int)ncols};
     View X{d_x, 1, h->n, (int)h->n, (int)ncols};

@@ -57,6 +57,7 @@ class Params:
     Device: int = 0
     RankCap: int = 0                      # rank capacity during H-LU (0: automatic)
     LuMode: str = "auto"                  # "auto" | "recursive" (lu! as written) | "tiles"
+    εTruncLU: float = 0.0                 # truncation inside H-LU (0: εTrunc, as in the reference)
 
 
 Hparams = Params()
@@ -98,6 +99,7 @@ def _params_struct(prm: Params, dim: int):
     p.device = prm.Device
     p.rank_cap = prm.RankCap
     p.lu_mode = {"auto": 0, "recursive": 1, "tiles": 2}[prm.LuMode]
+    p.eps_trunc_lu = prm.εTruncLU
     return p
 
 

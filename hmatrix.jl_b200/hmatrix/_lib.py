@@ -42,7 +42,8 @@ class hm_params(C.Structure):
         ("eps_comp", C.c_double), ("eps_trunc", C.c_double), ("max_rank", C.c_int32),
         ("max_block", C.c_int32), ("min_block", C.c_int32), ("cons_method", C.c_int32),
         ("aca_force", C.c_int32), ("storage", C.c_int32), ("device", C.c_int32),
-        ("rank_cap", C.c_int32), ("lu_mode", C.c_int32), ("reserved", C.c_int32 * 5),
+        ("rank_cap", C.c_int32), ("lu_mode", C.c_int32), ("reserved0", C.c_int32),
+        ("eps_trunc_lu", C.c_double), ("reserved", C.c_int32 * 2),
     ]
 
 

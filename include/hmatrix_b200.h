@@ -76,7 +76,12 @@ typedef struct hm_params {
     int32_t lu_mode;      /* H-LU schedule: 0 auto, 1 the recursion of lu!,
                              2 tile by tile (needs a level where every block
                              outside the diagonal tiles is one low-rank block) */
-    int32_t reserved[5];
+    int32_t reserved0;
+    double  eps_trunc_lu; /* truncation tolerance of the recompressions inside
+                             H-LU (0: eps_trunc, as in the reference); a looser
+                             value gives a cheaper factorisation that
+                             hm_solve_refined brings back to full accuracy */
+    int32_t reserved[2];
 } hm_params;
 
 /* info(H) of src/utils.jl:83-110 plus the byte counts used for rooflines. */
