@@ -44,6 +44,11 @@ struct LuError : std::runtime_error {
   LuError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
+#define HM_LU_CUDA(expr)                                                                    \
+  do {                                                                                      \
+    cudaError_t _e = (expr);                                                                \
+    if (_e != cudaSuccess) throw LuError(HM_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
 #define LU_LAUNCH_CHECK()                                                                   \
   do {                                                                                      \
     cudaError_t _e = cudaGetLastError();                                                    \
@@ -403,7 +408,17 @@ struct Ctx {
   double eps_trunc;
   const hm_handle* h;
   cublasHandle_t blas = nullptr;   // large plain products go to cuBLAS DGEMM
+  struct Arena* ar = nullptr;      // when set, temporaries come from this fixed buffer
 };
+
+// A fixed device buffer handed out front to back; nothing is returned before
+// the sequence that uses it ends.  A captured solve takes its temporaries from
+// one, so the graph holds no allocation nodes.
+struct Arena {
+  char* base = nullptr;
+  size_t size = 0, used = 0;
+};
+static inline size_t arena_round(size_t b) { return (std::max<size_t>(b, 8) + 255) & ~(size_t)255; }
 
 struct Blk {
   int8_t type = T_H;
@@ -428,7 +443,19 @@ struct Blk {
   View Bv() const { return View{B, 1, ldb, n, cap}; }
 };
 
+struct JobTape;
+static thread_local JobTape* g_tape = nullptr;
+static void tape_note_temporary(size_t bytes);
+
 static void* dmalloc(Ctx& c, Blk& b, size_t bytes) {
+  if (c.ar) {
+    const size_t r = arena_round(bytes);
+    if (c.ar->used + r > c.ar->size) throw LuError(HM_ERR_CUDA, "solve arena exhausted");
+    void* q = c.ar->base + c.ar->used;
+    c.ar->used += r;
+    return q;
+  }
+  tape_note_temporary(bytes);
   void* p = nullptr;
   cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(bytes, 8), c.st);
   if (e != cudaSuccess) throw LuError(HM_ERR_OOM, std::string("H-LU temporary: ") + cudaGetErrorString(e));
@@ -1013,9 +1040,40 @@ __global__ void lu_scatter_rows_kernel(View Xv, View W, const int64_t* __restric
 // ---------------------------------------------------------------------------
 // batched helpers
 // ---------------------------------------------------------------------------
+// Job arrays of a sequence that is later captured into a CUDA graph: the first
+// (recording) run keeps every uploaded array alive in order; the capture run
+// takes the same arrays back instead of uploading (a host-to-device copy of
+// pageable memory cannot be captured).  The job contents are identical since
+// the capture replays the recorded sequence on the same buffers.
+struct JobTape {
+  bool record = false, replay = false;
+  std::vector<void*> bufs;
+  std::vector<size_t> bytes;
+  size_t pos = 0;
+  size_t temp_bytes = 0;   // arena size that holds every temporary of the recorded run
+  ~JobTape() {             // the owner has synchronised the device
+    for (void* p : bufs) cudaFreeAsync(p, cudaStreamLegacy);
+  }
+};
+static void tape_note_temporary(size_t bytes) {
+  if (g_tape && g_tape->record) g_tape->temp_bytes += arena_round(bytes);
+}
+
 template <typename J>
 static J* upload_jobs(Ctx& c, Blk& owner, const std::vector<J>& v) {
-  J* d = (J*)dmalloc(c, owner, sizeof(J) * v.size());
+  if (g_tape && g_tape->replay) {
+    if (g_tape->pos >= g_tape->bufs.size() || g_tape->bytes[g_tape->pos] != sizeof(J) * v.size())
+      throw LuError(HM_ERR_CUDA, "job tape does not match the recorded sequence");
+    return (J*)g_tape->bufs[g_tape->pos++];
+  }
+  J* d = nullptr;
+  if (g_tape && g_tape->record) {
+    if (cudaMallocAsync(&d, sizeof(J) * v.size(), c.st) != cudaSuccess) throw LuError(HM_ERR_OOM, "job tape");
+    g_tape->bufs.push_back(d);
+    g_tape->bytes.push_back(sizeof(J) * v.size());
+  } else {
+    d = (J*)dmalloc(c, owner, sizeof(J) * v.size());
+  }
   if (cudaMemcpyAsync(d, v.data(), sizeof(J) * v.size(), cudaMemcpyHostToDevice, c.st) != cudaSuccess)
     throw LuError(HM_ERR_CUDA, "job upload");
   return d;
@@ -1384,12 +1442,12 @@ static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vecto
 }
 
 // y = P b, forward (unit L), backward (U) tile by tile; trans: U' then L'
-static void tile_solve(Ctx& c, const TileLU& TL, View X, bool trans) {
+static void tile_solve(Ctx& c, const TileLU& TL, View X, bool trans, double* Zext = nullptr) {
   const int T = TL.T, cap = c.cap, nc = X.cols;
   auto yv = [&](int i) { return vsub(X, (int)TL.start[i], 0, (int)TL.size[i], nc); };
   Blk tmp;
   tmp.st = c.st;
-  double* Z = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)T * cap * nc);
+  double* Z = Zext ? Zext : (double*)dmalloc(c, tmp, sizeof(double) * (size_t)T * cap * nc);
   if (!trans) {
     for (int k = 0; k < T; ++k) {                       // L y = b
       solve_rec(c, *TL.diag[k], yv(k), true);
@@ -1462,6 +1520,26 @@ static void tile_densify(Ctx& c, const TileLU& TL, View D) {
 // ---------------------------------------------------------------------------
 // state, entry points
 // ---------------------------------------------------------------------------
+// One captured solve: the launch sequence of a\y (or a'\y) for a fixed number
+// of right-hand sides, recorded into a CUDA graph that works on the plan's own
+// input/output buffers.  A call copies b in, launches the graph, copies x out.
+struct SolvePlan {
+  int64_t ncols = 0;
+  int trans = 0;
+  double* xin = nullptr;   // n x ncols, right-hand sides (the transposed solve works in place here)
+  double* xout = nullptr;  // n x ncols, solution
+  double* Z = nullptr;     // tile-solve product scratch
+  Arena arena;             // temporaries of the captured sequence
+  JobTape tape;
+  cudaGraphExec_t exec = nullptr;
+  bool no_graph = false;   // capture failed: the plan runs its sequence directly
+  ~SolvePlan() {           // the owner has synchronised the device
+    if (exec) cudaGraphExecDestroy(exec);
+    for (void* p : {(void*)xin, (void*)xout, (void*)Z, (void*)arena.base})
+      if (p) cudaFreeAsync(p, cudaStreamLegacy);
+  }
+};
+
 struct LuState {
   BP root;                       // recursive format
   std::unique_ptr<TileLU> tile;  // tile format
@@ -1470,18 +1548,32 @@ struct LuState {
   int cap = 0;
   cudaStream_t st = nullptr;
   cublasHandle_t blas = nullptr;
+  void* blas_ws = nullptr;
+  std::vector<std::unique_ptr<SolvePlan>> plans;
   ~LuState() {
+    if (!plans.empty()) cudaDeviceSynchronize();
+    plans.clear();
     root.reset();
     tile.reset();
     if (P) cudaFreeAsync(P, st);
     if (flags) cudaFreeAsync(flags, st);
     if (st) cudaStreamSynchronize(st);
     if (blas) cublasDestroy(blas);
+    if (blas_ws) cudaFree(blas_ws);
   }
-  // cuBLAS on the factorisation's stream (created on first use)
+  // cuBLAS on stream s (created on first use).  The handle gets a fixed
+  // workspace so that a captured product allocates nothing; cublasSetStream
+  // resets the workspace, hence it is set again after every stream change.
+  static constexpr size_t BLAS_WS = (size_t)32 << 20;
   cublasHandle_t blas_on(cudaStream_t s) {
-    if (!blas && cublasCreate(&blas) != CUBLAS_STATUS_SUCCESS) blas = nullptr;
-    if (blas) cublasSetStream(blas, s);
+    if (!blas) {
+      if (cublasCreate(&blas) != CUBLAS_STATUS_SUCCESS) blas = nullptr;
+      if (blas && cudaMalloc(&blas_ws, BLAS_WS) != cudaSuccess) blas_ws = nullptr;
+    }
+    if (blas) {
+      cublasSetStream(blas, s);
+      if (blas_ws) cublasSetWorkspace(blas, blas_ws, BLAS_WS);
+    }
     return blas;
   }
 };
@@ -1585,40 +1677,153 @@ int lu_factor(hm_handle* h) {
   return HM_OK;
 }
 
+// The launch sequence of a\y (trans = 0) or a'\y (trans = 1) from d_b into d_x.
+// W, when given, is the working copy of b for the transposed solve; it may be
+// d_b itself (the solve then overwrites b).
+static void issue_solve(Ctx& c, LuState* S, const hm_handle* h, const double* d_b, double* d_x, int nc,
+                        int trans, double* Z, double* W) {
+  View B{const_cast<double*>(d_b), 1, h->n, (int)h->n, nc};
+  View X{d_x, 1, h->n, (int)h->n, nc};
+  const int64_t tot = h->n * nc;
+  const unsigned g = (unsigned)std::min<int64_t>((tot + 255) / 256, 4096);
+  if (!trans) {
+    // a\y (src/hlu.jl:553-562): permute!(w, P), unit-L forward, U backward
+    lu_gather_rows_kernel<<<g, 256, 0, c.st>>>(X, B, S->P);
+    LU_LAUNCH_CHECK();
+    if (S->tile) {
+      tile_solve(c, *S->tile, X, false, Z);
+    } else {
+      solve_rec(c, *S->root, X, true);
+      solve_rec(c, *S->root, X, false);
+    }
+  } else {
+    Blk tmp;
+    tmp.st = c.st;
+    double* w = W ? W : (double*)dmalloc(c, tmp, sizeof(double) * (size_t)tot);
+    View Wv{w, 1, h->n, (int)h->n, nc};
+    if (w != d_b) axpby(c, Wv, B, 1.0, 0.0);
+    if (S->tile) {
+      tile_solve(c, *S->tile, Wv, true, Z);
+    } else {
+      solve_t_rec(c, *S->root, Wv, true);
+      solve_t_rec(c, *S->root, Wv, false);
+    }
+    lu_scatter_rows_kernel<<<g, 256, 0, c.st>>>(X, Wv, S->P);
+    LU_LAUNCH_CHECK();
+  }
+}
+
+// Solves with at most this many right-hand sides are captured into a graph.
+static constexpr int64_t SOLVE_GRAPH_MAX_COLS = 64;
+static constexpr size_t SOLVE_MAX_PLANS = 8;
+
+static SolvePlan* new_plan(LuState* S, const hm_handle* h, int64_t nc, int trans, cudaStream_t st) {
+  auto pl = std::make_unique<SolvePlan>();
+  pl->ncols = nc;
+  pl->trans = trans;
+  const size_t xb = sizeof(double) * (size_t)h->n * nc;
+  const size_t zb = S->tile ? sizeof(double) * (size_t)S->tile->T * S->cap * nc : 8;
+  if (cudaMallocAsync(&pl->xin, xb, st) != cudaSuccess || cudaMallocAsync(&pl->xout, xb, st) != cudaSuccess ||
+      cudaMallocAsync(&pl->Z, zb, st) != cudaSuccess) {
+    cudaGetLastError();
+    throw LuError(HM_ERR_OOM, "solve plan buffers");
+  }
+  if (S->plans.size() >= SOLVE_MAX_PLANS) {
+    cudaDeviceSynchronize();
+    S->plans.erase(S->plans.begin());
+  }
+  S->plans.push_back(std::move(pl));
+  return S->plans.back().get();
+}
+
+// Records the plan's sequence into a graph on a private stream.  Nothing runs
+// during capture; a failure leaves the plan without a graph.
+static void capture_plan(LuState* S, hm_handle* h, SolvePlan* pl, cudaStream_t caller) {
+  cudaStream_t cs = nullptr;
+  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    pl->no_graph = true;
+    return;
+  }
+  if (pl->tape.temp_bytes > 0 &&
+      cudaMallocAsync((void**)&pl->arena.base, pl->tape.temp_bytes, caller) != cudaSuccess) {
+    cudaGetLastError();
+    cudaStreamDestroy(cs);
+    pl->no_graph = true;
+    return;
+  }
+  pl->arena.size = pl->tape.temp_bytes;
+  pl->arena.used = 0;
+  Ctx c{cs, S->cap, S->P, S->flags, h->prm.eps_trunc, h, S->blas_on(cs), &pl->arena};
+  pl->tape.record = false;
+  pl->tape.replay = true;
+  pl->tape.pos = 0;
+  bool ok = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    g_tape = &pl->tape;
+    try {
+      issue_solve(c, S, h, pl->xin, pl->xout, (int)pl->ncols, pl->trans, pl->Z, pl->xin);
+    } catch (const LuError&) {
+      ok = false;
+    }
+    g_tape = nullptr;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamEndCapture(cs, &graph) != cudaSuccess) ok = false;
+    if (ok && pl->tape.pos != pl->tape.bufs.size()) ok = false;
+    if (ok && cudaGraphInstantiate(&pl->exec, graph, 0) != cudaSuccess) {
+      pl->exec = nullptr;
+      ok = false;
+    }
+    if (graph) cudaGraphDestroy(graph);
+  }
+  cudaGetLastError();                  // capture errors are not sticky; clear them
+  pl->tape.replay = false;
+  pl->no_graph = !ok;
+  cudaStreamDestroy(cs);
+  S->blas_on(caller);
+  // the plan's buffers were allocated in the caller's stream order; later
+  // calls may come on other streams
+  cudaStreamSynchronize(caller);
+}
+
 int lu_solve_device(hm_handle* h, const double* d_b, double* d_x, int64_t ncols, int trans, cudaStream_t st) {
   LuState* S = h->lu;
   if (!S) return fail(HM_ERR_STATE, "a has not been factorized");
   if (ncols <= 0) return HM_OK;
   Ctx c{st, S->cap, S->P, S->flags, h->prm.eps_trunc, h, S->blas_on(st)};
   try {
-    View B{const_cast<double*>(d_b), 1, h->n, (int)h->n, (int)ncols};
-    View X{d_x, 1, h->n, (int)h->n, (int)ncols};
-    const int64_t tot = h->n * ncols;
-    const unsigned g = (unsigned)std::min<int64_t>((tot + 255) / 256, 4096);
-    if (!trans) {
-      // a\y (src/hlu.jl:553-562): permute!(w, P), unit-L forward, U backward
-      lu_gather_rows_kernel<<<g, 256, 0, st>>>(X, B, S->P);
-      LU_LAUNCH_CHECK();
-      if (S->tile) {
-        tile_solve(c, *S->tile, X, false);
-      } else {
-        solve_rec(c, *S->root, X, true);
-        solve_rec(c, *S->root, X, false);
-      }
+    if (ncols > SOLVE_GRAPH_MAX_COLS) {
+      issue_solve(c, S, h, d_b, d_x, (int)ncols, trans, nullptr, nullptr);
     } else {
-      Blk tmp;
-      tmp.st = st;
-      double* w = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)tot);
-      View W{w, 1, h->n, (int)h->n, (int)ncols};
-      axpby(c, W, B, 1.0, 0.0);
-      if (S->tile) {
-        tile_solve(c, *S->tile, W, true);
-      } else {
-        solve_t_rec(c, *S->root, W, true);
-        solve_t_rec(c, *S->root, W, false);
+      SolvePlan* pl = nullptr;
+      for (auto& q : S->plans)
+        if (q->ncols == ncols && q->trans == trans) pl = q.get();
+      const size_t xb = sizeof(double) * (size_t)h->n * ncols;
+      if (pl && pl->exec) {
+        HM_LU_CUDA(cudaMemcpyAsync(pl->xin, d_b, xb, cudaMemcpyDeviceToDevice, st));
+        HM_LU_CUDA(cudaGraphLaunch(pl->exec, st));
+        HM_LU_CUDA(cudaMemcpyAsync(d_x, pl->xout, xb, cudaMemcpyDeviceToDevice, st));
+      } else if (pl) {                 // capture failed earlier: direct run on the plan's buffers
+        HM_LU_CUDA(cudaMemcpyAsync(pl->xin, d_b, xb, cudaMemcpyDeviceToDevice, st));
+        issue_solve(c, S, h, pl->xin, pl->xout, (int)ncols, trans, pl->Z, pl->xin);
+        HM_LU_CUDA(cudaMemcpyAsync(d_x, pl->xout, xb, cudaMemcpyDeviceToDevice, st));
+      } else {                         // first solve of this shape: run it recording, then capture
+        pl = new_plan(S, h, ncols, trans, st);
+        HM_LU_CUDA(cudaMemcpyAsync(pl->xin, d_b, xb, cudaMemcpyDeviceToDevice, st));
+        pl->tape.record = true;
+        g_tape = &pl->tape;
+        try {
+          issue_solve(c, S, h, pl->xin, pl->xout, (int)ncols, trans, pl->Z, pl->xin);
+        } catch (...) {
+          g_tape = nullptr;
+          pl->tape.record = false;
+          throw;
+        }
+        g_tape = nullptr;
+        pl->tape.record = false;
+        HM_LU_CUDA(cudaMemcpyAsync(d_x, pl->xout, xb, cudaMemcpyDeviceToDevice, st));
+        capture_plan(S, h, pl, st);
       }
-      lu_scatter_rows_kernel<<<g, 256, 0, st>>>(X, W, S->P);
-      LU_LAUNCH_CHECK();
     }
   } catch (const LuError& e) {
     return fail(e.code, std::string("H\\y: ") + e.what());

@@ -194,3 +194,28 @@ def test_lu_copy_of_factorised():
     y = np.random.default_rng(5).random(2000)
     assert np.array_equal(L.solve(y), L2.solve(y))
     assert np.array_equal(L.P, L2.P)
+
+
+@pytest.mark.parametrize("mode", ["recursive", "tiles"])
+def test_captured_solve_replays(mode):
+    # the first solve of each shape (ncols, transposed) runs directly and is
+    # captured into a CUDA graph; later solves of that shape replay the graph
+    # on fresh right-hand sides.  More than 64 columns run directly every time.
+    import hmatrix as hm
+    n = 4096
+    prm = hm.Params(Geom=np.linspace(0, 10, n), Kernel=hm.Cauchy(1.0), MaxBlock=512, MinBlock=64, MaxRank=16,
+                    ConsMethod="aca2", εComp=1e-10, Tree="bisect", Shift=1.0, LuMode=mode)
+    c, H = hm.NewHmat(prm)
+    D = H.to_dense()
+    L = hm.lu(H)
+    rng = np.random.default_rng(11)
+    for shape in [(n,), (n, 3), (n, 70)]:
+        for trans in (False, True):
+            A = D.T if trans else D
+            ys = [rng.standard_normal(shape) for _ in range(3)]
+            xs = [L.solve(y, trans=trans) for y in ys]
+            for y, x in zip(ys, xs):
+                assert close(x, np.linalg.solve(A, y), 1e-9)
+            assert np.array_equal(L.solve(ys[0], trans=trans), xs[0])   # replay == first run
+    Xr, it, rr = L.solve_refined(rng.standard_normal((n, 2)), tol=1e-13, max_iter=5)
+    assert rr <= 1e-13
