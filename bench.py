@@ -52,6 +52,11 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-lu", action="store_true", help="skip the H-LU + solve leg")
     ap.add_argument("--lu-n", type=int, default=1 << 16, help="size of the H-LU + solve leg")
+    ap.add_argument("--rhs", default="16,64",
+                    help="column counts of the multi-RHS matvec leg (comma separated; empty to skip)")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="also run the batched uneven H-LU + solve leg with this many problems (256 in full)")
+    ap.add_argument("--batch-nthreads", type=int, default=0, help="host threads of the batched calls (0: auto)")
     return ap.parse_args()
 
 
@@ -83,8 +88,18 @@ class Clocks:
                  "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the first query initialises NVML, which can hold the driver for a
+            # while: let it finish before anything is timed
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 10 and self.proc.poll() is None:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
+        self.m0 = 0
+
+    def mark(self):
+        """Start of the timed region: samples before it are not reported."""
+        self.m0 = len(self.lines)
 
     def _read(self):
         for ln in self.proc.stdout:
@@ -100,7 +115,8 @@ class Clocks:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        use = self.lines[self.m0:] or self.lines[-1:]
+        for ln in use:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -237,8 +253,11 @@ def measure(H, a, torch, dist, world):
         dist.barrier()
     torch.cuda.synchronize()
     clocks.start()
-    time.sleep(0.3)
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.mark()
     e0.record(st)
     for _ in range(a.steps):
         step()
@@ -265,6 +284,53 @@ def measure(H, a, torch, dist, world):
     got = y.cpu().numpy()[rows]
     rel = float(np.linalg.norm(got - ex) / np.linalg.norm(ex))
     return ms, ph, ck, e2e_ms, rel
+
+
+def multi_rhs_leg(H, cols, steps, torch, bytes_1):
+    """H*X for X of c N(0,1) columns (seed 1): device time per call (CUDA
+    events over `steps` calls after 3 warm-up calls), the factor bytes
+    streamed per second, the equivalent single-column rate (c x the bytes
+    of one column's matvec per second), and the agreement with the
+    single-column kernel on the first and last columns."""
+    import ctypes as C
+    from hmatrix import _lib
+    L = _lib.lib()
+    st = torch.cuda.current_stream()
+    sp = C.c_void_p(st.cuda_stream or 1)
+    info = H.info()
+    out = {}
+    for c in cols:
+        g = torch.Generator(device="cuda").manual_seed(1)
+        X = torch.randn(c, H.n, generator=g, device="cuda", dtype=torch.float64)   # column-major n x c
+        Y = torch.empty_like(X)
+
+        def step():
+            _lib.check(L.hm_matvec(H._h, C.c_void_p(X.data_ptr()), C.c_void_p(Y.data_ptr()), c, 0,
+                                   _lib.HM_FLAG_DEVICE_PTRS, sp))
+        for _ in range(3):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            step()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        y1 = torch.empty(H.n, device="cuda", dtype=torch.float64)
+        err = 0.0
+        for j in (0, c - 1):
+            _lib.check(L.hm_matvec(H._h, C.c_void_p(X[j].data_ptr()), C.c_void_p(y1.data_ptr()), 1, 0,
+                                   _lib.HM_FLAG_DEVICE_PTRS, sp))
+            torch.cuda.synchronize()
+            err = max(err, float(torch.linalg.norm(Y[j] - y1) / torch.linalg.norm(y1)))
+        flops = 2.0 * c * (info.rk_entries + info.dense_entries)
+        out[str(c)] = {"ms": ms, "factor_GB/s": bytes_1 / (ms * 1e-3) / 1e9,
+                       "equiv_single_column_GB/s": c * bytes_1 / (ms * 1e-3) / 1e9,
+                       "fp64_GFLOP/s": flops / (ms * 1e-3) / 1e9, "rel_diff_vs_single_column": err}
+        del X, Y
+        torch.cuda.empty_cache()
+    return out
 
 
 def lu_solve_leg(n, torch):
@@ -294,6 +360,70 @@ def lu_solve_leg(n, torch):
                      "relres": float(np.linalg.norm(r) / np.linalg.norm(y)), "eps_trunc_lu": epslu or 1e-10}
         del L, H
         torch.cuda.empty_cache()
+    out["mixed_speedup"] = out["fp64"]["total_s"] / out["mixed"]["total_s"]
+    return out
+
+
+def batched_problems(count, seed=3, nmin=2 ** 10, nmax=2 ** 16):
+    """The batched uneven 1-D problems: n = round(2^U(log2 nmin, log2 nmax)),
+    points sorted U[0, L] with L ~ U[5, 20], K = 1/(1+((x-y)/l)^2) + delta_xy
+    with l ~ U[0.5, 2], one N(0,1) right-hand side each."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(round(2 ** rng.uniform(np.log2(nmin), np.log2(nmax))))
+        L = rng.uniform(5, 20)
+        ell = rng.uniform(0.5, 2)
+        x = np.sort(rng.uniform(0, L, n))
+        out.append((x, ell, rng.standard_normal(n)))
+    return out
+
+
+def batch_leg(count, torch, nthreads=0, budget_gb=90.0):
+    """All problems factored (lu!) and solved with FP64 refinement to a
+    relative residual <= 1e-10 through the batched entry points, in waves
+    whose factor memory (about 2.5 n^2 bytes a problem) fits the budget.
+    Timed: factorisation + refined solve of every problem (host right-hand
+    sides in, solutions out); construction is not timed."""
+    import hmatrix as hm
+    probs = batched_problems(count)
+    waves, cur, acc = [], [], 0.0
+    for i, (x, _, _) in enumerate(probs):
+        need = 2.5 * len(x) ** 2 / 1e9
+        if cur and acc + need > budget_gb:
+            waves.append(cur)
+            cur, acc = [], 0.0
+        cur.append(i)
+        acc += need
+    if cur:
+        waves.append(cur)
+    out = {"config": {"problems": count, "sum_n": int(sum(len(p[0]) for p in probs)),
+                      "n_range": [int(min(len(p[0]) for p in probs)), int(max(len(p[0]) for p in probs))],
+                      "kernel": "1/(1+((x-y)/l)^2) + delta_xy", "MaxBlock": 256, "MinBlock": 32, "MaxRank": 12,
+                      "aca_tol": 1e-10, "target_relres": 1e-10, "tree": "median bisection", "waves": len(waves),
+                      "host_threads": nthreads or "auto"}}
+    for name, epslu in (("fp64", 0.0), ("mixed", 1e-6)):
+        t_all, worst, steps = 0.0, 0.0, 0
+        for w in waves:
+            Hs, ys = [], []
+            for i in w:
+                x, ell, y = probs[i]
+                prm = hm.Params(Geom=x, Kernel=hm.Cauchy(ell), MaxBlock=256, MinBlock=32, MaxRank=12,
+                                ConsMethod="aca2", εComp=1e-10, Tree="bisect", Shift=1.0, εTruncLU=epslu,
+                                Device=torch.cuda.current_device())
+                Hs.append(hm.NewHmat(prm)[1])
+                ys.append(y)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            hm.lu_batch_(Hs, nthreads)
+            xs, it, rr = hm.solve_refined_batch(Hs, ys, tol=1e-10, max_iter=20, nthreads=nthreads)
+            t_all += time.perf_counter() - t0
+            worst = max(worst, float(rr.max()))
+            steps = max(steps, int(it.max()))
+            del Hs, xs
+            torch.cuda.empty_cache()
+        out[name] = {"total_s": t_all, "max_relres": worst, "max_refine_steps": steps,
+                     "eps_trunc_lu": epslu or 1e-10}
     out["mixed_speedup"] = out["fp64"]["total_s"] / out["mixed"]["total_s"]
     return out
 
@@ -331,6 +461,10 @@ def run_ours(a):
     traffic = None
     if tr and dom_name in tr:
         traffic = tr[dom_name] * p_bytes[dom]
+    multi = None
+    cols = [int(v) for v in a.rhs.split(",") if v.strip()]
+    if cols and world == 1:
+        multi = multi_rhs_leg(H, cols, max(3, min(a.steps, 10)), torch, bytes_mv)
     extra = {}
     if a.extra_precisions and world == 1:
         for s in ("f32", "bf16"):
@@ -353,6 +487,11 @@ def run_ours(a):
         H = None
         torch.cuda.empty_cache()
         lu = lu_solve_leg(a.lu_n, torch)
+    batch = None
+    if a.batch > 0 and world == 1:
+        H = None
+        torch.cuda.empty_cache()
+        batch = batch_leg(a.batch, torch, a.batch_nthreads)
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -379,8 +518,10 @@ def run_ours(a):
             "structure": {"n_rk": info.n_rk, "n_dense": info.n_dense, "rk_entries": info.rk_entries,
                           "dense_entries": info.dense_entries, "max_rank": info.max_rank,
                           "algorithmic_bytes": bytes_mv, "build_s": t_build},
+            "multi_rhs": multi,
             "extra_precisions": extra or None,
-            "lu_solve": lu}
+            "lu_solve": lu,
+            "batched_lu_solve": batch}
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

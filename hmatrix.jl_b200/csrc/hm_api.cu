@@ -2,7 +2,11 @@
 #include "hm_internal.h"
 
 #include <cstring>
+#include <mutex>
 #include <new>
+#include <set>
+#include <thread>
+#include <atomic>
 
 namespace hm {
 
@@ -12,6 +16,19 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 int fail(int code, const std::string& msg) {
   g_last_error = msg;
   return code;
+}
+
+cudaError_t smem_attr(const void* kernel, int bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({kernel, dev})) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done.insert({kernel, dev});
+  return e;
 }
 
 namespace {
@@ -62,6 +79,52 @@ struct IoBuf {
     return HM_OK;
   }
 };
+
+// Runs fn(i) for i in [0, count) on up to nthreads host threads (the calling
+// thread is one of them) and folds the per-problem statuses.
+template <typename F>
+int run_batch(hm_handle* const* hs, int64_t count, int32_t nthreads, int32_t* status, F fn) {
+  if (count < 0 || (count > 0 && !hs)) return fail(HM_ERR_ARG, "invalid batch");
+  if (count == 0) return HM_OK;
+  {
+    std::set<const hm_handle*> seen;
+    for (int64_t i = 0; i < count; ++i) {
+      if (!hs[i]) return fail(HM_ERR_ARG, "batch entry " + std::to_string(i) + " is NULL");
+      if (!seen.insert(hs[i]).second)
+        return fail(HM_ERR_ARG, "batch entry " + std::to_string(i) + " repeats a handle");
+    }
+  }
+  const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
+  const int64_t T = std::min<int64_t>(nthreads > 0 ? nthreads : std::min<int64_t>(hw, 16), count);
+  std::vector<int> st((size_t)count, HM_OK);
+  std::vector<std::string> msg((size_t)count);
+  std::atomic<int64_t> next{0};
+  auto worker = [&]() {
+    for (;;) {
+      const int64_t i = next.fetch_add(1);
+      if (i >= count) break;
+      st[i] = fn(i);
+      if (st[i] != HM_OK) msg[i] = g_last_error;     // this worker's own message
+    }
+  };
+  std::vector<std::thread> th;
+  try {
+    for (int64_t t = 1; t < T; ++t) th.emplace_back(worker);
+  } catch (const std::exception&) {
+    // fewer threads than asked: the ones running (and this one) take the rest
+  }
+  worker();
+  for (auto& t : th) t.join();
+  int first = HM_OK;
+  for (int64_t i = 0; i < count; ++i) {
+    if (status) status[i] = st[i];
+    if (st[i] != HM_OK && first == HM_OK) {
+      first = st[i];
+      fail(st[i], "problem " + std::to_string(i) + ": " + msg[i]);
+    }
+  }
+  return first;
+}
 
 }  // namespace
 }  // namespace hm
@@ -169,6 +232,7 @@ int hm_info(const hm_handle* h, hm_info_t* o) {
   o->matvec_bytes = (int64_t)eb * o->rk_entries + (int64_t)deb * o->dense_entries + 16 * h->n;
   o->n_row_groups = h->fwd.nwin;
   o->factorized = h->factorized ? 1 : 0;
+  if (h->lu) lu_describe(h, &o->lu_tiles, &o->lu_rank_cap);
   return HM_OK;
 }
 
@@ -218,17 +282,18 @@ int hm_matvec(hm_handle* h, const double* X, double* Y, int64_t ncols, int32_t t
   DeviceGuard g(h->device);
   cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
   const int64_t n = h->n;
-  if (flags & HM_FLAG_DEVICE_PTRS) {
-    for (int64_t c = 0; c < ncols; ++c) HM_TRY(matvec_device(h, X + c * n, Y + c * n, trans ? 1 : 0, st));
-    return HM_OK;
-  }
+  // one column: the single-vector kernels; a block: every factor streamed once per column block
+  auto run = [&](const double* dx, double* dy) -> int {
+    if (ncols == 1) return matvec_device(h, dx, dy, trans ? 1 : 0, st);
+    return matvec_multi_device(h, dx, dy, ncols, trans ? 1 : 0, st);
+  };
+  if (ncols == 0) return HM_OK;
+  if (flags & HM_FLAG_DEVICE_PTRS) return run(X, Y);
   IoBuf io{h};
-  HM_TRY(io.get(sizeof(double) * 2 * n));
-  for (int64_t c = 0; c < ncols; ++c) {
-    HM_CUDA_TRY(cudaMemcpyAsync(io.ptr, X + c * n, sizeof(double) * n, cudaMemcpyHostToDevice, st));
-    HM_TRY(matvec_device(h, io.ptr, io.ptr + n, trans ? 1 : 0, st));
-    HM_CUDA_TRY(cudaMemcpyAsync(Y + c * n, io.ptr + n, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
-  }
+  HM_TRY(io.get(sizeof(double) * 2 * n * ncols));
+  HM_CUDA_TRY(cudaMemcpyAsync(io.ptr, X, sizeof(double) * n * ncols, cudaMemcpyHostToDevice, st));
+  HM_TRY(run(io.ptr, io.ptr + n * ncols));
+  HM_CUDA_TRY(cudaMemcpyAsync(Y, io.ptr + n * ncols, sizeof(double) * n * ncols, cudaMemcpyDeviceToHost, st));
   HM_CUDA_TRY(cudaStreamSynchronize(st));
   return HM_OK;
 }
@@ -347,6 +412,35 @@ int hm_solve_refined(hm_handle* h, const double* B, double* X, int64_t ncols, do
   if (iters) *iters = it;
   if (relres) *relres = rr;
   return s;
+}
+
+int hm_batch_lu(hm_handle* const* hs, int64_t count, int32_t nthreads, int32_t* status) {
+  return run_batch(hs, count, nthreads, status, [&](int64_t i) { return hm_lu(hs[i]); });
+}
+
+int hm_batch_solve(hm_handle* const* hs, int64_t count, const double* const* B, double* const* X,
+                   int64_t ncols, uint32_t flags, int32_t nthreads, int32_t* status) {
+  if (count > 0 && (!B || !X)) return fail(HM_ERR_ARG, "NULL B or X");
+  return run_batch(hs, count, nthreads, status,
+                   [&](int64_t i) { return hm_solve(hs[i], B[i], X[i], ncols, flags, nullptr); });
+}
+
+int hm_batch_solve_refined(hm_handle* const* hs, int64_t count, const double* const* B,
+                           double* const* X, int64_t ncols, double tol, int32_t max_iter,
+                           uint32_t flags, int32_t nthreads, int32_t* status, int32_t* iters,
+                           double* relres) {
+  if (count > 0 && (!B || !X)) return fail(HM_ERR_ARG, "NULL B or X");
+  return run_batch(hs, count, nthreads, status, [&](int64_t i) {
+    return hm_solve_refined(hs[i], B[i], X[i], ncols, tol, max_iter, flags, nullptr,
+                            iters ? iters + i : nullptr, relres ? relres + i : nullptr);
+  });
+}
+
+int hm_batch_matvec(hm_handle* const* hs, int64_t count, const double* const* X, double* const* Y,
+                    int64_t ncols, int32_t trans, uint32_t flags, int32_t nthreads, int32_t* status) {
+  if (count > 0 && (!X || !Y)) return fail(HM_ERR_ARG, "NULL X or Y");
+  return run_batch(hs, count, nthreads, status,
+                   [&](int64_t i) { return hm_matvec(hs[i], X[i], Y[i], ncols, trans, flags, nullptr); });
 }
 
 int aca_wrapper(double* AA, double* UU, double* VV, int m, int n, double epsilon, int rank) {

@@ -288,7 +288,6 @@ int build_handle(hm_handle* h, const double* geom, int64_t ncl, const int64_t* c
 // order; the transposed plan reads the same data with A and B swapped.
 // ---------------------------------------------------------------------------
 int build_matvec_plans(hm_handle* h) {
-  const int64_t n = h->n;
   const int eb = elem_bytes(h->storage), deb = dense_elem_bytes(h->storage);
   const int64_t ncl = (int64_t)h->cl_s.size();
 
@@ -364,12 +363,16 @@ void free_handle_data(hm_handle* h) {
   fr(h->d_xs);
   fr(h->d_counter);
   fr(h->d_io);
+  fr(h->d_z);
+  fr(h->d_xm);
   free_mv_plan(h->fwd);
   free_mv_plan(h->bwd);
   h->d_geom = nullptr;
-  h->d_rk = h->d_dense = h->d_xs = nullptr;
+  h->d_rk = h->d_dense = h->d_xs = h->d_xm = nullptr;
+  h->d_z = nullptr;
   h->d_counter = nullptr;
   h->d_io = nullptr;
+  h->xs_bytes = h->io_bytes = h->xm_bytes = 0;
   lu_free(h);
 }
 

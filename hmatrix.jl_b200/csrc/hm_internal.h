@@ -18,6 +18,9 @@ namespace hm {
 // ---------------------------------------------------------------------------
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
+// Raises a kernel's dynamic shared-memory limit to `bytes` once per (kernel,
+// current device); safe to call from several host threads.
+cudaError_t smem_attr(const void* kernel, int bytes);
 
 #define HM_CUDA_TRY(expr)                                                      \
   do {                                                                         \
@@ -137,6 +140,9 @@ constexpr int MV_WROWS = 1024;         // rows per phase-2 window (8 warps x 32 
 struct MvPlan {
   P1Desc* d_p1 = nullptr;
   int64_t np1 = 0;
+  P1Desc* d_p1s = nullptr;         // the same descriptors ordered by input segment (multi-RHS phase 1; built on first use)
+  uint32_t* d_g1s = nullptr;       // groups of d_p1s sharing a segment (ng1 + 1 starts)
+  int64_t ng1 = 0;
   P2Desc* d_p2 = nullptr;
   int64_t np2 = 0;
   MvWin* d_win = nullptr;
@@ -183,6 +189,8 @@ struct hm_handle {
   int* d_counter = nullptr;        // work counters
   double* d_io = nullptr;          // staging for host pointers
   size_t io_bytes = 0;
+  void* d_xm = nullptr;            // multi-RHS matvec: row-major input block + phase-1 results
+  size_t xm_bytes = 0;
 
   hm::LuState* lu = nullptr;       // set once factorised
   bool factorized = false;
@@ -222,10 +230,14 @@ int apply_shift(hm_handle* h, double lambda);
 int apply_scale(hm_handle* h, double u);
 int copy_handle(const hm_handle* h, hm_handle** out);
 void free_handle_data(hm_handle* h);
+void lu_describe(const hm_handle* h, int64_t* tiles, int64_t* cap);
 
 // matvec (hm_matvec.cu)
 int matvec_device(hm_handle* h, const double* d_x, double* d_y, int trans, cudaStream_t st,
                   cudaEvent_t* ev = nullptr);
+// Y = H X (trans 0) or H' X (trans 1) for an n x ncols column-major block,
+// factors streamed once per column block (hm_matvec_multi.cu)
+int matvec_multi_device(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st);
 int exact_rows_device(hm_handle* h, const int64_t* d_rows, int64_t nrows,
                       const double* d_x, double* d_y, cudaStream_t st);
 

@@ -492,13 +492,8 @@ __global__ void __launch_bounds__(256) core_recompress_one_kernel(CoreJob J, int
 }
 
 int launch_core_one(const CoreJob& J, double eps_trunc, int* d_flags, cudaStream_t st) {
-  static bool attr_set = false;
   const size_t smem = (size_t)3 * RCORE_MAX * RCORE_MAX * sizeof(double);
-  if (!attr_set) {
-    HM_CUDA_TRY(cudaFuncSetAttribute(core_recompress_one_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
-    attr_set = true;
-  }
+  HM_CUDA_TRY(smem_attr((const void*)core_recompress_one_kernel, (int)smem));
   core_recompress_one_kernel<<<1, 256, smem, st>>>(J, RCORE_MAX, eps_trunc, d_flags);
   HM_CUDA_TRY(cudaGetLastError());
   return HM_OK;
@@ -510,12 +505,7 @@ int launch_core_recompress(const CoreJob* d_jobs, int njobs, int rmax, double ep
   if (rmax > RCORE_MAX) return fail(HM_ERR_UNSUPPORTED, "recompression core above " + std::to_string(RCORE_MAX));
   rmax = std::max(rmax, 1);
   size_t smem = (size_t)3 * rmax * rmax * sizeof(double);
-  static bool attr_set = false;
-  if (!attr_set) {
-    HM_CUDA_TRY(cudaFuncSetAttribute(core_recompress_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)((size_t)3 * RCORE_MAX * RCORE_MAX * sizeof(double))));
-    attr_set = true;
-  }
+  HM_CUDA_TRY(smem_attr((const void*)core_recompress_kernel, (int)((size_t)3 * RCORE_MAX * RCORE_MAX * sizeof(double))));
   // small cores: 2 warps per job, so that many jobs share an SM
   core_recompress_kernel<<<njobs, rmax <= 32 ? 64 : 256, smem, st>>>(d_jobs, rmax, eps_trunc, d_flags);
   HM_CUDA_TRY(cudaGetLastError());

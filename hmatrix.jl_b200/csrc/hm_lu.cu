@@ -535,13 +535,8 @@ static void trsm_lower(Ctx& c, View L, View X, bool unit) {
     LU_LAUNCH_CHECK();
     return;
   }
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(lu_trsm_lower_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             96 * 96 * (int)sizeof(double)) != cudaSuccess)
-      throw LuError(HM_ERR_CUDA, "trsm smem attribute");
-    attr = true;
-  }
+  if (smem_attr((const void*)lu_trsm_lower_kernel, 96 * 96 * (int)sizeof(double)) != cudaSuccess)
+    throw LuError(HM_ERR_CUDA, "trsm smem attribute");
   const size_t smem = L.rows <= 96 ? sizeof(double) * (size_t)L.rows * L.rows : 0;
   lu_trsm_lower_kernel<<<(X.cols + 127) / 128, 128, smem, c.st>>>(L, X, unit ? 1 : 0);
   LU_LAUNCH_CHECK();
@@ -557,12 +552,8 @@ static void getrf(Ctx& c, View C, int64_t goff) {
   }
   const size_t smem = sizeof(double) * (size_t)m * m + sizeof(int) * m;
   if (smem > 200 * 1024) throw LuError(HM_ERR_UNSUPPORTED, "diagonal leaf above 150 rows (MinBlock too large)");
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(lu_getrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
-      throw LuError(HM_ERR_CUDA, "getrf smem attribute");
-    attr = true;
-  }
+  if (smem_attr((const void*)lu_getrf_kernel, 200 * 1024) != cudaSuccess)
+    throw LuError(HM_ERR_CUDA, "getrf smem attribute");
   lu_getrf_kernel<<<1, 256, smem, c.st>>>(C, c.P, goff, c.flags);
   LU_LAUNCH_CHECK();
 }
@@ -1267,31 +1258,30 @@ struct TileLU {
 };
 
 // tile structure of the handle, or false when the partition has no such level
-static bool tile_structure(const hm_handle* h, std::vector<int32_t>& gcl, std::vector<int32_t>& diag_node) {
-  const int64_t ncl = (int64_t)h->cl_s.size();
-  std::vector<char> is_row(ncl, 0);
-  for (auto& L : h->leaves) is_row[L.s] = 1;
-  std::vector<char> covered(ncl, 0);
-  gcl.clear();
-  for (int64_t c = 0; c < ncl; ++c) {
-    if (!covered[c] && is_row[c]) gcl.push_back((int32_t)c);
-    if (h->cl_left[c] >= 0) {
-      const char cv = covered[c] || is_row[c];
-      covered[h->cl_left[c]] = cv;
-      covered[h->cl_right[c]] = cv;
-    }
-  }
-  std::sort(gcl.begin(), gcl.end(), [&](int32_t a, int32_t b) { return h->cl_s[a] < h->cl_s[b]; });
+// A tiling of [0, n) by clusters gcl (sorted by start) can run the tile
+// schedule when every leaf off the tile diagonal is a low-rank leaf whose rows
+// and columns are unions of whole tiles (a leaf spanning several tiles is
+// loaded as its tile parts, which keep its rank) and every diagonal tile is a
+// node of the block tree (leaves inside it stay in its recursive tree).
+static bool tile_check(const hm_handle* h, const std::vector<int32_t>& gcl, std::vector<int32_t>& diag_node) {
   const int T = (int)gcl.size();
   if (T < 2) return false;
+  if (h->cl_s[gcl[0]] != 0 || h->cl_e[gcl[T - 1]] != h->n) return false;
+  for (int i = 1; i < T; ++i)
+    if (h->cl_s[gcl[i]] != h->cl_e[gcl[i - 1]]) return false;
   std::vector<int64_t> st(T);
   for (int i = 0; i < T; ++i) st[i] = h->cl_s[gcl[i]];
   auto tile_of = [&](int64_t r) { return (int)(std::upper_bound(st.begin(), st.end(), r) - st.begin()) - 1; };
+  auto aligned = [&](int64_t a, int64_t len, int t0, int t1) { return a == st[t0] && a + len == h->cl_e[gcl[t1]]; };
   for (auto& L : h->leaves) {
-    const int i = tile_of(L.row0), j = tile_of(L.col0);
-    if (i == j) continue;
-    if (L.type != T_RK || L.s != gcl[i] || L.t != gcl[j]) return false;
+    const int i0 = tile_of(L.row0), i1 = tile_of(L.row0 + L.m - 1);
+    const int j0 = tile_of(L.col0), j1 = tile_of(L.col0 + L.n - 1);
+    if (i0 == i1 && j0 == j1 && i0 == j0) continue;            // inside a diagonal tile
+    const bool overlap = !(i1 < j0 || j1 < i0);                 // would cover part of a diagonal tile
+    if (overlap || L.type != T_RK || !aligned(L.row0, L.m, i0, i1) || !aligned(L.col0, L.n, j0, j1))
+      return false;
   }
+  const int64_t ncl = (int64_t)h->cl_s.size();
   diag_node.assign(T, -1);
   std::vector<int32_t> tile_of_cluster(ncl, -1);
   for (int i = 0; i < T; ++i) tile_of_cluster[gcl[i]] = i;
@@ -1302,6 +1292,48 @@ static bool tile_structure(const hm_handle* h, std::vector<int32_t>& gcl, std::v
   for (int i = 0; i < T; ++i)
     if (diag_node[i] < 0) return false;
   return true;
+}
+
+// The tile level.  First candidate: the highest clusters that are the row
+// cluster of some leaf (for a balanced partition, the clusters of the first
+// admissible level; for a KMeans tree the tiles may sit at several depths).
+// Otherwise the shallowest depth whose clusters form a valid tiling (a median
+// bisection of an n that is not a power of two mixes cluster sizes on both
+// sides of MaxBlock on one level, so the admissible blocks start one level
+// lower on part of it).
+static bool tile_structure(const hm_handle* h, std::vector<int32_t>& gcl, std::vector<int32_t>& diag_node) {
+  const int64_t ncl = (int64_t)h->cl_s.size();
+  auto by_start = [&](int32_t a, int32_t b) { return h->cl_s[a] < h->cl_s[b]; };
+  {
+    std::vector<char> is_row(ncl, 0), covered(ncl, 0);
+    for (auto& L : h->leaves) is_row[L.s] = 1;
+    gcl.clear();
+    for (int64_t c = 0; c < ncl; ++c) {
+      if (!covered[c] && is_row[c]) gcl.push_back((int32_t)c);
+      if (h->cl_left[c] >= 0) {
+        const char cv = covered[c] || is_row[c];
+        covered[h->cl_left[c]] = cv;
+        covered[h->cl_right[c]] = cv;
+      }
+    }
+    std::sort(gcl.begin(), gcl.end(), by_start);
+    if (tile_check(h, gcl, diag_node)) return true;
+  }
+  int maxd = 0;
+  for (int64_t c = 0; c < ncl; ++c) maxd = std::max(maxd, (int)h->cl_depth[c]);
+  for (int d = 1; d <= maxd; ++d) {
+    gcl.clear();
+    int64_t cover = 0;
+    for (int64_t c = 0; c < ncl; ++c)
+      if (h->cl_depth[c] == d) {
+        gcl.push_back((int32_t)c);
+        cover += h->cl_e[c] - h->cl_s[c];
+      }
+    if (cover != h->n) return false;            // a cluster leaf above depth d: no deeper level covers
+    std::sort(gcl.begin(), gcl.end(), by_start);
+    if (tile_check(h, gcl, diag_node)) return true;
+  }
+  return false;
 }
 
 static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vector<int32_t>& gcl,
@@ -1333,15 +1365,21 @@ static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vecto
   Loader ld;
   const char* base = (const char*)h->d_rk;
   for (auto& L : h->leaves) {
-    const int i = tile_of(L.row0), j = tile_of(L.col0);
-    if (i == j) continue;
+    const int i0 = tile_of(L.row0), i1 = tile_of(L.row0 + L.m - 1);
+    const int j0 = tile_of(L.col0), j1 = tile_of(L.col0 + L.n - 1);
+    if (i0 == i1 && j0 == j1 && i0 == j0) continue;            // part of a diagonal tile's tree
     if (L.k > cap) throw LuError(HM_ERR_RANK, "leaf rank above the H-LU rank capacity");
-    kh[i * T + j] = L.k;
     const int64_t npad = col_pad(L.n, eb), mpad = col_pad(L.m, eb);
-    ld.jobs.push_back(LoadJob{base + L.off * eb, npad, L.n, L.k, h->storage, TL.Bj(i, j, cap), L.n, cap,
-                              nullptr, 0});
-    ld.jobs.push_back(LoadJob{base + (L.off + npad * L.k) * eb, mpad, L.m, L.k, h->storage, TL.Ai(i, j, cap),
-                              L.m, cap, nullptr, 0});
+    // a leaf spanning several tiles: tile (i, j) holds rows of A and of B
+    for (int i = i0; i <= i1; ++i)
+      for (int j = j0; j <= j1; ++j) {
+        kh[i * T + j] = L.k;
+        const int64_t ro = TL.start[i] - L.row0, co = TL.start[j] - L.col0;
+        ld.jobs.push_back(LoadJob{base + (L.off + co) * eb, npad, (int)TL.size[j], L.k, h->storage,
+                                  TL.Bj(i, j, cap), TL.size[j], cap, nullptr, 0});
+        ld.jobs.push_back(LoadJob{base + (L.off + npad * L.k + ro) * eb, mpad, (int)TL.size[i], L.k, h->storage,
+                                  TL.Ai(i, j, cap), TL.size[i], cap, nullptr, 0});
+      }
   }
   if (cudaMemcpyAsync(TL.kmat, kh.data(), sizeof(int32_t) * T * T, cudaMemcpyHostToDevice, c.st) != cudaSuccess)
     throw LuError(HM_ERR_CUDA, "rank upload");
@@ -1903,6 +1941,11 @@ int lu_solve_refined(hm_handle* h, const double* d_b, double* d_x, int64_t ncols
   if (iters) *iters = it;
   if (relres) *relres = worst;
   return status;
+}
+
+void lu_describe(const hm_handle* h, int64_t* tiles, int64_t* cap) {
+  *tiles = h->lu && h->lu->tile ? h->lu->tile->T : 0;
+  *cap = h->lu ? h->lu->cap : 0;
 }
 
 int lu_perm(const hm_handle* h, int64_t* P) {

@@ -333,6 +333,8 @@ __global__ void __launch_bounds__(P2_WARPS * 32) mv_phase2_kernel(const MvWin* _
 // ---------------------------------------------------------------------------
 void free_mv_plan(MvPlan& p) {
   if (p.d_p1) cudaFree(p.d_p1);
+  if (p.d_p1s) cudaFree(p.d_p1s);
+  if (p.d_g1s) cudaFree(p.d_g1s);
   if (p.d_p2) cudaFree(p.d_p2);
   if (p.d_win) cudaFree(p.d_win);
   p = MvPlan{};

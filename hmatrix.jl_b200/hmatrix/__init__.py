@@ -330,6 +330,80 @@ def lu_(H: Hmat):
     return H.lu_()
 
 
+# -- independent problems in one call (no counterpart in the reference) ------
+def _handles(Hs):
+    return (C.c_void_p * len(Hs))(*[H._h for H in Hs])
+
+
+def _batch_check(status, st):
+    if status != _lib.HM_OK:
+        raise HmError(status, _lib.last_error())
+
+
+def lu_batch_(Hs, nthreads=0):
+    """``lu!`` on every H-matrix of ``Hs`` in one library call; the problems
+    run concurrently, each on its own stream."""
+    Hs = list(Hs)
+    st = np.zeros(len(Hs), np.int32)
+    _batch_check(lib().hm_batch_lu(_handles(Hs), len(Hs), int(nthreads), _ptr(st)), st)
+    return Hs
+
+
+def lu_batch(Hs, nthreads=0):
+    """``lu`` (factorised copies) of every H-matrix of ``Hs``."""
+    return lu_batch_([H.copy() for H in Hs], nthreads)
+
+
+def _rhs_list(Ls, ys):
+    Bs = [np.asfortranarray(np.asarray(y, dtype=np.float64).reshape(L.n, -1)) for L, y in zip(Ls, ys)]
+    nc = {B.shape[1] for B in Bs}
+    if len(nc) > 1:
+        raise HmError(_lib.HM_ERR_ARG, "every problem needs the same number of right-hand sides")
+    Xs = [np.zeros_like(B, order="F") for B in Bs]
+    pb = (C.c_void_p * len(Bs))(*[B.ctypes.data for B in Bs])
+    px = (C.c_void_p * len(Xs))(*[X.ctypes.data for X in Xs])
+    return Bs, Xs, pb, px, (nc.pop() if nc else 1)
+
+
+def solve_batch(Ls, ys, trans=False, nthreads=0):
+    """``L\\y`` for every factorised ``L`` of ``Ls`` with its right-hand side."""
+    Ls, ys = list(Ls), list(ys)
+    if len(Ls) != len(ys):
+        raise HmError(_lib.HM_ERR_ARG, "one right-hand side per problem")
+    Bs, Xs, pb, px, nc = _rhs_list(Ls, ys)
+    st = np.zeros(len(Ls), np.int32)
+    _batch_check(lib().hm_batch_solve(_handles(Ls), len(Ls), pb, px, nc,
+                                      _lib.HM_FLAG_TRANS if trans else 0, int(nthreads), _ptr(st)), st)
+    return [X.reshape(np.shape(y)) for X, y in zip(Xs, ys)]
+
+
+def solve_refined_batch(Ls, ys, tol=1e-10, max_iter=10, trans=False, nthreads=0):
+    """Refined solves of every problem; returns (xs, refinement steps, residuals)."""
+    Ls, ys = list(Ls), list(ys)
+    if len(Ls) != len(ys):
+        raise HmError(_lib.HM_ERR_ARG, "one right-hand side per problem")
+    Bs, Xs, pb, px, nc = _rhs_list(Ls, ys)
+    st = np.zeros(len(Ls), np.int32)
+    it = np.zeros(len(Ls), np.int32)
+    rr = np.zeros(len(Ls), np.float64)
+    _batch_check(lib().hm_batch_solve_refined(_handles(Ls), len(Ls), pb, px, nc, float(tol), int(max_iter),
+                                              _lib.HM_FLAG_TRANS if trans else 0, int(nthreads), _ptr(st),
+                                              _ptr(it), _ptr(rr)), st)
+    return [X.reshape(np.shape(y)) for X, y in zip(Xs, ys)], it, rr
+
+
+def matvec_batch(Hs, xs, trans=False, nthreads=0):
+    """``H*x`` for every H-matrix of ``Hs`` with its vector."""
+    Hs, xs = list(Hs), list(xs)
+    if len(Hs) != len(xs):
+        raise HmError(_lib.HM_ERR_ARG, "one vector per problem")
+    Bs, Ys, pb, py, nc = _rhs_list(Hs, xs)
+    st = np.zeros(len(Hs), np.int32)
+    _batch_check(lib().hm_batch_matvec(_handles(Hs), len(Hs), pb, py, nc, int(bool(trans)), 0, int(nthreads),
+                                       _ptr(st)), st)
+    return [Y.reshape(np.shape(x)) for Y, x in zip(Ys, xs)]
+
+
 def getl(A, unitdiag=True):
     """src/hlu.jl:193-199."""
     L = np.tril(A)

@@ -31,6 +31,7 @@ EXPORTED = [
     "hm_version", "hm_last_error", "hm_default_params", "hm_new", "hm_destroy", "hm_info",
     "hm_leaves", "hm_leaf_factors", "hm_to_dense", "hm_matvec", "hm_matvec_profile", "hm_exact_rows",
     "hm_add_identity", "hm_scale", "hm_copy", "hm_lu", "hm_lu_perm", "hm_solve", "hm_solve_refined",
+    "hm_batch_lu", "hm_batch_solve", "hm_batch_solve_refined", "hm_batch_matvec",
     "aca_wrapper",
     "aca_wrapper_noalloc",
 ]
@@ -52,7 +53,8 @@ class hm_info_t(C.Structure):
         ("n", C.c_int64), ("n_dense", C.c_int64), ("n_rk", C.c_int64), ("depth", C.c_int64),
         ("compress_ratio", C.c_double), ("dense_entries", C.c_int64), ("rk_entries", C.c_int64),
         ("max_rank", C.c_int64), ("pool_bytes", C.c_int64), ("matvec_bytes", C.c_int64),
-        ("n_row_groups", C.c_int64), ("factorized", C.c_int64), ("reserved", C.c_int64 * 4),
+        ("n_row_groups", C.c_int64), ("factorized", C.c_int64), ("lu_tiles", C.c_int64),
+        ("lu_rank_cap", C.c_int64), ("reserved", C.c_int64 * 2),
     ]
 
 
@@ -97,6 +99,11 @@ def lib():
     L.hm_solve.argtypes = [vp, vp, vp, C.c_int64, C.c_uint32, vp]
     L.hm_solve_refined.argtypes = [vp, vp, vp, C.c_int64, C.c_double, C.c_int32, C.c_uint32, vp,
                                    C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+    L.hm_batch_lu.argtypes = [vp, C.c_int64, C.c_int32, vp]
+    L.hm_batch_solve.argtypes = [vp, C.c_int64, vp, vp, C.c_int64, C.c_uint32, C.c_int32, vp]
+    L.hm_batch_solve_refined.argtypes = [vp, C.c_int64, vp, vp, C.c_int64, C.c_double, C.c_int32, C.c_uint32,
+                                         C.c_int32, vp, vp, vp]
+    L.hm_batch_matvec.argtypes = [vp, C.c_int64, vp, vp, C.c_int64, C.c_int32, C.c_uint32, C.c_int32, vp]
     L.aca_wrapper.argtypes = [pd, pd, pd, C.c_int, C.c_int, C.c_double, C.c_int]
     L.aca_wrapper.restype = C.c_int
     L.aca_wrapper_noalloc.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_double, C.c_int, vp]

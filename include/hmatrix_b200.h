@@ -98,7 +98,9 @@ typedef struct hm_info_t {
     int64_t matvec_bytes;     /* algorithmic bytes of one single-RHS matvec    */
     int64_t n_row_groups;
     int64_t factorized;       /* 1 after lu!                                   */
-    int64_t reserved[4];
+    int64_t lu_tiles;         /* after lu!: tiles of the tile schedule (0: the recursion ran) */
+    int64_t lu_rank_cap;      /* after lu!: column capacity of the low-rank factors */
+    int64_t reserved[2];
 } hm_info_t;
 
 typedef struct hm_handle hm_handle;
@@ -198,6 +200,33 @@ int hm_solve(hm_handle* h, const double* B, double* X, int64_t ncols,
 int hm_solve_refined(hm_handle* h, const double* B, double* X, int64_t ncols,
                      double tol, int32_t max_iter, uint32_t flags, void* stream,
                      int32_t* iters, double* relres);
+
+/* ---- independent problems in one call (no counterpart in the reference,
+ * whose Julia code handles one H-matrix at a time).  hs holds `count`
+ * distinct handles; each is worked on its own stream by one of `nthreads`
+ * host threads (0: min(hardware threads, 16)), so the GPU overlaps the
+ * problems.  status (optional, count entries) receives each problem's status;
+ * the return value is HM_OK or the first failing problem's status, with
+ * hm_last_error naming the problem.  A handle listed twice is an error. */
+
+/* lu!(H) on every handle (src/hlu.jl:465-521 each). */
+int hm_batch_lu(hm_handle* const* hs, int64_t count, int32_t nthreads, int32_t* status);
+
+/* H\y on every factorized handle: B[i], X[i] are n_i x ncols column-major
+ * (host, or device with HM_FLAG_DEVICE_PTRS); HM_FLAG_TRANS solves with H'. */
+int hm_batch_solve(hm_handle* const* hs, int64_t count, const double* const* B, double* const* X,
+                   int64_t ncols, uint32_t flags, int32_t nthreads, int32_t* status);
+
+/* hm_solve_refined on every factorized handle; iters and relres (optional,
+ * count entries) receive each problem's refinement steps and residual. */
+int hm_batch_solve_refined(hm_handle* const* hs, int64_t count, const double* const* B,
+                           double* const* X, int64_t ncols, double tol, int32_t max_iter,
+                           uint32_t flags, int32_t nthreads, int32_t* status, int32_t* iters,
+                           double* relres);
+
+/* H*y on every handle (src/harithm.jl:317-329 each), host or device X[i], Y[i]. */
+int hm_batch_matvec(hm_handle* const* hs, int64_t count, const double* const* X, double* const* Y,
+                    int64_t ncols, int32_t trans, uint32_t flags, int32_t nthreads, int32_t* status);
 
 /* Drop-in for the reference's native entry point
  * int aca_wrapper(double*, double*, double*, int, int, double, int)
