@@ -1255,6 +1255,15 @@ struct TileLU {
   BP hold;                               // owns the panel memory
   double* Ai(int i, int j, int cap) const { return Ap[i] + (int64_t)j * cap * size[i]; }
   double* Bj(int i, int j, int cap) const { return Bp[j] + (int64_t)i * cap * size[j]; }
+  // for the sweep solve (built on the first solve): the inverses of the
+  // diagonal tiles' unit-lower L and upper U, each stored column-major and
+  // row-major, and device tables of the panels
+  BP sweep_hold;
+  const double** d_Ap = nullptr;
+  const double** d_Bp = nullptr;
+  const double** d_inv[4] = {nullptr, nullptr, nullptr, nullptr};   // see sweep_apply_inverse
+  int64_t* d_start = nullptr;
+  int32_t* d_size = nullptr;
 };
 
 // tile structure of the handle, or false when the partition has no such level
@@ -1480,7 +1489,270 @@ static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vecto
 }
 
 // y = P b, forward (unit L), backward (U) tile by tile; trans: U' then L'
-static void tile_solve(Ctx& c, const TileLU& TL, View X, bool trans, double* Zext = nullptr) {
+// ---- sweep solve ---------------------------------------------------------
+// The triangular solves over the tile level as one kernel per tile: step k of
+// a sweep finishes tile k (the update from the tile finished at step k-1, then
+// the diagonal tile's triangular solve) in CTA 0, while the other CTAs apply
+// the same finished tile's update to every later tile: 2T launches a solve.
+// The diagonal solves multiply by the inverses of the diagonal tiles' L and U
+// factors (computed once from the factored tiles), so a step has no
+// row-by-row dependency chain.
+constexpr int SW_THREADS = 256;
+
+struct SweepTab {
+  const double* const* Ap;
+  const double* const* Bp;
+  const double* const* Inv[4];   // per tile, the matrix of sweep_apply_inverse for each `which`
+  const int64_t* start;
+  const int32_t* size;
+  const int32_t* kmat;
+  int T, cap;
+};
+
+// y_i -= P (Q' y_s): non-transposed P = A_is, Q = B_is (tile (i,s) = A B');
+// transposed P = B_si, Q = A_si (tile (s,i)' = B A')
+__device__ void sweep_update(const SweepTab& t, double* Y, int64_t ldy, int nc, int i, int s, bool trans,
+                             double* zsh) {
+  const int Si = t.size[i], Ss = t.size[s];
+  const double* P;
+  const double* Q;
+  int r;
+  if (!trans) {
+    P = t.Ap[i] + (int64_t)s * t.cap * Si;
+    Q = t.Bp[s] + (int64_t)i * t.cap * Ss;
+    r = t.kmat[i * t.T + s];
+  } else {
+    P = t.Bp[i] + (int64_t)s * t.cap * Si;
+    Q = t.Ap[s] + (int64_t)i * t.cap * Ss;
+    r = t.kmat[s * t.T + i];
+  }
+  if (r <= 0) return;
+  const double* ys = Y + t.start[s];
+  double* yi = Y + t.start[i];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int qc = warp; qc < r * nc; qc += SW_THREADS / 32) {
+    const int q = qc % r, cc = qc / r;
+    double acc = 0.0;
+    for (int row = lane; row < Ss; row += 32) acc = fma(Q[row + (int64_t)q * Ss], ys[row + cc * ldy], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) zsh[q + cc * r] = acc;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < Si * nc; e += SW_THREADS) {
+    const int row = e % Si, cc = e / Si;
+    double acc = 0.0;
+    for (int q = 0; q < r; ++q) acc = fma(P[row + (int64_t)q * Si], zsh[q + cc * r], acc);
+    yi[row + cc * ldy] -= acc;
+  }
+  __syncthreads();
+}
+
+// y <- M y with M[q*S + r] = M(r, q) (the inverse stored so that consecutive
+// rows are consecutive in memory): which 0 L^-1 and 2 (U^-1)' are lower
+// triangular, 1 U^-1 and 3 (L^-1)' upper.  A thread per row, loads coalesced
+// over the rows; column chunks of y are staged in shared memory (the product
+// is not in place).
+__device__ void sweep_apply_inverse(const double* M, int S, int which, double* y, int64_t ldy, int nc,
+                                    double* ysh, int chunk) {
+  const bool lower = which == 0 || which == 2;
+  for (int c0 = 0; c0 < nc; c0 += chunk) {
+    const int ncc = min(chunk, nc - c0);
+    for (int e = threadIdx.x; e < S * ncc; e += SW_THREADS) ysh[e] = y[e % S + (int64_t)(c0 + e / S) * ldy];
+    __syncthreads();
+    for (int e = threadIdx.x; e < S * ncc; e += SW_THREADS) {
+      const int r = e % S, cc = e / S;
+      const int q0 = lower ? 0 : r, q1 = lower ? r + 1 : S;
+      const double* ys = ysh + cc * S;
+      double acc = 0.0;
+#pragma unroll 8
+      for (int q = q0; q < q1; ++q) acc = fma(M[(int64_t)q * S + r], ys[q], acc);
+      y[r + (int64_t)(c0 + cc) * ldy] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+// which: 0 L (forward), 1 U (backward), 2 U' (forward), 3 L' (backward)
+__global__ void __launch_bounds__(SW_THREADS) lu_sweep_kernel(SweepTab t, double* Y, int64_t ldy, int nc, int k,
+                                                              int dir, int which, int chunk) {
+  extern __shared__ double sh[];
+  double* zsh = sh;                                  // cap x nc
+  double* ysh = sh + (size_t)t.cap * nc;             // S x chunk
+  const bool trans = which >= 2;
+  const int s = k - dir;
+  const bool has_src = s >= 0 && s < t.T;
+  if (blockIdx.x == 0) {
+    if (has_src) sweep_update(t, Y, ldy, nc, k, s, trans, zsh);
+    sweep_apply_inverse(t.Inv[which][k], t.size[k], which, Y + t.start[k], ldy, nc, ysh, chunk);
+  } else if (has_src) {
+    sweep_update(t, Y, ldy, nc, k + dir * (int)blockIdx.x, s, trans, zsh);
+  }
+}
+
+// dense copy of the factored diagonal tiles' leaves (dense or low-rank)
+struct DensJob {
+  double* dst;
+  int64_t ldd;
+  const double* C;
+  int64_t ldc;
+  const double* A;
+  int64_t lda;
+  const double* B;
+  int64_t ldb;
+  const int32_t* k;
+  int m, n, type;
+};
+__global__ void lu_densify_batch_kernel(const DensJob* __restrict__ jobs) {
+  const DensJob J = jobs[blockIdx.x];
+  const int k = J.type == T_RK ? *J.k : 0;
+  for (int64_t e = threadIdx.x; e < (int64_t)J.m * J.n; e += blockDim.x) {
+    const int i = (int)(e % J.m), j = (int)(e / J.m);
+    double v;
+    if (J.type == T_DENSE) {
+      v = J.C[i + (int64_t)j * J.ldc];
+    } else {
+      v = 0.0;
+      for (int q = 0; q < k; ++q) v = fma(J.A[i + (int64_t)q * J.lda], J.B[j + (int64_t)q * J.ldb], v);
+    }
+    J.dst[i + (int64_t)j * J.ldd] = v;
+  }
+}
+
+static void densify_jobs(const Blk& H, double* dst, int64_t ldd, std::vector<DensJob>& out) {
+  if (H.type == T_H) {
+    const int m = H.ch[0]->m, n = H.ch[0]->n;
+    densify_jobs(*H.ch[0], dst, ldd, out);
+    densify_jobs(*H.ch[1], dst + (int64_t)n * ldd, ldd, out);
+    densify_jobs(*H.ch[2], dst + m, ldd, out);
+    densify_jobs(*H.ch[3], dst + m + (int64_t)n * ldd, ldd, out);
+    return;
+  }
+  out.push_back(DensJob{dst, ldd, H.C, H.ldc, H.A, H.lda, H.B, H.ldb, H.k, H.m, H.n, H.type});
+}
+
+// Inverses of the unit-lower L (upper = 0) or the upper U (upper = 1) of the
+// packed S x S tiles D (column-major), one thread per column of the inverse,
+// written row-major to W (W[i*S + j] = inverse(i, j)) and column-major to Wc.
+// All threads of a tile run the same substitution, so the reads of D are
+// broadcasts and the reads and writes of W are coalesced.
+__global__ void lu_tri_inverse_kernel(const double* const* __restrict__ D, double* const* __restrict__ W,
+                                      double* const* __restrict__ Wc, const int32_t* __restrict__ size, int upper) {
+  const int tile = blockIdx.y;
+  const int S = size[tile];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (blockIdx.x * blockDim.x >= S) return;
+  const double* d = D[tile];
+  double* w = W[tile];
+  double* wc = Wc[tile];
+  const bool act = j < S;
+  if (!upper) {
+    for (int i = 0; i < S; ++i) {
+      double s = (i == j) ? 1.0 : 0.0;
+      for (int l = 0; l < i; ++l) s = fma(-d[i + (int64_t)l * S], act ? w[(int64_t)l * S + j] : 0.0, s);
+      if (act) {
+        const double v = (i < j) ? 0.0 : s;
+        w[(int64_t)i * S + j] = v;
+        wc[i + (int64_t)j * S] = v;
+      }
+    }
+  } else {
+    for (int i = S - 1; i >= 0; --i) {
+      double s = (i == j) ? 1.0 : 0.0;
+      for (int l = i + 1; l < S; ++l) s = fma(-d[i + (int64_t)l * S], act ? w[(int64_t)l * S + j] : 0.0, s);
+      if (act) {
+        const double v = (i > j) ? 0.0 : s / d[i + (int64_t)i * S];
+        w[(int64_t)i * S + j] = v;
+        wc[i + (int64_t)j * S] = v;
+      }
+    }
+  }
+}
+
+// inverse factors and device tables, once per factorisation
+static void ensure_sweep(Ctx& c, TileLU& TL) {
+  if (TL.d_inv[0]) return;
+  const int T = TL.T;
+  auto hold = std::make_shared<Blk>();
+  hold->st = c.st;
+  Blk tmp;
+  tmp.st = c.st;
+  int smax = 0;
+  std::vector<double*> D(T);
+  std::vector<const double*> inv[4];         // Lc, Uc, Ur, Lr: the matrices of which = 0..3
+  std::vector<DensJob> jobs;
+  for (int k = 0; k < T; ++k) {
+    const int S = (int)TL.size[k];
+    smax = std::max(smax, S);
+    D[k] = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)S * S);
+    for (int w = 0; w < 4; ++w) inv[w].push_back((double*)dmalloc(c, *hold, sizeof(double) * (size_t)S * S));
+    densify_jobs(*TL.diag[k], D[k], S, jobs);
+  }
+  for (size_t b = 0; b < jobs.size(); b += 65535) {
+    const size_t nb = std::min<size_t>(65535, jobs.size() - b);
+    std::vector<DensJob> part(jobs.begin() + b, jobs.begin() + b + nb);
+    DensJob* dj = upload_jobs(c, tmp, part);
+    lu_densify_batch_kernel<<<(unsigned)nb, 256, 0, c.st>>>(dj);
+    LU_LAUNCH_CHECK();
+  }
+  std::vector<int32_t> sz(T);
+  for (int k = 0; k < T; ++k) sz[k] = (int32_t)TL.size[k];
+  std::vector<const double*> Ap(TL.Ap.begin(), TL.Ap.end()), Bp(TL.Bp.begin(), TL.Bp.end());
+  auto up = [&](const void* src, size_t bytes) {
+    void* d = dmalloc(c, *hold, bytes);
+    if (cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, c.st) != cudaSuccess)
+      throw LuError(HM_ERR_CUDA, "sweep tables");
+    return d;
+  };
+  double** dD = (double**)dmalloc(c, tmp, sizeof(void*) * T);
+  if (cudaMemcpyAsync(dD, D.data(), sizeof(void*) * T, cudaMemcpyHostToDevice, c.st) != cudaSuccess)
+    throw LuError(HM_ERR_CUDA, "sweep tables");
+  TL.d_Ap = (const double**)up(Ap.data(), sizeof(void*) * T);
+  TL.d_Bp = (const double**)up(Bp.data(), sizeof(void*) * T);
+  for (int w = 0; w < 4; ++w) TL.d_inv[w] = (const double**)up(inv[w].data(), sizeof(void*) * T);
+  TL.d_start = (int64_t*)up(TL.start.data(), sizeof(int64_t) * T);
+  TL.d_size = (int32_t*)up(sz.data(), sizeof(int32_t) * T);
+  const dim3 g((smax + 127) / 128, T);
+  // L^-1: row-major (which 3) and column-major (which 0); U^-1: row-major (2), column-major (1)
+  lu_tri_inverse_kernel<<<g, 128, 0, c.st>>>(dD, (double* const*)TL.d_inv[3], (double* const*)TL.d_inv[0],
+                                             TL.d_size, 0);
+  LU_LAUNCH_CHECK();
+  lu_tri_inverse_kernel<<<g, 128, 0, c.st>>>(dD, (double* const*)TL.d_inv[2], (double* const*)TL.d_inv[1],
+                                             TL.d_size, 1);
+  LU_LAUNCH_CHECK();
+  if (cudaStreamSynchronize(c.st) != cudaSuccess) throw LuError(HM_ERR_CUDA, "sweep set-up");
+  TL.sweep_hold = hold;
+}
+
+static void tile_solve(Ctx& c, const TileLU& TL, View X, bool trans, double* Zext);
+
+// the two sweeps of a\y (trans 0) or a'\y (trans 1) on X in place (X already
+// permuted for a\y; permuted afterwards by the caller for a'\y)
+static void tile_sweeps(Ctx& c, const TileLU& TL, View X, bool trans) {
+  const int T = TL.T, nc = X.cols;
+  int smax = 1;
+  for (int k = 0; k < T; ++k) smax = std::max<int>(smax, (int)TL.size[k]);
+  // columns staged per pass of the inverse product: few, so that the update
+  // CTAs (which share the launch's shared-memory size) still pack the SMs
+  const int chunk = std::min(nc, 8);
+  const size_t smem = sizeof(double) * ((size_t)c.cap * nc + (size_t)smax * chunk);
+  if (smem > 200 * 1024) {
+    tile_solve(c, TL, X, trans, nullptr);
+    return;
+  }
+  if (smem_attr((const void*)lu_sweep_kernel, 200 * 1024) != cudaSuccess) throw LuError(HM_ERR_CUDA, "sweep smem");
+  SweepTab t{TL.d_Ap, TL.d_Bp, {TL.d_inv[0], TL.d_inv[1], TL.d_inv[2], TL.d_inv[3]}, TL.d_start, TL.d_size,
+             TL.kmat, T, c.cap};
+  for (int k = 0; k < T; ++k) {
+    lu_sweep_kernel<<<T - k, SW_THREADS, smem, c.st>>>(t, X.p, X.cs, nc, k, 1, trans ? 2 : 0, chunk);
+    LU_LAUNCH_CHECK();
+  }
+  for (int k = T - 1; k >= 0; --k) {
+    lu_sweep_kernel<<<k + 1, SW_THREADS, smem, c.st>>>(t, X.p, X.cs, nc, k, -1, trans ? 3 : 1, chunk);
+    LU_LAUNCH_CHECK();
+  }
+}
+
+static void tile_solve(Ctx& c, const TileLU& TL, View X, bool trans, double* Zext) {
   const int T = TL.T, cap = c.cap, nc = X.cols;
   auto yv = [&](int i) { return vsub(X, (int)TL.start[i], 0, (int)TL.size[i], nc); };
   Blk tmp;
@@ -1715,6 +1987,9 @@ int lu_factor(hm_handle* h) {
   return HM_OK;
 }
 
+// right-hand sides per sweep solve (the update's z values sit in shared memory)
+static constexpr int SWEEP_MAX_COLS = 64;
+
 // The launch sequence of a\y (trans = 0) or a'\y (trans = 1) from d_b into d_x.
 // W, when given, is the working copy of b for the transposed solve; it may be
 // d_b itself (the solve then overwrites b).
@@ -1728,7 +2003,9 @@ static void issue_solve(Ctx& c, LuState* S, const hm_handle* h, const double* d_
     // a\y (src/hlu.jl:553-562): permute!(w, P), unit-L forward, U backward
     lu_gather_rows_kernel<<<g, 256, 0, c.st>>>(X, B, S->P);
     LU_LAUNCH_CHECK();
-    if (S->tile) {
+    if (S->tile && S->tile->d_inv[0] && nc <= SWEEP_MAX_COLS) {
+      tile_sweeps(c, *S->tile, X, false);
+    } else if (S->tile) {
       tile_solve(c, *S->tile, X, false, Z);
     } else {
       solve_rec(c, *S->root, X, true);
@@ -1740,7 +2017,9 @@ static void issue_solve(Ctx& c, LuState* S, const hm_handle* h, const double* d_
     double* w = W ? W : (double*)dmalloc(c, tmp, sizeof(double) * (size_t)tot);
     View Wv{w, 1, h->n, (int)h->n, nc};
     if (w != d_b) axpby(c, Wv, B, 1.0, 0.0);
-    if (S->tile) {
+    if (S->tile && S->tile->d_inv[0] && nc <= SWEEP_MAX_COLS) {
+      tile_sweeps(c, *S->tile, Wv, true);
+    } else if (S->tile) {
       tile_solve(c, *S->tile, Wv, true, Z);
     } else {
       solve_t_rec(c, *S->root, Wv, true);
@@ -1830,6 +2109,7 @@ int lu_solve_device(hm_handle* h, const double* d_b, double* d_x, int64_t ncols,
   if (ncols <= 0) return HM_OK;
   Ctx c{st, S->cap, S->P, S->flags, h->prm.eps_trunc, h, S->blas_on(st)};
   try {
+    if (S->tile) ensure_sweep(c, *S->tile);
     if (ncols > SOLVE_GRAPH_MAX_COLS) {
       issue_solve(c, S, h, d_b, d_x, (int)ncols, trans, nullptr, nullptr);
     } else {
