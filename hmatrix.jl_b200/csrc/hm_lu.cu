@@ -1261,7 +1261,7 @@ struct TileLU {
   BP sweep_hold;
   const double** d_Ap = nullptr;
   const double** d_Bp = nullptr;
-  const double** d_inv[4] = {nullptr, nullptr, nullptr, nullptr};   // see sweep_apply_inverse
+  const double** d_inv[4] = {nullptr, nullptr, nullptr, nullptr};   // see sweep_finish
   int64_t* d_start = nullptr;
   int32_t* d_size = nullptr;
 };
@@ -1502,21 +1502,23 @@ constexpr int SW_THREADS = 256;
 struct SweepTab {
   const double* const* Ap;
   const double* const* Bp;
-  const double* const* Inv[4];   // per tile, the matrix of sweep_apply_inverse for each `which`
+  // per tile, the inverse factor sweep_finish applies for which = 0, 1, 2, 3
+  const double* const* Inv0;
+  const double* const* Inv1;
+  const double* const* Inv2;
+  const double* const* Inv3;
   const int64_t* start;
   const int32_t* size;
   const int32_t* kmat;
   int T, cap;
 };
 
-// y_i -= P (Q' y_s): non-transposed P = A_is, Q = B_is (tile (i,s) = A B');
-// transposed P = B_si, Q = A_si (tile (s,i)' = B A')
-__device__ void sweep_update(const SweepTab& t, double* Y, int64_t ldy, int nc, int i, int s, bool trans,
-                             double* zsh) {
+// The low-rank factors of tile (i, s) as used by a sweep step: y_i -= P (Q' y_s)
+// with, non-transposed, P = A_is and Q = B_is (tile (i,s) = A B') and,
+// transposed, P = B_si and Q = A_si (tile (s,i)' = B A'); r is the rank.
+__device__ __forceinline__ void sweep_factors(const SweepTab& t, int i, int s, bool trans, const double*& P,
+                                              const double*& Q, int& r) {  // inlined: no addresses taken
   const int Si = t.size[i], Ss = t.size[s];
-  const double* P;
-  const double* Q;
-  int r;
   if (!trans) {
     P = t.Ap[i] + (int64_t)s * t.cap * Si;
     Q = t.Bp[s] + (int64_t)i * t.cap * Ss;
@@ -1526,66 +1528,134 @@ __device__ void sweep_update(const SweepTab& t, double* Y, int64_t ldy, int nc, 
     Q = t.Ap[s] + (int64_t)i * t.cap * Ss;
     r = t.kmat[s * t.T + i];
   }
-  if (r <= 0) return;
-  const double* ys = Y + t.start[s];
-  double* yi = Y + t.start[i];
+}
+
+// zsh[q + c r] = (Q' y_s)[q, c], y_s = the finished tile s in F
+__device__ void sweep_z(const SweepTab& t, const double* F, int64_t ldy, int nc, int s, const double* Q, int r,
+                        double* zsh) {
+  const int Ss = t.size[s];
+  const double* ys = F + t.start[s];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int qc = warp; qc < r * nc; qc += SW_THREADS / 32) {
     const int q = qc % r, cc = qc / r;
     double acc = 0.0;
-    for (int row = lane; row < Ss; row += 32) acc = fma(Q[row + (int64_t)q * Ss], ys[row + cc * ldy], acc);
+#pragma unroll 8
+    for (int row = lane; row < Ss; row += 32)
+      acc = fma(__ldg(Q + row + (int64_t)q * Ss), __ldg(ys + row + cc * ldy), acc);
     acc = warp_sum(acc);
     if (lane == 0) zsh[q + cc * r] = acc;
   }
   __syncthreads();
+}
+
+// A_i -= P (Q' y_s): the finished tile s applied to the pending tile i
+__device__ void sweep_update(const SweepTab& t, double* A, const double* F, int64_t ldy, int nc, int i, int s,
+                             bool trans, double* zsh) {
+  const double* P;
+  const double* Q;
+  int r;
+  sweep_factors(t, i, s, trans, P, Q, r);
+  if (r <= 0) return;
+  sweep_z(t, F, ldy, nc, s, Q, r, zsh);
+  const int Si = t.size[i];
+  double* yi = A + t.start[i];
   for (int e = threadIdx.x; e < Si * nc; e += SW_THREADS) {
     const int row = e % Si, cc = e / Si;
     double acc = 0.0;
-    for (int q = 0; q < r; ++q) acc = fma(P[row + (int64_t)q * Si], zsh[q + cc * r], acc);
+#pragma unroll 8
+    for (int q = 0; q < r; ++q) acc = fma(__ldg(P + row + (int64_t)q * Si), zsh[q + cc * r], acc);
     yi[row + cc * ldy] -= acc;
   }
-  __syncthreads();
 }
 
-// y <- M y with M[q*S + r] = M(r, q) (the inverse stored so that consecutive
-// rows are consecutive in memory): which 0 L^-1 and 2 (U^-1)' are lower
-// triangular, 1 U^-1 and 3 (L^-1)' upper.  A thread per row, loads coalesced
-// over the rows; column chunks of y are staged in shared memory (the product
-// is not in place).
-__device__ void sweep_apply_inverse(const double* M, int S, int which, double* y, int64_t ldy, int nc,
-                                    double* ysh, int chunk) {
+// Finisher f of tile k: rows [f rpf, f rpf + rpf) (rpf <= 32) of
+// M (A_k - P (Q' y_s)) written to F, where M = Inv[which][k] (M[q*S + r] =
+// M(r, q); which 0 and 2 lower, 1 and 3 upper).  Lane = row, warp = segment
+// of the columns q the rows need: each thread loads its part of M into
+// registers first (those loads wait for nothing), then the update of tile k
+// from the finished tile s (if any) is recomputed for the rows q needed, and
+// the 8 segment sums of a row are added in shared memory.
+constexpr int SW_MREG = 32;
+__device__ void sweep_finish(const SweepTab& t, const double* A, double* F, int64_t ldy, int nc, int k, int s,
+                             bool has_src, bool trans, int which, int f, int rpf, int chunk, double* sh) {
+  constexpr int NW = SW_THREADS / 32;
+  const int S = t.size[k];
+  const int r0 = f * rpf, r1 = min(S, r0 + rpf), nr = r1 - r0;
+  if (nr <= 0) return;
   const bool lower = which == 0 || which == 2;
+  const int qa = lower ? 0 : r0, qb = lower ? r1 : S, span = qb - qa;
+  const int segl = (span + NW - 1) / NW;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool row_ok = lane < nr;
+  const int qs = qa + warp * segl;                    // this thread's columns [qs, qs + segl)
+  const double* const* inv = which == 0 ? t.Inv0 : which == 1 ? t.Inv1 : which == 2 ? t.Inv2 : t.Inv3;
+  const double* M = inv[k] + r0 + lane;               // M(r0 + lane, q) = M[q*S]
+  double mreg[SW_MREG];
+  const bool in_reg = segl <= SW_MREG;
+  if (in_reg) {
+#pragma unroll
+    for (int j = 0; j < SW_MREG; ++j)
+      mreg[j] = (row_ok && j < segl && qs + j < qb) ? __ldg(M + (int64_t)(qs + j) * S) : 0.0;
+  }
+  double* ysh = sh;                                   // span x chunk
+  double* part = ysh + (size_t)S * chunk;             // NW x 32 x chunk
+  double* zsh = part + (size_t)NW * 32 * chunk;       // cap x nc
+  const double* P = nullptr;
+  const double* Q = nullptr;
+  int r = 0;
+  if (has_src) sweep_factors(t, k, s, trans, P, Q, r);
+  if (r > 0) sweep_z(t, F, ldy, nc, s, Q, r, zsh);
+  const double* yk = A + t.start[k];
+  double* out = F + t.start[k];
   for (int c0 = 0; c0 < nc; c0 += chunk) {
     const int ncc = min(chunk, nc - c0);
-    for (int e = threadIdx.x; e < S * ncc; e += SW_THREADS) ysh[e] = y[e % S + (int64_t)(c0 + e / S) * ldy];
-    __syncthreads();
-    for (int e = threadIdx.x; e < S * ncc; e += SW_THREADS) {
-      const int r = e % S, cc = e / S;
-      const int q0 = lower ? 0 : r, q1 = lower ? r + 1 : S;
-      const double* ys = ysh + cc * S;
-      double acc = 0.0;
+    __syncthreads();                                  // ysh and part free
+    for (int e = threadIdx.x; e < span * ncc; e += SW_THREADS) {
+      const int q = e % span, cc = e / span;
+      double v = yk[qa + q + (int64_t)(c0 + cc) * ldy];
 #pragma unroll 8
-      for (int q = q0; q < q1; ++q) acc = fma(M[(int64_t)q * S + r], ys[q], acc);
-      y[r + (int64_t)(c0 + cc) * ldy] = acc;
+      for (int j = 0; j < r; ++j) v = fma(-__ldg(P + qa + q + (int64_t)j * S), zsh[j + (c0 + cc) * r], v);
+      ysh[q + cc * span] = v;
     }
     __syncthreads();
+    for (int cc = 0; cc < ncc; ++cc) {
+      const double* yv = ysh + cc * span - qa;        // yv[q], q in [qa, qb)
+      double acc = 0.0;
+      if (in_reg) {
+#pragma unroll
+        for (int j = 0; j < SW_MREG; ++j)
+          if (j < segl && qs + j < qb) acc = fma(mreg[j], yv[qs + j], acc);
+      } else if (row_ok) {
+        for (int q = qs; q < min(qs + segl, qb); ++q) acc = fma(__ldg(M + (int64_t)q * S), yv[q], acc);
+      }
+      part[(cc * NW + warp) * 32 + lane] = acc;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nr * ncc; e += SW_THREADS) {
+      const int ii = e % nr, cc = e / nr;
+      double acc = 0.0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) acc += part[(cc * NW + w) * 32 + ii];
+      out[r0 + ii + (int64_t)(c0 + cc) * ldy] = acc;
+    }
   }
 }
 
-// which: 0 L (forward), 1 U (backward), 2 U' (forward), 3 L' (backward)
-__global__ void __launch_bounds__(SW_THREADS) lu_sweep_kernel(SweepTab t, double* Y, int64_t ldy, int nc, int k,
-                                                              int dir, int which, int chunk) {
+// Step k of a sweep (dir +1 forward, -1 backward; which: 0 L, 1 U, 2 U', 3 L').
+// A holds the pending right-hand sides, F receives the finished tiles; the
+// finished tile s = k - dir is applied to tile k by the nf finisher CTAs and
+// to every later tile of the sweep by one CTA each.
+__global__ void __launch_bounds__(SW_THREADS, 2) lu_sweep_kernel(SweepTab t, double* A, double* F, int64_t ldy,
+                                                              int nc, int k, int dir, int which, int nf, int rpf,
+                                                              int chunk) {
   extern __shared__ double sh[];
-  double* zsh = sh;                                  // cap x nc
-  double* ysh = sh + (size_t)t.cap * nc;             // S x chunk
   const bool trans = which >= 2;
   const int s = k - dir;
   const bool has_src = s >= 0 && s < t.T;
-  if (blockIdx.x == 0) {
-    if (has_src) sweep_update(t, Y, ldy, nc, k, s, trans, zsh);
-    sweep_apply_inverse(t.Inv[which][k], t.size[k], which, Y + t.start[k], ldy, nc, ysh, chunk);
+  if ((int)blockIdx.x < nf) {
+    sweep_finish(t, A, F, ldy, nc, k, s, has_src, trans, which, blockIdx.x, rpf, chunk, sh);
   } else if (has_src) {
-    sweep_update(t, Y, ldy, nc, k + dir * (int)blockIdx.x, s, trans, zsh);
+    sweep_update(t, A, F, ldy, nc, k + dir * ((int)blockIdx.x - nf + 1), s, trans, sh);
   }
 }
 
@@ -1726,28 +1796,36 @@ static void ensure_sweep(Ctx& c, TileLU& TL) {
 static void tile_solve(Ctx& c, const TileLU& TL, View X, bool trans, double* Zext);
 
 // the two sweeps of a\y (trans 0) or a'\y (trans 1) on X in place (X already
-// permuted for a\y; permuted afterwards by the caller for a'\y)
+// permuted for a\y; permuted afterwards by the caller for a'\y).  The
+// forward sweep finishes tiles into a second array W, the backward sweep
+// takes W as its right-hand sides and finishes into X.
 static void tile_sweeps(Ctx& c, const TileLU& TL, View X, bool trans) {
   const int T = TL.T, nc = X.cols;
   int smax = 1;
   for (int k = 0; k < T; ++k) smax = std::max<int>(smax, (int)TL.size[k]);
-  // columns staged per pass of the inverse product: few, so that the update
-  // CTAs (which share the launch's shared-memory size) still pack the SMs
-  const int chunk = std::min(nc, 8);
-  const size_t smem = sizeof(double) * ((size_t)c.cap * nc + (size_t)smax * chunk);
-  if (smem > 200 * 1024) {
+  const int rpf = 32;                                              // rows of a finisher (a lane each)
+  const int chunk = std::min(nc, 8);                               // columns staged per pass
+  const size_t smem = sizeof(double) * ((size_t)smax * chunk + (size_t)SW_THREADS * chunk + (size_t)c.cap * nc);
+  if (smem > 200 * 1024 || X.rs != 1) {
     tile_solve(c, TL, X, trans, nullptr);
     return;
   }
   if (smem_attr((const void*)lu_sweep_kernel, 200 * 1024) != cudaSuccess) throw LuError(HM_ERR_CUDA, "sweep smem");
-  SweepTab t{TL.d_Ap, TL.d_Bp, {TL.d_inv[0], TL.d_inv[1], TL.d_inv[2], TL.d_inv[3]}, TL.d_start, TL.d_size,
+  Blk tmp;
+  tmp.st = c.st;
+  double* W = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)X.cs * nc);
+  SweepTab t{TL.d_Ap, TL.d_Bp, TL.d_inv[0], TL.d_inv[1], TL.d_inv[2], TL.d_inv[3], TL.d_start, TL.d_size,
              TL.kmat, T, c.cap};
   for (int k = 0; k < T; ++k) {
-    lu_sweep_kernel<<<T - k, SW_THREADS, smem, c.st>>>(t, X.p, X.cs, nc, k, 1, trans ? 2 : 0, chunk);
+    const int nf = ((int)TL.size[k] + rpf - 1) / rpf;
+    const int nu = k > 0 ? T - 1 - k : 0;
+    lu_sweep_kernel<<<nf + nu, SW_THREADS, smem, c.st>>>(t, X.p, W, X.cs, nc, k, 1, trans ? 2 : 0, nf, rpf, chunk);
     LU_LAUNCH_CHECK();
   }
   for (int k = T - 1; k >= 0; --k) {
-    lu_sweep_kernel<<<k + 1, SW_THREADS, smem, c.st>>>(t, X.p, X.cs, nc, k, -1, trans ? 3 : 1, chunk);
+    const int nf = ((int)TL.size[k] + rpf - 1) / rpf;
+    const int nu = k < T - 1 ? k : 0;
+    lu_sweep_kernel<<<nf + nu, SW_THREADS, smem, c.st>>>(t, W, X.p, X.cs, nc, k, -1, trans ? 3 : 1, nf, rpf, chunk);
     LU_LAUNCH_CHECK();
   }
 }
