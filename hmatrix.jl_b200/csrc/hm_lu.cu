@@ -1201,6 +1201,60 @@ static void recompress_batch(Ctx& c, const std::vector<RcReq>& reqs, int rmax) {
   }
 }
 
+// The off-diagonal part of step k's trailing update, generated on the device:
+// for every pair i != j of trailing tiles, A_ij B_ij' - Q_ij B_kj' is gathered
+// into one [A | -Q] [B | B_kj] pair and recompressed (Q_ij = A_ik W_kj, the
+// panel product of step k).  Job q of the batch is pair (ii, jj) of the
+// trailing tiles with the diagonal skipped; its scratch is a fixed stride.
+struct TileJobArgs {
+  const double* const* Ap;
+  const double* const* Bp;
+  const int64_t* start;
+  const int32_t* size;
+  int32_t* kmat;
+  int T, cap, k, rmax;
+  int64_t R;                 // (T-k-1) cap: columns of a Q panel row
+  const double* qbase;       // Q_i = qbase + (start[i] - start[k+1]) R
+  double* scratch;
+  int64_t stride;            // scratch doubles per job
+  int32_t* rr;               // gathered rank per job
+  int* flags;
+  CoreJob* cj;
+  int64_t q0;                // first job of this batch
+};
+__global__ void __launch_bounds__(256) lu_tile_gather_kernel(TileJobArgs a) {
+  const int64_t q = blockIdx.x;
+  const int64_t gq = a.q0 + q;
+  const int Tr = a.T - a.k - 1;
+  const int ii = (int)(gq / (Tr - 1));
+  int jj = (int)(gq % (Tr - 1));
+  if (jj >= ii) ++jj;
+  const int i = a.k + 1 + ii, j = a.k + 1 + jj;
+  const int mi = a.size[i], nj = a.size[j];
+  const double* Qi = a.qbase + (a.start[i] - a.start[a.k + 1]) * a.R;
+  double* Aij = const_cast<double*>(a.Ap[i]) + (int64_t)j * a.cap * mi;
+  double* Bij = const_cast<double*>(a.Bp[j]) + (int64_t)i * a.cap * nj;
+  GatherArgs g{};
+  g.pc[0] = Piece{Aij, mi, Bij, nj, a.kmat + i * a.T + j, mi, nj, 0, 0, 1.0};
+  g.pc[1] = Piece{Qi + (int64_t)(j - a.k - 1) * a.cap * mi, mi, a.Bp[j] + (int64_t)a.k * a.cap * nj, nj,
+                  a.kmat + a.k * a.T + j, mi, nj, 0, 0, -1.0};
+  g.np = 2;
+  g.SA = a.scratch + q * a.stride;
+  g.SB = g.SA + (int64_t)mi * a.rmax;
+  g.M = mi; g.N = nj; g.rmax = a.rmax;
+  g.r_out = a.rr + q;
+  g.flags = a.flags;
+  if (threadIdx.x == 0) {
+    CoreJob J{};
+    J.A = g.SA; J.B = g.SB; J.outA = Aij; J.outB = Bij;
+    J.m = mi; J.n = nj; J.lda = max(mi, 1); J.ldb = max(nj, 1);
+    J.ldoa = mi; J.ldob = nj; J.kcap = a.cap;
+    J.zero_test = 1; J.rank = a.kmat + i * a.T + j; J.r_dev = g.r_out; J.zero_fill = 1;
+    a.cj[q] = J;
+  }
+  gather_pieces(g);
+}
+
 // H_tile += s * A B' for an H-structured diagonal tile, as jobs: dense leaves
 // get a product, low-rank leaves a recompression (hmat_add! of H += Rk splits
 // the low-rank term over the children, src/harithm.jl:129-142)
@@ -1345,6 +1399,40 @@ static bool tile_structure(const hm_handle* h, std::vector<int32_t>& gcl, std::v
   return false;
 }
 
+static void recompress_tile_pairs(Ctx& c, const TileLU& TL, int k, int64_t R, const double* qbase, int rmax) {
+  const int T = TL.T, Tr = T - k - 1;
+  const int64_t njobs = (int64_t)Tr * (Tr - 1);
+  if (njobs <= 0) return;
+  rmax = std::min(std::max(rmax, 1), RCORE_MAX);
+  int64_t smax = 1;
+  for (int i = k + 1; i < T; ++i) smax = std::max<int64_t>(smax, TL.size[i]);
+  const int64_t stride = 2 * smax * rmax;
+  const int64_t per = std::max<int64_t>(1, std::min<int64_t>(((int64_t)1 << 28) / stride, 65535));
+  Blk tmp;
+  tmp.st = c.st;
+  const int64_t nb0 = std::min(per, njobs);
+  double* scratch = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)(nb0 * stride));
+  int32_t* rr = (int32_t*)dmalloc(c, tmp, sizeof(int32_t) * (size_t)nb0);
+  CoreJob* cj = (CoreJob*)dmalloc(c, tmp, sizeof(CoreJob) * (size_t)nb0);
+  int32_t* dmax = (int32_t*)dmalloc(c, tmp, sizeof(int32_t));
+  for (int64_t q0 = 0; q0 < njobs; q0 += per) {
+    const int64_t nb = std::min(per, njobs - q0);
+    TileJobArgs a{TL.d_Ap, TL.d_Bp, TL.d_start, TL.d_size, TL.kmat, T, c.cap, k, rmax, R, qbase, scratch, stride,
+                  rr, c.flags, cj, q0};
+    lu_tile_gather_kernel<<<(unsigned)nb, 256, 0, c.st>>>(a);
+    LU_LAUNCH_CHECK();
+    lu_max_int_kernel<<<1, 256, 0, c.st>>>(rr, (int)nb, dmax);
+    LU_LAUNCH_CHECK();
+    int32_t hmax = 0;
+    if (cudaMemcpyAsync(&hmax, dmax, sizeof(int32_t), cudaMemcpyDeviceToHost, c.st) != cudaSuccess ||
+        cudaStreamSynchronize(c.st) != cudaSuccess)
+      throw LuError(HM_ERR_CUDA, "core size read-back");
+    const int rlaunch = std::min(rmax, std::max(8, (hmax + 7) / 8 * 8));
+    int st = launch_core_recompress(cj, (int)nb, rlaunch, c.eps_trunc, c.flags, c.st);
+    if (st != HM_OK) throw LuError(st, "batched recompression launch");
+  }
+}
+
 static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vector<int32_t>& gcl,
                         const std::vector<int32_t>& dnode) {
   const int T = (int)gcl.size(), cap = c.cap;
@@ -1364,6 +1452,21 @@ static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vecto
     TL.Bp[i] = (double*)dmalloc(c, *TL.hold, sizeof(double) * TL.size[i] * T * cap);
   }
   TL.kmat = (int32_t*)dmalloc(c, *TL.hold, sizeof(int32_t) * T * T);
+  {
+    std::vector<const double*> ap(TL.Ap.begin(), TL.Ap.end()), bp(TL.Bp.begin(), TL.Bp.end());
+    std::vector<int32_t> sz(TL.size.begin(), TL.size.end());
+    TL.d_Ap = (const double**)dmalloc(c, *TL.hold, sizeof(void*) * T);
+    TL.d_Bp = (const double**)dmalloc(c, *TL.hold, sizeof(void*) * T);
+    TL.d_start = (int64_t*)dmalloc(c, *TL.hold, sizeof(int64_t) * T);
+    TL.d_size = (int32_t*)dmalloc(c, *TL.hold, sizeof(int32_t) * T);
+    if (cudaMemcpyAsync(TL.d_Ap, ap.data(), sizeof(void*) * T, cudaMemcpyHostToDevice, c.st) != cudaSuccess ||
+        cudaMemcpyAsync(TL.d_Bp, bp.data(), sizeof(void*) * T, cudaMemcpyHostToDevice, c.st) != cudaSuccess ||
+        cudaMemcpyAsync(TL.d_start, TL.start.data(), sizeof(int64_t) * T, cudaMemcpyHostToDevice, c.st) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(TL.d_size, sz.data(), sizeof(int32_t) * T, cudaMemcpyHostToDevice, c.st) != cudaSuccess ||
+        cudaStreamSynchronize(c.st) != cudaSuccess)
+      throw LuError(HM_ERR_CUDA, "tile tables");
+  }
   if (cudaMemsetAsync(TL.kmat, 0, sizeof(int32_t) * T * T, c.st) != cudaSuccess) throw LuError(HM_ERR_CUDA, "memset");
   // load the off-diagonal tiles into the panels and the diagonal tiles as trees
   const int eb = elem_bytes(h->storage);
@@ -1462,29 +1565,14 @@ static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vecto
     }
     std::vector<RcReq> rj;
     std::vector<GemmJob> gd;
-    for (int i = k + 1; i < T; ++i) {
+    for (int i = k + 1; i < T; ++i) {                      // diagonal tiles: H-structured targets
       const int mi = (int)TL.size[i];
-      for (int j = k + 1; j < T; ++j) {
-        const int nj = (int)TL.size[j];
-        const double* Qij = Q[i] + (int64_t)(j - k - 1) * cap * mi;
-        const int32_t* kkj = TL.kmat + k * T + j;
-        if (i == j) {
-          tile_add_lowrank(*TL.diag[i], 0, 0, Qij, mi, TL.Bj(k, i, cap), nj, kkj, cap, -1.0, gd, rj);
-        } else {
-          RcReq Rq{};
-          Rq.pc[0] = Piece{TL.Ai(i, j, cap), mi, TL.Bj(i, j, cap), nj, TL.kmat + i * T + j, mi, nj, 0, 0, 1.0};
-          Rq.pc[1] = Piece{Qij, mi, TL.Bj(k, j, cap), nj, kkj, mi, nj, 0, 0, -1.0};
-          Rq.np = 2;
-          Rq.outA = TL.Ai(i, j, cap); Rq.ldoa = mi;
-          Rq.outB = TL.Bj(i, j, cap); Rq.ldob = nj;
-          Rq.k = TL.kmat + i * T + j;
-          Rq.m = mi; Rq.n = nj; Rq.kcap = cap;
-          rj.push_back(Rq);
-        }
-      }
+      const double* Qii = Q[i] + (int64_t)(i - k - 1) * cap * mi;
+      tile_add_lowrank(*TL.diag[i], 0, 0, Qii, mi, TL.Bj(k, i, cap), mi, TL.kmat + k * T + i, cap, -1.0, gd, rj);
     }
     gemm_batch(c, gd);
-    recompress_batch(c, rj, 2 * cap);
+    recompress_batch(c, rj, 2 * cap);                      // low-rank leaves of the diagonal tiles
+    recompress_tile_pairs(c, TL, k, R, Q[k + 1], 2 * cap);  // the off-diagonal tiles
   }
 }
 
@@ -1776,11 +1864,13 @@ static void ensure_sweep(Ctx& c, TileLU& TL) {
   double** dD = (double**)dmalloc(c, tmp, sizeof(void*) * T);
   if (cudaMemcpyAsync(dD, D.data(), sizeof(void*) * T, cudaMemcpyHostToDevice, c.st) != cudaSuccess)
     throw LuError(HM_ERR_CUDA, "sweep tables");
-  TL.d_Ap = (const double**)up(Ap.data(), sizeof(void*) * T);
-  TL.d_Bp = (const double**)up(Bp.data(), sizeof(void*) * T);
+  if (!TL.d_Ap) {                            // a copied factorisation has no tables yet
+    TL.d_Ap = (const double**)up(Ap.data(), sizeof(void*) * T);
+    TL.d_Bp = (const double**)up(Bp.data(), sizeof(void*) * T);
+    TL.d_start = (int64_t*)up(TL.start.data(), sizeof(int64_t) * T);
+    TL.d_size = (int32_t*)up(sz.data(), sizeof(int32_t) * T);
+  }
   for (int w = 0; w < 4; ++w) TL.d_inv[w] = (const double**)up(inv[w].data(), sizeof(void*) * T);
-  TL.d_start = (int64_t*)up(TL.start.data(), sizeof(int64_t) * T);
-  TL.d_size = (int32_t*)up(sz.data(), sizeof(int32_t) * T);
   const dim3 g((smax + 127) / 128, T);
   // L^-1: row-major (which 3) and column-major (which 0); U^-1: row-major (2), column-major (1)
   lu_tri_inverse_kernel<<<g, 128, 0, c.st>>>(dD, (double* const*)TL.d_inv[3], (double* const*)TL.d_inv[0],
