@@ -1,6 +1,7 @@
 // Batched low-rank kernels for sm_100a: aca2, fully pivoted ACA and the
 // QR + one-sided-Jacobi-SVD recompression core.
 #include "hm_lowrank.cuh"
+#include "hm_core.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -272,213 +273,6 @@ int launch_aca_fp_one(const AcaFpJob& J, cudaStream_t st) {
   aca_fp_one_kernel<<<1, 512, 0, st>>>(J);
   HM_CUDA_TRY(cudaGetLastError());
   return HM_OK;
-}
-
-// ===========================================================================
-// Recompression core (K3): CGS2 QR of A and B in place, W = R_A R_B^T, one
-// sided Jacobi SVD of W, truncation k = #{s_i/s_1 > eps_trunc}, and
-// A' = Q_A U_k, B' = Q_B V_k S_k.  One CTA per job; smem 3*rmax^2 doubles.
-// ===========================================================================
-__device__ void cgs2_qr(double* X, int len, int ld, int r, double* Rm /* r x r, col-major */,
-                        double* proj /* r */, double* red) {
-  for (int e = threadIdx.x; e < r * r; e += blockDim.x) Rm[e] = 0.0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int j = 0; j < r; ++j) {
-    double* xj = X + (int64_t)j * ld;
-    for (int pass = 0; pass < 2; ++pass) {
-      for (int i = w; i < j; i += nw) {
-        const double* qi = X + (int64_t)i * ld;
-        double s = 0.0;
-        for (int t = lane; t < len; t += 32) s = fma(qi[t], xj[t], s);
-        s = warp_sum(s);
-        if (lane == 0) proj[i] = s;
-      }
-      __syncthreads();
-      for (int t = threadIdx.x; t < len; t += blockDim.x) {
-        double s = 0.0;
-        for (int i = 0; i < j; ++i) s = fma(X[t + (int64_t)i * ld], proj[i], s);
-        xj[t] -= s;
-      }
-      if (threadIdx.x < j) Rm[threadIdx.x + j * r] += proj[threadIdx.x];
-      __syncthreads();
-    }
-    double ss = 0.0;
-    for (int t = threadIdx.x; t < len; t += blockDim.x) ss = fma(xj[t], xj[t], ss);
-    const double nrm = sqrt(block_sum(ss, red));
-    const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
-    for (int t = threadIdx.x; t < len; t += blockDim.x) xj[t] *= inv;
-    if (threadIdx.x == 0) Rm[j + j * r] = nrm;
-    __syncthreads();
-  }
-}
-
-__device__ void zero_cols(double* X, int len, int64_t ld, int c0, int c1) {
-  for (int64_t e = threadIdx.x; e < (int64_t)len * (c1 - c0); e += blockDim.x)
-    X[(e % len) + (int64_t)(c0 + e / len) * ld] = 0.0;
-}
-
-__device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, int* __restrict__ flags) {
-  extern __shared__ double sm[];
-  __shared__ double red[32];
-  __shared__ double proj[RCORE_MAX];
-  __shared__ double sig[RCORE_MAX];
-  __shared__ int ord[RCORE_MAX];
-  __shared__ int s_rot;
-  __shared__ int s_k;
-  int r = J.r_dev ? *J.r_dev : J.r;
-  double* b0 = sm;                       // R_A, later V (Jacobi right vectors)
-  double* b1 = sm + rmax * rmax;         // R_B, later U-coefficients
-  double* b2 = sm + 2 * rmax * rmax;     // W, later V-coefficients
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int pre = J.pre_status ? *J.pre_status : 0;
-  if (pre != 0 || r > rmax) {
-    // pre == 3: compress() of an absolutely tiny block -> rank-1 zeros;
-    // otherwise the input could not be reduced (not converged / too large)
-    if (threadIdx.x == 0 && pre != 3) atomicOr(flags, pre == 2 ? 2 : 1);
-    zero_cols(J.outA, J.m, J.ldoa, 0, J.kcap);
-    zero_cols(J.outB, J.n, J.ldob, 0, J.kcap);
-    if (threadIdx.x == 0) *J.rank = (pre == 3) ? 1 : 0;
-    return;
-  }
-  if (r == 0) {
-    if (J.zero_fill) {
-      zero_cols(J.outA, J.m, J.ldoa, 0, J.kcap);
-      zero_cols(J.outB, J.n, J.ldob, 0, J.kcap);
-    }
-    if (threadIdx.x == 0) *J.rank = 0;
-    return;
-  }
-  cgs2_qr(J.A, J.m, J.lda, r, b0, proj, red);
-  cgs2_qr(J.B, J.n, J.ldb, r, b1, proj, red);
-  // W = R_A R_B^T  (r x r, column-major, ld r)
-  double sabs = 0.0;
-  for (int e = threadIdx.x; e < r * r; e += blockDim.x) {
-    const int i = e % r, j = e / r;
-    double s = 0.0;
-    for (int q = max(i, j); q < r; ++q) s = fma(b0[i + q * r], b1[j + q * r], s);
-    b2[e] = s;
-    sabs += fabs(s);
-  }
-  sabs = block_sum(sabs, red);
-  bool nonfinite = !isfinite(sabs);
-  if (J.zero_test && sabs < 1e-5) {
-    // compress(): an (absolutely) tiny core becomes rank-1 zeros (src/hlu.jl:163-167)
-    const int kz = J.zero_fill ? J.kcap : 1;
-    zero_cols(J.outA, J.m, J.ldoa, 0, kz);
-    zero_cols(J.outB, J.n, J.ldob, 0, kz);
-    if (threadIdx.x == 0) *J.rank = 1;
-    return;
-  }
-  // V = I
-  for (int e = threadIdx.x; e < r * r; e += blockDim.x) b0[e] = (e % r == e / r) ? 1.0 : 0.0;
-  __syncthreads();
-  // one-sided Jacobi on the columns of W, round-robin pairing
-  const int rr = (r + 1) & ~1;
-  for (int sweep = 0; sweep < 60; ++sweep) {
-    if (threadIdx.x == 0) s_rot = 0;
-    __syncthreads();
-    for (int round = 0; round < rr - 1; ++round) {
-      for (int pidx = w; pidx < rr / 2; pidx += nw) {
-        // tournament pairing: position 0 fixed, others rotate
-        auto posv = [&](int q) { return q == 0 ? 0 : 1 + (q - 1 + round) % (rr - 1); };
-        int p = posv(pidx), q = posv(rr - 1 - pidx);
-        if (p > q) { int t = p; p = q; q = t; }
-        if (q >= r) continue;
-        double* wp = b2 + p * r;
-        double* wq = b2 + q * r;
-        double al = 0.0, be = 0.0, ga = 0.0;
-        for (int t = lane; t < r; t += 32) {
-          al = fma(wp[t], wp[t], al);
-          be = fma(wq[t], wq[t], be);
-          ga = fma(wp[t], wq[t], ga);
-        }
-        al = warp_sum(al); be = warp_sum(be); ga = warp_sum(ga);
-        if (ga != 0.0 && fabs(ga) > 1e-15 * sqrt(al * be)) {
-          const double zeta = (be - al) / (2.0 * ga);
-          const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-          const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
-          double* vp = b0 + p * r;
-          double* vq = b0 + q * r;
-          for (int t2 = lane; t2 < r; t2 += 32) {
-            const double x = wp[t2], y = wq[t2];
-            wp[t2] = c * x - s * y;
-            wq[t2] = s * x + c * y;
-            const double u = vp[t2], v = vq[t2];
-            vp[t2] = c * u - s * v;
-            vq[t2] = s * u + c * v;
-          }
-          if (lane == 0) atomicAdd(&s_rot, 1);
-        }
-      }
-      __syncthreads();
-    }
-    if (s_rot == 0) break;
-    __syncthreads();
-  }
-  // singular values = column norms of W; sort descending
-  for (int j = w; j < r; j += nw) {
-    double s = 0.0;
-    for (int t = lane; t < r; t += 32) s = fma(b2[t + j * r], b2[t + j * r], s);
-    s = warp_sum(s);
-    if (lane == 0) sig[j] = sqrt(s);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int j = 0; j < r; ++j) ord[j] = j;
-    for (int a = 0; a < r; ++a) {             // stable selection sort, descending
-      int b = a;
-      for (int c = a + 1; c < r; ++c)
-        if (sig[ord[c]] > sig[ord[b]]) b = c;
-      int t = ord[b];
-      for (int c = b; c > a; --c) ord[c] = ord[c - 1];
-      ord[a] = t;
-    }
-    const double s1 = sig[ord[0]];
-    int k = 0;
-    for (int j = 0; j < r; ++j)
-      if (sig[ord[j]] / s1 > eps_trunc) k = j + 1;   // findlast(S/S[1] .> εTrunc)
-    if (!(s1 > 0.0)) k = 0;
-    s_k = k;
-  }
-  __syncthreads();
-  int k = s_k;
-  if (k > J.kcap) {
-    if (threadIdx.x == 0) atomicOr(flags, 1);
-    k = J.kcap;
-  }
-  if (nonfinite && threadIdx.x == 0) atomicOr(flags, 2);
-  // coefficients: CU[j][c] = W[j, ord c] / s ; CV[j][c] = V[j, ord c] * s
-  for (int e = threadIdx.x; e < r * k; e += blockDim.x) {
-    const int j = e % r, c = e / r;
-    const int o = ord[c];
-    const double s = sig[o];
-    b1[e] = s > 0.0 ? b2[j + o * r] / s : 0.0;
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < r * k; e += blockDim.x) {
-    const int j = e % r, c = e / r;
-    const int o = ord[c];
-    b2[e] = b0[j + o * r] * sig[o];
-  }
-  __syncthreads();
-  for (int64_t e = threadIdx.x; e < (int64_t)J.m * k; e += blockDim.x) {
-    const int i = (int)(e % J.m), c = (int)(e / J.m);
-    double s = 0.0;
-    for (int j = 0; j < r; ++j) s = fma(J.A[i + (int64_t)j * J.lda], b1[j + c * r], s);
-    J.outA[i + (int64_t)c * J.ldoa] = s;
-  }
-  for (int64_t e = threadIdx.x; e < (int64_t)J.n * k; e += blockDim.x) {
-    const int i = (int)(e % J.n), c = (int)(e / J.n);
-    double s = 0.0;
-    for (int j = 0; j < r; ++j) s = fma(J.B[i + (int64_t)j * J.ldb], b2[j + c * r], s);
-    J.outB[i + (int64_t)c * J.ldob] = s;
-  }
-  if (J.zero_fill && k < J.kcap) {
-    zero_cols(J.outA, J.m, J.ldoa, k, J.kcap);
-    zero_cols(J.outB, J.n, J.ldob, k, J.kcap);
-  }
-  if (threadIdx.x == 0) *J.rank = k;
 }
 
 __global__ void __launch_bounds__(256) core_recompress_kernel(const CoreJob* __restrict__ jobs, int rmax,

@@ -13,6 +13,7 @@
 // permutation is one device array P with H[P,:] = L U.
 #include "hm_internal.h"
 #include "hm_lowrank.cuh"
+#include "hm_core.cuh"
 
 #include <cublas_v2.h>
 
@@ -1399,6 +1400,75 @@ static bool tile_structure(const hm_handle* h, std::vector<int32_t>& gcl, std::v
   return false;
 }
 
+// The same update with the gather fused into the recompression: the CTA
+// loads [A_ij | -Q_ij] and [B_ij | B_kj] into shared memory (rl columns at
+// most, smax rows) and runs the QR + SVD core there.
+__global__ void __launch_bounds__(128) lu_tile_core_kernel(TileJobArgs a, int rl, int smax, double eps_trunc) {
+  extern __shared__ double sm[];
+  const int64_t gq = a.q0 + blockIdx.x;
+  const int Tr = a.T - a.k - 1;
+  const int ii = (int)(gq / (Tr - 1));
+  int jj = (int)(gq % (Tr - 1));
+  if (jj >= ii) ++jj;
+  const int i = a.k + 1 + ii, j = a.k + 1 + jj;
+  const int mi = a.size[i], nj = a.size[j];
+  const double* Qij = a.qbase + (a.start[i] - a.start[a.k + 1]) * a.R + (int64_t)(j - a.k - 1) * a.cap * mi;
+  double* Aij = const_cast<double*>(a.Ap[i]) + (int64_t)j * a.cap * mi;
+  double* Bij = const_cast<double*>(a.Bp[j]) + (int64_t)i * a.cap * nj;
+  const double* Bkj = a.Bp[j] + (int64_t)a.k * a.cap * nj;
+  int32_t* kij = a.kmat + i * a.T + j;
+  const int k1 = *kij, k2 = a.kmat[a.k * a.T + j];
+  int r = k1 + k2;
+  if (r > rl) {                      // cannot happen: rl bounds every pair of the step
+    if (threadIdx.x == 0) atomicOr(a.flags, 1);
+    r = rl;
+  }
+  double* XA = sm + 3 * rl * rl;
+  double* XB = XA + (int64_t)smax * rl;
+  for (int e = threadIdx.x; e < mi * r; e += blockDim.x) {
+    const int t = e % mi, q = e / mi;
+    XA[e] = q < k1 ? Aij[t + (int64_t)q * mi] : -Qij[t + (int64_t)(q - k1) * mi];
+  }
+  for (int e = threadIdx.x; e < nj * r; e += blockDim.x) {
+    const int t = e % nj, q = e / nj;
+    XB[e] = q < k1 ? Bij[t + (int64_t)q * nj] : Bkj[t + (int64_t)(q - k1) * nj];
+  }
+  __syncthreads();
+  CoreJob J{};
+  J.A = XA; J.B = XB; J.outA = Aij; J.outB = Bij;
+  J.m = mi; J.n = nj; J.r = r; J.lda = max(mi, 1); J.ldb = max(nj, 1);
+  J.ldoa = mi; J.ldob = nj; J.kcap = a.cap;
+  J.zero_test = 1; J.rank = kij; J.zero_fill = 1;
+  core_body(J, rl, eps_trunc, a.flags);
+}
+
+// an upper bound of rank(A_ij) + rank(B_kj) over the trailing pairs of step k
+__global__ void lu_tile_rank_bound_kernel(const int32_t* __restrict__ kmat, int T, int k, int32_t* out) {
+  __shared__ int32_t red[256];
+  int32_t m1 = 0, m2 = 0;
+  const int Tr = T - k - 1;
+  for (int e = threadIdx.x; e < Tr * Tr; e += blockDim.x) {
+    const int i = k + 1 + e / Tr, j = k + 1 + e % Tr;
+    if (i != j) m1 = max(m1, kmat[i * T + j]);
+  }
+  for (int j = k + 1 + threadIdx.x; j < T; j += blockDim.x) m2 = max(m2, kmat[k * T + j]);
+  red[threadIdx.x] = m1;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] = max(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  const int32_t a1 = red[0];
+  __syncthreads();
+  red[threadIdx.x] = m2;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] = max(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = a1 + red[0];
+}
+
 static void recompress_tile_pairs(Ctx& c, const TileLU& TL, int k, int64_t R, const double* qbase, int rmax) {
   const int T = TL.T, Tr = T - k - 1;
   const int64_t njobs = (int64_t)Tr * (Tr - 1);
@@ -1406,10 +1476,34 @@ static void recompress_tile_pairs(Ctx& c, const TileLU& TL, int k, int64_t R, co
   rmax = std::min(std::max(rmax, 1), RCORE_MAX);
   int64_t smax = 1;
   for (int i = k + 1; i < T; ++i) smax = std::max<int64_t>(smax, TL.size[i]);
-  const int64_t stride = 2 * smax * rmax;
-  const int64_t per = std::max<int64_t>(1, std::min<int64_t>(((int64_t)1 << 28) / stride, 65535));
   Blk tmp;
   tmp.st = c.st;
+  {
+    // fused path: one rank bound per step, the pairs' factors staged in shared memory
+    int32_t* dmax = (int32_t*)dmalloc(c, tmp, sizeof(int32_t));
+    lu_tile_rank_bound_kernel<<<1, 256, 0, c.st>>>(TL.kmat, T, k, dmax);
+    LU_LAUNCH_CHECK();
+    int32_t hb = 0;
+    if (cudaMemcpyAsync(&hb, dmax, sizeof(int32_t), cudaMemcpyDeviceToHost, c.st) != cudaSuccess ||
+        cudaStreamSynchronize(c.st) != cudaSuccess)
+      throw LuError(HM_ERR_CUDA, "rank bound read-back");
+    const int rl = std::min(rmax, std::max(8, (hb + 7) / 8 * 8));
+    const size_t smem = sizeof(double) * ((size_t)3 * rl * rl + (size_t)2 * smax * rl);
+    if (smem <= 200 * 1024) {
+      if (smem_attr((const void*)lu_tile_core_kernel, 200 * 1024) != cudaSuccess)
+        throw LuError(HM_ERR_CUDA, "tile core smem");
+      for (int64_t q0 = 0; q0 < njobs; q0 += INT32_MAX) {
+        const int64_t nb = std::min<int64_t>(INT32_MAX, njobs - q0);
+        TileJobArgs a{TL.d_Ap, TL.d_Bp, TL.d_start, TL.d_size, TL.kmat, T, c.cap, k, rmax, R, qbase, nullptr, 0,
+                      nullptr, c.flags, nullptr, q0};
+        lu_tile_core_kernel<<<(unsigned)nb, 128, smem, c.st>>>(a, rl, (int)smax, c.eps_trunc);
+        LU_LAUNCH_CHECK();
+      }
+      return;
+    }
+  }
+  const int64_t stride = 2 * smax * rmax;
+  const int64_t per = std::max<int64_t>(1, std::min<int64_t>(((int64_t)1 << 28) / stride, 65535));
   const int64_t nb0 = std::min(per, njobs);
   double* scratch = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)(nb0 * stride));
   int32_t* rr = (int32_t*)dmalloc(c, tmp, sizeof(int32_t) * (size_t)nb0);
