@@ -49,10 +49,11 @@ struct DeviceGuard {
 int check_params(const hm_params* p) {
   if (!p) return fail(HM_ERR_ARG, "params is NULL");
   if (p->dim < 1 || p->dim > 3) return fail(HM_ERR_ARG, "dim must be 1, 2 or 3");
-  if (p->kernel != HM_KERNEL_CAUCHY && p->kernel != HM_KERNEL_INVQUAD && p->kernel != HM_KERNEL_GAUSS)
+  if (p->kernel < HM_KERNEL_CAUCHY || p->kernel > HM_KERNEL_GAUSS_DP)
     return fail(HM_ERR_ARG, "unknown kernel id " + std::to_string(p->kernel) +
                                 "; Hparams.Kernel must map to HM_KERNEL_*");
-  if (!(p->kparam > 0.0) && p->kernel != HM_KERNEL_INVQUAD) return fail(HM_ERR_ARG, "kernel parameter must be > 0");
+  if (!(p->kparam > 0.0) && p->kernel != HM_KERNEL_INVQUAD && p->kernel != HM_KERNEL_INVQUAD_DP)
+    return fail(HM_ERR_ARG, "kernel parameter must be > 0");
   if (p->max_rank < 1 || p->max_rank > 64) return fail(HM_ERR_ARG, "MaxRank must be in [1, 64]");
   if (p->min_block < 1) return fail(HM_ERR_ARG, "MinBlock must be >= 1");
   if (p->cons_method != HM_CONS_ACA2 && p->cons_method != HM_CONS_SVD)

@@ -53,7 +53,7 @@ __device__ __forceinline__ double kernel_eval(const KernelDesc& kd,
                                               const double* __restrict__ geom,
                                               int64_t n, int64_t i, int64_t j) {
   double s = 0.0;
-  if (kd.kind == HM_KERNEL_CAUCHY && kd.p != 1.0) {
+  if ((kd.kind == HM_KERNEL_CAUCHY && kd.p != 1.0) || kd.kind == HM_KERNEL_CAUCHY_DP) {
 #pragma unroll 3
     for (int q = 0; q < kd.dim; ++q) {
       double d = __ddiv_rn(__dsub_rn(geom[i + q * n], geom[j + q * n]), kd.p);
@@ -73,6 +73,15 @@ __device__ __forceinline__ double kernel_eval(const KernelDesc& kd,
     v = exp(-__ddiv_rn(s, __dmul_rn(__dmul_rn(2.0, kd.p), kd.p)));
   } else if (kd.kind == HM_KERNEL_INVQUAD) {
     v = __ddiv_rn(1.0, __dadd_rn(kd.p, s));
+  } else if (kd.kind == HM_KERNEL_CAUCHY_DP) {            // s = |x-y|^2 / p^2
+    const double t = __dadd_rn(1.0, s);
+    v = __ddiv_rn(__ddiv_rn(__dmul_rn(2.0, s), kd.p), __dmul_rn(t, t));
+  } else if (kd.kind == HM_KERNEL_INVQUAD_DP) {
+    const double t = __dadd_rn(kd.p, s);
+    v = -__ddiv_rn(1.0, __dmul_rn(t, t));
+  } else if (kd.kind == HM_KERNEL_GAUSS_DP) {
+    const double p3 = __dmul_rn(__dmul_rn(kd.p, kd.p), kd.p);
+    v = __dmul_rn(exp(-__ddiv_rn(s, __dmul_rn(__dmul_rn(2.0, kd.p), kd.p))), __ddiv_rn(s, p3));
   } else {
     v = __ddiv_rn(1.0, __dadd_rn(1.0, s));
   }

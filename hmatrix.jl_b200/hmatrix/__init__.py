@@ -25,12 +25,13 @@ import numpy as np
 from . import _lib
 from ._lib import HmError, check, lib
 from .cluster import Cluster, construct_cluster, neighbor_pairs
-from .kernels import Cauchy, Gauss, InvQuad, Kernel
+from .kernels import Cauchy, CauchyDP, Gauss, GaussDP, InvQuad, InvQuadDP, Kernel
 
 __all__ = [
     "Hparams", "Params", "NewHmat", "FullMat", "Hmat", "lu", "lu_", "getl", "getu", "info",
     "Cauchy", "InvQuad", "Gauss", "Kernel", "Cluster", "construct_cluster", "HmError",
-    "aca_wrapper", "F64", "F32", "BF16",
+    "aca_wrapper", "F64", "F32", "BF16", "new_on_cluster", "CauchyDP", "InvQuadDP", "GaussDP",
+    "lu_batch", "lu_batch_", "solve_batch", "solve_refined_batch", "matvec_batch",
 ]
 
 F64, F32, BF16 = _lib.HM_F64, _lib.HM_F32, _lib.HM_BF16
@@ -311,14 +312,27 @@ def NewHmat(prm: Params = None):
     if prm.MaxBlock == -1:
         prm.MaxBlock = n // 4                          # src/cluster.jl:37-39
     c = construct_cluster(X, prm.MinBlock, prm.Tree)
+    return c, new_on_cluster(prm, c)
+
+
+def new_on_cluster(prm: Params, c: Cluster):
+    """The H-matrix of ``prm`` on an existing cluster tree ``c`` (as NewHmat
+    after construct_cluster): H-matrices of several kernels on one tree share
+    the permutation and the block partition."""
+    X = np.asarray(c.X, dtype=np.float64)
+    if X.ndim == 1:
+        X = X.reshape(-1, 1)
+    n, d = X.shape
+    if prm.MaxBlock == -1:
+        prm.MaxBlock = n // 4                          # src/cluster.jl:37-39
     p = _params_struct(prm, d)
-    geom = np.asfortranarray(c.X)
+    geom = np.asfortranarray(X)
     nb = neighbor_pairs(c, prm.Adj)
     out = C.c_void_p()
     check(lib().hm_new(C.byref(p), n, _ptr(geom), c.ncluster, _ptr(c.s), _ptr(c.e), _ptr(c.left),
                        _ptr(c.right), 0 if nb is None else len(nb),
                        None if nb is None else _ptr(np.ascontiguousarray(nb)), C.byref(out)))
-    return c, Hmat(out.value, n, c)
+    return Hmat(out.value, n, c)
 
 
 def lu(H: Hmat):

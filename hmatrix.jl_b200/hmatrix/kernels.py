@@ -34,6 +34,11 @@ class Kernel:
     def __repr__(self):
         return "%s(%g)" % (type(self).__name__, self.p)
 
+    def dp(self):
+        """The derivative kernel dk/dp (same parameter p), for hyper-parameter
+        gradients; an H-matrix built with it compresses dk/dp itself."""
+        raise NotImplementedError("%s has no derivative kernel" % type(self).__name__)
+
 
 class Cauchy(Kernel):
     """k(x,y) = 1/(1 + |x-y|^2/ell^2); ``(x,y)->1/(1+(x-y)^2)`` of README.md:27 is Cauchy(1)."""
@@ -41,6 +46,9 @@ class Cauchy(Kernel):
 
     def __call__(self, X, Y):
         return 1.0 / (1.0 + self._sq(X, Y, None if self.p == 1.0 else self.p))
+
+    def dp(self):
+        return CauchyDP(self.p)
 
 
 class InvQuad(Kernel):
@@ -50,6 +58,9 @@ class InvQuad(Kernel):
     def __call__(self, X, Y):
         return 1.0 / (self.p + self._sq(X, Y))
 
+    def dp(self):
+        return InvQuadDP(self.p)
+
 
 class Gauss(Kernel):
     """k(x,y) = exp(-|x-y|^2/(2 ell^2))."""
@@ -57,3 +68,33 @@ class Gauss(Kernel):
 
     def __call__(self, X, Y):
         return np.exp(-self._sq(X, Y) / (2.0 * self.p * self.p))
+
+    def dp(self):
+        return GaussDP(self.p)
+
+
+class CauchyDP(Kernel):
+    """d/d ell of Cauchy(ell): 2 s/ell / (1 + s)^2 with s = |x-y|^2/ell^2."""
+    kind = _lib.HM_KERNEL_CAUCHY_DP
+
+    def __call__(self, X, Y):
+        s = self._sq(X, Y, self.p)
+        return 2.0 * s / self.p / ((1.0 + s) * (1.0 + s))
+
+
+class InvQuadDP(Kernel):
+    """d/dc of InvQuad(c): -1/(c + |x-y|^2)^2."""
+    kind = _lib.HM_KERNEL_INVQUAD_DP
+
+    def __call__(self, X, Y):
+        t = self.p + self._sq(X, Y)
+        return -1.0 / (t * t)
+
+
+class GaussDP(Kernel):
+    """d/d ell of Gauss(ell): exp(-|x-y|^2/(2 ell^2)) |x-y|^2 / ell^3."""
+    kind = _lib.HM_KERNEL_GAUSS_DP
+
+    def __call__(self, X, Y):
+        s = self._sq(X, Y)
+        return np.exp(-s / (2.0 * self.p * self.p)) * s / self.p ** 3

@@ -42,6 +42,12 @@ extern "C" {
 #define HM_KERNEL_CAUCHY   1   /* 1/(1 + |x-y|^2/p^2)      p = kparam (ell)   */
 #define HM_KERNEL_INVQUAD  2   /* 1/(p + |x-y|^2)          p = kparam (c)     */
 #define HM_KERNEL_GAUSS    3   /* exp(-|x-y|^2/(2 p^2))    p = kparam (ell)   */
+/* Derivatives of the kernels above with respect to their parameter p, for the
+ * hyper-parameter gradients u'(dH/dp)v (no counterpart in the reference): an
+ * H-matrix built with one of these ids compresses dK/dp itself. */
+#define HM_KERNEL_CAUCHY_DP   4   /* 2 s/p / (1 + s)^2, s = |x-y|^2/p^2         */
+#define HM_KERNEL_INVQUAD_DP  5   /* -1/(p + |x-y|^2)^2                          */
+#define HM_KERNEL_GAUSS_DP    6   /* exp(-|x-y|^2/(2 p^2)) |x-y|^2 / p^3         */
 
 /* ---- construction methods (Hparams.ConsMethod) --------------------------- */
 #define HM_CONS_ACA2       1   /* partially pivoted ACA, src/hlu.jl:59-111    */
