@@ -31,7 +31,7 @@ __all__ = [
     "Hparams", "Params", "NewHmat", "FullMat", "Hmat", "lu", "lu_", "getl", "getu", "info",
     "Cauchy", "InvQuad", "Gauss", "Kernel", "Cluster", "construct_cluster", "HmError",
     "aca_wrapper", "F64", "F32", "BF16", "new_on_cluster", "CauchyDP", "InvQuadDP", "GaussDP",
-    "lu_batch", "lu_batch_", "solve_batch", "solve_refined_batch", "matvec_batch",
+    "lu_batch", "lu_batch_", "solve_batch", "solve_refined_batch", "matvec_batch", "gmres", "bicgstab",
 ]
 
 F64, F32, BF16 = _lib.HM_F64, _lib.HM_F32, _lib.HM_BF16
@@ -456,3 +456,6 @@ def aca_wrapper(A, eps, rank):
         raise HmError(-R, _lib.last_error())
     M = min(R, rank + 1)
     return Uf[:, :M].copy(), Vf[:, :M].copy(), R
+
+
+from .krylov import bicgstab, gmres  # noqa: E402  (src/tools.jl:7-65)
