@@ -12,12 +12,15 @@ namespace hm {
 // sided Jacobi SVD of W, truncation k = #{s_i/s_1 > eps_trunc}, and
 // A' = Q_A U_k, B' = Q_B V_k S_k.  One CTA per job; smem 3*rmax^2 doubles.
 // ===========================================================================
+// Columns [0, j0) are already orthonormal and their block of Rm is set by the
+// caller (cgs2_qr zeroes the rest of Rm first).
 static __device__ void cgs2_qr(double* X, int len, int ld, int r, double* Rm /* r x r, col-major */,
-                        double* proj /* r */, double* red) {
-  for (int e = threadIdx.x; e < r * r; e += blockDim.x) Rm[e] = 0.0;
+                        double* proj /* r */, double* red, int j0 = 0) {
+  for (int e = threadIdx.x; e < r * r; e += blockDim.x)
+    if (!(e % r < j0 && e / r < j0)) Rm[e] = 0.0;
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int j = 0; j < r; ++j) {
+  for (int j = j0; j < r; ++j) {
     double* xj = X + (int64_t)j * ld;
     for (int pass = 0; pass < 2; ++pass) {
       for (int i = w; i < j; i += nw) {
@@ -82,8 +85,32 @@ static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, i
     if (threadIdx.x == 0) *J.rank = 0;
     return;
   }
-  cgs2_qr(J.A, J.m, J.lda, r, b0, proj, red);
-  cgs2_qr(J.B, J.n, J.ldb, r, b1, proj, red);
+  const int ok = min(J.ortho_k, r);
+  if (ok > 0) {
+    // A's leading columns are orthonormal: R_A = I there.  B's are orthogonal:
+    // normalise them, R_B = diag(norms).
+    for (int e = threadIdx.x; e < ok * ok; e += blockDim.x) {
+      const int i = e % ok, j = e / ok;
+      b0[i + j * r] = (i == j) ? 1.0 : 0.0;
+      b1[i + j * r] = 0.0;
+    }
+    for (int j = w; j < ok; j += nw) {
+      double s = 0.0;
+      for (int t = lane; t < J.n; t += 32) s = fma(J.B[t + (int64_t)j * J.ldb], J.B[t + (int64_t)j * J.ldb], s);
+      s = warp_sum(s);
+      if (lane == 0) proj[j] = sqrt(s);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < J.n * ok; e += blockDim.x) {
+      const int t = e % J.n, j = e / J.n;
+      const double nj = proj[j];
+      J.B[t + (int64_t)j * J.ldb] = nj > 0.0 ? J.B[t + (int64_t)j * J.ldb] / nj : 0.0;
+    }
+    if (threadIdx.x < ok) b1[threadIdx.x + threadIdx.x * r] = proj[threadIdx.x];
+    __syncthreads();
+  }
+  cgs2_qr(J.A, J.m, J.lda, r, b0, proj, red, ok);
+  cgs2_qr(J.B, J.n, J.ldb, r, b1, proj, red, ok);
   // W = R_A R_B^T  (r x r, column-major, ld r)
   double sabs = 0.0;
   for (int e = threadIdx.x; e < r * r; e += blockDim.x) {

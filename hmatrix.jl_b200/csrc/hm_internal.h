@@ -152,6 +152,9 @@ struct MvPlan {
   P1Desc* d_p1s = nullptr;         // the same descriptors ordered by input segment (multi-RHS phase 1; built on first use)
   uint32_t* d_g1s = nullptr;       // groups of d_p1s sharing a segment (ng1 + 1 starts)
   int64_t ng1 = 0;
+  uint32_t* d_t1s = nullptr;       // segment tasks of d_p1s (nt1 + 1 starts)
+  int64_t nt1 = 0;
+  uint32_t maxlen1 = 0;            // longest segment
   P2Desc* d_p2 = nullptr;
   int64_t np2 = 0;
   MvWin* d_win = nullptr;

@@ -84,6 +84,8 @@ struct CoreJob {
   const int32_t* r_dev;    // if set: the core size r is read on the device
   const int32_t* pre_status;  // if set: status of the fully pivoted ACA that made A, B
   int32_t zero_fill;       // zero the output columns [k, kcap)
+  int32_t ortho_k;         // the first ortho_k columns of A are orthonormal and those of B
+                           // mutually orthogonal (a previous core's output): no QR for them
 };
 
 // Fully pivoted ACA job (deps/src/ACA_FullyPivoted.cpp:9-151).  rel_mode: the

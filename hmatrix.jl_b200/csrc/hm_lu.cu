@@ -1439,6 +1439,9 @@ __global__ void __launch_bounds__(128) lu_tile_core_kernel(TileJobArgs a, int rl
   J.m = mi; J.n = nj; J.r = r; J.lda = max(mi, 1); J.ldb = max(nj, 1);
   J.ldoa = mi; J.ldob = nj; J.kcap = a.cap;
   J.zero_test = 1; J.rank = kij; J.zero_fill = 1;
+  // from step 1 on, every trailing tile (and tile (k, j)) is a previous step's
+  // core output: A_ij orthonormal, B_ij and B_kj with orthogonal columns
+  J.ortho_k = a.k >= 1 ? k1 : 0;
   core_body(J, rl, eps_trunc, a.flags);
 }
 

@@ -335,6 +335,7 @@ void free_mv_plan(MvPlan& p) {
   if (p.d_p1) cudaFree(p.d_p1);
   if (p.d_p1s) cudaFree(p.d_p1s);
   if (p.d_g1s) cudaFree(p.d_g1s);
+  if (p.d_t1s) cudaFree(p.d_t1s);
   if (p.d_p2) cudaFree(p.d_p2);
   if (p.d_win) cudaFree(p.d_win);
   p = MvPlan{};

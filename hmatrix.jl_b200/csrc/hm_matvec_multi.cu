@@ -182,6 +182,84 @@ __global__ void __launch_bounds__(256) mvm_phase1_kernel(const P1Desc* __restric
   }
 }
 
+// Phase 1, segment tasks: a CTA takes up to S1_LEAVES leaves that share one
+// input segment (descriptors ordered by segment) and stages the segment's rows
+// of X (its CB columns) in shared memory once; each warp then runs one leaf at
+// a time with lane = (row sub-index, column pair) reading X from shared memory
+// and the factor values of a 32-row chunk handed out by shuffles.
+constexpr int S1_LEAVES = 64;
+constexpr int S1_ROWS = 512;                // factor rows prefetched per pass
+
+template <typename T, int CB>
+__global__ void __launch_bounds__(256) mvm_phase1_seg_kernel(const P1Desc* __restrict__ d,
+                                                             const uint32_t* __restrict__ task, int64_t ntask,
+                                                             const T* __restrict__ pool,
+                                                             const double* __restrict__ xr, int ld, int ncb,
+                                                             double* __restrict__ zr) {
+  constexpr int CP = CB / 2, RS = 32 / CP, IT = 32 / RS;
+  extern __shared__ double xs[];                     // len x CB, row-major
+  const int64_t tk = blockIdx.x / ncb;
+  const int cb = (int)(blockIdx.x % ncb);
+  const uint32_t b0 = task[tk], b1 = task[tk + 1];
+  const uint32_t seg0 = d[b0].seg0, len = d[b0].len;
+  const double* xb = xr + (int64_t)seg0 * ld + cb * CB;
+  for (uint32_t e = threadIdx.x; e < len * (CB / 2); e += blockDim.x) {
+    const uint32_t row = e / (CB / 2), c2 = e % (CB / 2);
+    reinterpret_cast<double2*>(xs)[e] = __ldg(reinterpret_cast<const double2*>(xb + (int64_t)row * ld) + c2);
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int cp = lane % CP, rs = lane / CP;
+  for (uint32_t b = b0 + warp; b < b1; b += blockDim.x / 32) {
+    const P1Desc D = d[b];
+    const T* F = pool + D.off;
+    for (int r = 0; r < D.k; r += 2) {
+      const bool two = r + 1 < D.k;
+      const T* f0 = F + (int64_t)r * D.stride;
+      double a00 = 0.0, a01 = 0.0, a10 = 0.0, a11 = 0.0;
+      // blocks of S1_ROWS rows: all factor values of a block are loaded first
+      // (one memory round trip), then handed out chunk by chunk
+      for (uint32_t base = 0; base < len; base += S1_ROWS) {
+        double u0[S1_ROWS / 32], u1[S1_ROWS / 32];
+#pragma unroll
+        for (int q = 0; q < S1_ROWS / 32; ++q) {
+          const uint32_t row = base + 32 * q + lane;
+          u0[q] = row < len ? (double)from_store<T>(f0[row]) : 0.0;
+          u1[q] = (two && row < len) ? (double)from_store<T>(f0[D.stride + row]) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < S1_ROWS / 32; ++q) {
+          const uint32_t r0 = base + 32 * q;
+          if (r0 >= len) break;
+#pragma unroll
+          for (int it = 0; it < IT; ++it) {
+            const uint32_t rr = r0 + RS * it + rs;
+            const double2 xv = rr < len ? reinterpret_cast<const double2*>(xs)[rr * CP + cp] : make_double2(0.0, 0.0);
+            const double u = __shfl_sync(0xffffffffu, u0[q], RS * it + rs);
+            const double v = __shfl_sync(0xffffffffu, u1[q], RS * it + rs);
+            a00 = fma(u, xv.x, a00);
+            a01 = fma(u, xv.y, a01);
+            a10 = fma(v, xv.x, a10);
+            a11 = fma(v, xv.y, a11);
+          }
+        }
+      }
+#pragma unroll
+      for (int o = CP; o < 32; o <<= 1) {
+        a00 += __shfl_xor_sync(0xffffffffu, a00, o);
+        a01 += __shfl_xor_sync(0xffffffffu, a01, o);
+        a10 += __shfl_xor_sync(0xffffffffu, a10, o);
+        a11 += __shfl_xor_sync(0xffffffffu, a11, o);
+      }
+      if (rs == 0) {
+        *reinterpret_cast<double2*>(zr + (int64_t)(D.zoff + r) * ld + cb * CB + 2 * cp) = make_double2(a00, a01);
+        if (two)
+          *reinterpret_cast<double2*>(zr + (int64_t)(D.zoff + r + 1) * ld + cb * CB + 2 * cp) = make_double2(a10, a11);
+      }
+    }
+  }
+}
+
 constexpr int M2_THREADS = 256;             // 2 rows a thread: half a window
 constexpr int M2_NB = 32;                   // descriptors staged per round
 constexpr uint64_t M2_DENSE_FLAG = 1ull << 63;
@@ -198,7 +276,7 @@ __global__ void __launch_bounds__(M2_THREADS) mvm_phase2_kernel(const MvWin* __r
                                                                 const double* __restrict__ xr, int ld, int ncb,
                                                                 double* __restrict__ Y, int64_t ldy, int ncols) {
   constexpr int EMAX = M2Cfg<CB>::EMAX;
-  constexpr int U = 2;
+  constexpr int U = CB >= 16 ? 4 : 8;         // entries whose factor loads are in flight together
   __shared__ P2Desc sd[M2_NB];
   __shared__ int spre[M2_NB + 1];
   __shared__ uint64_t e_off[EMAX];
@@ -347,6 +425,21 @@ static int ensure_sorted_p1(MvPlan& P) {
   }
   P.ng1 = (int64_t)g.size();
   g.push_back((uint32_t)v.size());
+  // segment tasks: runs of equal (seg0, len), cut every S1_LEAVES leaves
+  std::vector<uint32_t> tk;
+  uint32_t maxlen = 0;
+  for (size_t i = 0; i < v.size();) {
+    size_t j = i + 1;
+    while (j < v.size() && j - i < (size_t)S1_LEAVES && v[j].seg0 == v[i].seg0 && v[j].len == v[i].len) ++j;
+    tk.push_back((uint32_t)i);
+    maxlen = std::max(maxlen, v[i].len);
+    i = j;
+  }
+  P.nt1 = (int64_t)tk.size();
+  P.maxlen1 = maxlen;
+  tk.push_back((uint32_t)v.size());
+  HM_CUDA_TRY(cudaMalloc(&P.d_t1s, sizeof(uint32_t) * tk.size()));
+  HM_CUDA_TRY(cudaMemcpy(P.d_t1s, tk.data(), sizeof(uint32_t) * tk.size(), cudaMemcpyHostToDevice));
   HM_CUDA_TRY(cudaMalloc(&P.d_p1s, sizeof(P1Desc) * v.size()));
   HM_CUDA_TRY(cudaMemcpy(P.d_p1s, v.data(), sizeof(P1Desc) * v.size(), cudaMemcpyHostToDevice));
   HM_CUDA_TRY(cudaMalloc(&P.d_g1s, sizeof(uint32_t) * g.size()));
@@ -379,7 +472,12 @@ int launch_multi(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, in
     const unsigned g = (unsigned)std::min<int64_t>((tot + 255) / 256, (int64_t)nsm * 16);
     mvm_xr_kernel<<<g, 256, 0, st>>>(d_x, h->n, h->n, (int)ncols, xr, ld);
   }
-  if (P.np1 > 0) {
+  const size_t seg_smem = sizeof(double) * (size_t)P.maxlen1 * CB;
+  if (P.np1 > 0 && seg_smem <= 96 * 1024 && P.nt1 * ncb <= (int64_t)INT32_MAX) {
+    HM_CUDA_TRY(smem_attr((const void*)mvm_phase1_seg_kernel<T, CB>, 96 * 1024));
+    mvm_phase1_seg_kernel<T, CB><<<(unsigned)(P.nt1 * ncb), 256, seg_smem, st>>>(P.d_p1s, P.d_t1s, P.nt1,
+                                                                               (const T*)h->d_rk, xr, ld, ncb, zr);
+  } else if (P.np1 > 0) {                        // segments too long to stage: grouped leaves
     const int64_t warps = P.ng1 * ncb;
     const int64_t blocks = std::min<int64_t>((warps + 7) / 8, (int64_t)nsm * 8);
     mvm_phase1_kernel<T, CB><<<(unsigned)blocks, 256, 0, st>>>(P.d_p1s, P.d_g1s, P.ng1, (const T*)h->d_rk, xr, ld,
