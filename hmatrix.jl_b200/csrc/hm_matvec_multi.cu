@@ -184,11 +184,13 @@ __global__ void __launch_bounds__(256) mvm_phase1_kernel(const P1Desc* __restric
 
 // Phase 1, segment tasks: a CTA takes up to S1_LEAVES leaves that share one
 // input segment (descriptors ordered by segment) and stages the segment's rows
-// of X (its CB columns) in shared memory once; each warp then runs one leaf at
-// a time with lane = (row sub-index, column pair) reading X from shared memory
-// and the factor values of a 32-row chunk handed out by shuffles.
+// of X (its CB columns) in shared memory once, rows padded by two doubles so
+// that the 32 rows a warp reads at a time fall in distinct banks.  Each warp
+// runs one leaf at a time, lane = row: its factor values come from its own
+// coalesced loads (a block of S1_ROWS rows prefetched at once), its x row from
+// shared memory, and the 2 x CB sums are reduced over the warp at the end.
 constexpr int S1_LEAVES = 64;
-constexpr int S1_ROWS = 512;                // factor rows prefetched per pass
+constexpr int S1_ROWS = 256;                // factor rows prefetched per pass
 
 template <typename T, int CB>
 __global__ void __launch_bounds__(256) mvm_phase1_seg_kernel(const P1Desc* __restrict__ d,
@@ -196,8 +198,9 @@ __global__ void __launch_bounds__(256) mvm_phase1_seg_kernel(const P1Desc* __res
                                                              const T* __restrict__ pool,
                                                              const double* __restrict__ xr, int ld, int ncb,
                                                              double* __restrict__ zr) {
-  constexpr int CP = CB / 2, RS = 32 / CP, IT = 32 / RS;
-  extern __shared__ double xs[];                     // len x CB, row-major
+  constexpr int XS = CB + 2;                          // padded row of the staged X
+  constexpr int NV = 2 * CB;
+  extern __shared__ double xs[];                     // len x XS
   const int64_t tk = blockIdx.x / ncb;
   const int cb = (int)(blockIdx.x % ncb);
   const uint32_t b0 = task[tk], b1 = task[tk + 1];
@@ -205,20 +208,20 @@ __global__ void __launch_bounds__(256) mvm_phase1_seg_kernel(const P1Desc* __res
   const double* xb = xr + (int64_t)seg0 * ld + cb * CB;
   for (uint32_t e = threadIdx.x; e < len * (CB / 2); e += blockDim.x) {
     const uint32_t row = e / (CB / 2), c2 = e % (CB / 2);
-    reinterpret_cast<double2*>(xs)[e] = __ldg(reinterpret_cast<const double2*>(xb + (int64_t)row * ld) + c2);
+    *reinterpret_cast<double2*>(xs + row * XS + 2 * c2) =
+        __ldg(reinterpret_cast<const double2*>(xb + (int64_t)row * ld) + c2);
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int cp = lane % CP, rs = lane / CP;
   for (uint32_t b = b0 + warp; b < b1; b += blockDim.x / 32) {
     const P1Desc D = d[b];
     const T* F = pool + D.off;
     for (int r = 0; r < D.k; r += 2) {
       const bool two = r + 1 < D.k;
       const T* f0 = F + (int64_t)r * D.stride;
-      double a00 = 0.0, a01 = 0.0, a10 = 0.0, a11 = 0.0;
-      // blocks of S1_ROWS rows: all factor values of a block are loaded first
-      // (one memory round trip), then handed out chunk by chunk
+      double v[NV];
+#pragma unroll
+      for (int c = 0; c < NV; ++c) v[c] = 0.0;
       for (uint32_t base = 0; base < len; base += S1_ROWS) {
         double u0[S1_ROWS / 32], u1[S1_ROWS / 32];
 #pragma unroll
@@ -229,32 +232,26 @@ __global__ void __launch_bounds__(256) mvm_phase1_seg_kernel(const P1Desc* __res
         }
 #pragma unroll
         for (int q = 0; q < S1_ROWS / 32; ++q) {
-          const uint32_t r0 = base + 32 * q;
-          if (r0 >= len) break;
+          const uint32_t row = base + 32 * q + lane;
+          if (base + 32 * q >= len) break;
+          if (row < len) {
+            const double* xrow = xs + row * XS;
 #pragma unroll
-          for (int it = 0; it < IT; ++it) {
-            const uint32_t rr = r0 + RS * it + rs;
-            const double2 xv = rr < len ? reinterpret_cast<const double2*>(xs)[rr * CP + cp] : make_double2(0.0, 0.0);
-            const double u = __shfl_sync(0xffffffffu, u0[q], RS * it + rs);
-            const double v = __shfl_sync(0xffffffffu, u1[q], RS * it + rs);
-            a00 = fma(u, xv.x, a00);
-            a01 = fma(u, xv.y, a01);
-            a10 = fma(v, xv.x, a10);
-            a11 = fma(v, xv.y, a11);
+            for (int c = 0; c < CB; c += 2) {
+              const double2 xv = *reinterpret_cast<const double2*>(xrow + c);
+              v[c] = fma(u0[q], xv.x, v[c]);
+              v[c + 1] = fma(u0[q], xv.y, v[c + 1]);
+              v[CB + c] = fma(u1[q], xv.x, v[CB + c]);
+              v[CB + c + 1] = fma(u1[q], xv.y, v[CB + c + 1]);
+            }
           }
         }
       }
-#pragma unroll
-      for (int o = CP; o < 32; o <<= 1) {
-        a00 += __shfl_xor_sync(0xffffffffu, a00, o);
-        a01 += __shfl_xor_sync(0xffffffffu, a01, o);
-        a10 += __shfl_xor_sync(0xffffffffu, a10, o);
-        a11 += __shfl_xor_sync(0xffffffffu, a11, o);
-      }
-      if (rs == 0) {
-        *reinterpret_cast<double2*>(zr + (int64_t)(D.zoff + r) * ld + cb * CB + 2 * cp) = make_double2(a00, a01);
-        if (two)
-          *reinterpret_cast<double2*>(zr + (int64_t)(D.zoff + r + 1) * ld + cb * CB + 2 * cp) = make_double2(a10, a11);
+      int idx;
+      const double sum = warp_reduce_scatter<NV>(v, lane, idx);
+      if ((lane & (32 / NV - 1)) == 0) {
+        const int rank = r + idx / CB, col = idx % CB;
+        if (rank < D.k) zr[(int64_t)(D.zoff + rank) * ld + cb * CB + col] = sum;
       }
     }
   }
@@ -472,7 +469,7 @@ int launch_multi(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, in
     const unsigned g = (unsigned)std::min<int64_t>((tot + 255) / 256, (int64_t)nsm * 16);
     mvm_xr_kernel<<<g, 256, 0, st>>>(d_x, h->n, h->n, (int)ncols, xr, ld);
   }
-  const size_t seg_smem = sizeof(double) * (size_t)P.maxlen1 * CB;
+  const size_t seg_smem = sizeof(double) * (size_t)P.maxlen1 * (CB + 2);
   if (P.np1 > 0 && seg_smem <= 96 * 1024 && P.nt1 * ncb <= (int64_t)INT32_MAX) {
     HM_CUDA_TRY(smem_attr((const void*)mvm_phase1_seg_kernel<T, CB>, 96 * 1024));
     mvm_phase1_seg_kernel<T, CB><<<(unsigned)(P.nt1 * ncb), 256, seg_smem, st>>>(P.d_p1s, P.d_t1s, P.nt1,
