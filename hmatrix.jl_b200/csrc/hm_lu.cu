@@ -1673,15 +1673,14 @@ static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vecto
   }
 }
 
-// y = P b, forward (unit L), backward (U) tile by tile; trans: U' then L'
 // ---- sweep solve ---------------------------------------------------------
 // The triangular solves over the tile level as one kernel per tile: step k of
 // a sweep finishes tile k (the update from the tile finished at step k-1, then
-// the diagonal tile's triangular solve) in CTA 0, while the other CTAs apply
-// the same finished tile's update to every later tile: 2T launches a solve.
-// The diagonal solves multiply by the inverses of the diagonal tiles' L and U
-// factors (computed once from the factored tiles), so a step has no
-// row-by-row dependency chain.
+// the diagonal tile's triangular solve) in a few finisher CTAs, while the
+// other CTAs apply the same finished tile's update to every later tile: 2T
+// launches a solve.  The diagonal solves multiply by the inverses of the
+// diagonal tiles' L and U factors (computed once from the factored tiles), so
+// a step has no row-by-row dependency chain.
 constexpr int SW_THREADS = 256;
 
 struct SweepTab {
@@ -2017,6 +2016,8 @@ static void tile_sweeps(Ctx& c, const TileLU& TL, View X, bool trans) {
   }
 }
 
+// y = P b, forward (unit L), backward (U) tile by tile; trans: U' then L'
+// (the launch-per-operation form, used beyond SWEEP_MAX_COLS right-hand sides)
 static void tile_solve(Ctx& c, const TileLU& TL, View X, bool trans, double* Zext) {
   const int T = TL.T, cap = c.cap, nc = X.cols;
   auto yv = [&](int i) { return vsub(X, (int)TL.start[i], 0, (int)TL.size[i], nc); };
