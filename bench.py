@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--lu-n", type=int, default=1 << 16, help="size of the H-LU + solve leg")
     ap.add_argument("--rhs", default="16,64",
                     help="column counts of the multi-RHS matvec leg (comma separated; empty to skip)")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with --gpus N > 1: N independent copies of H instead of row shards of one H")
     ap.add_argument("--batch", type=int, default=0,
                     help="also run the batched uneven H-LU + solve leg with this many problems (256 in full)")
     ap.add_argument("--batch-nthreads", type=int, default=0, help="host threads of the batched calls (0: auto)")
@@ -194,13 +196,18 @@ def run_reference(a):
 # --------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------
-def build(n, storage):
+def build(n, storage, shard=None):
+    """The benchmark H-matrix; with shard = (rank, world), this rank's row shard."""
     import hmatrix as hm
     prm = hm.Params(Geom=np.linspace(0, 10, n), Kernel=hm.Cauchy(1.0), MaxBlock=512, MinBlock=64,
                     MaxRank=16, ConsMethod="aca2", εComp=1e-8, Tree="bisect",
                     Storage={"f64": hm.F64, "f32": hm.F32, "bf16": hm.BF16}[storage],
                     Device=int(os.environ.get("LOCAL_RANK", "0")))
     t0 = time.perf_counter()
+    if shard is not None:
+        from hmatrix.shard import ShardedHmat
+        S = ShardedHmat(prm, shard[0], shard[1])
+        return S.c, S.H, time.perf_counter() - t0
     c, H = hm.NewHmat(prm)
     return c, H, time.perf_counter() - t0
 
@@ -222,7 +229,7 @@ def job_value(bytes_per_rank, world, ms):
     return world * bytes_per_rank / (ms * 1e-3) / 1e9
 
 
-def measure(H, a, torch, dist, world):
+def measure(H, a, torch, dist, world, shard=False):
     import ctypes as C
     from hmatrix import _lib
     L = _lib.lib()
@@ -237,6 +244,8 @@ def measure(H, a, torch, dist, world):
 
     def step():
         _lib.check(L.hm_matvec(H._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), 1, 0, flags, sp))
+        if shard:                            # every rank's rows -> the full H*x on every rank
+            dist.all_reduce(y)
 
     for _ in range(a.warmup):
         step()
@@ -267,16 +276,29 @@ def measure(H, a, torch, dist, world):
     ms = job_time(e0.elapsed_time(e1) / a.steps, dist, "cuda")
     if dist is not None:
         dist.barrier()
-    # end to end through the C ABI with host pinned buffers
+    # end to end with host pinned buffers: through the C ABI's host-pointer path
+    # on one GPU; with shards, x copied in, the shard's matvec, the all-reduce
+    # and y copied out, every step
     xh = x.cpu().pin_memory()
     yh = torch.empty_like(xh).pin_memory()
+    xd, yd = torch.empty_like(x), torch.empty_like(x)
+
+    def e2e_step():
+        if not shard:
+            _lib.check(L.hm_matvec(H._h, C.c_void_p(xh.data_ptr()), C.c_void_p(yh.data_ptr()), 1, 0, 0, None))
+            return
+        xd.copy_(xh, non_blocking=True)
+        _lib.check(L.hm_matvec(H._h, C.c_void_p(xd.data_ptr()), C.c_void_p(yd.data_ptr()), 1, 0, flags, sp))
+        dist.all_reduce(yd)
+        yh.copy_(yd, non_blocking=True)
+        torch.cuda.synchronize()
     for _ in range(2):
-        _lib.check(L.hm_matvec(H._h, C.c_void_p(xh.data_ptr()), C.c_void_p(yh.data_ptr()), 1, 0, 0, None))
+        e2e_step()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     ke = max(3, a.steps // 2)
     for _ in range(ke):
-        _lib.check(L.hm_matvec(H._h, C.c_void_p(xh.data_ptr()), C.c_void_p(yh.data_ptr()), 1, 0, 0, None))
+        e2e_step()
     e2e_ms = job_time((time.perf_counter() - t0) / ke * 1e3, dist, "cuda")
     # accuracy: 4096 sampled rows against exact FP64 kernel rows (dense oracle)
     rows = np.sort(np.random.default_rng(2).choice(n, 4096, replace=False))
@@ -440,14 +462,23 @@ def run_ours(a):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     import hmatrix as hm
-    c, H, t_build = build(a.n, a.storage)
+    shard = world > 1 and not a.replicas
+    c, H, t_build = build(a.n, a.storage, (rank, world) if shard else None)
     info = H.info()
-    ms, ph, ck, e2e_ms, rel = measure(H, a, torch, dist, world)
+    ms, ph, ck, e2e_ms, rel = measure(H, a, torch, dist, world, shard)
     eb = {"f64": 8, "f32": 4, "bf16": 2}[a.storage]
     deb = 8 if a.storage == "f64" else 4
     bytes_mv = eb * info.rk_entries + deb * info.dense_entries + 16 * a.n
-    value = job_value(bytes_mv, world, ms)
-    e2e = job_value(bytes_mv, world, e2e_ms)
+    if shard:
+        # strong scaling: one H over all ranks; its bytes are the sum of the shards'
+        tb = torch.tensor([float(eb * info.rk_entries + deb * info.dense_entries)], device="cuda")
+        dist.all_reduce(tb)
+        bytes_mv = float(tb.item()) + 16 * a.n
+        value = bytes_mv / (ms * 1e-3) / 1e9
+        e2e = bytes_mv / (e2e_ms * 1e-3) / 1e9
+    else:
+        value = job_value(bytes_mv, world, ms)
+        e2e = job_value(bytes_mv, world, e2e_ms)
     peak, peak_kind = peaks()
     # dominant kernel: the phase with the larger device time; its algorithmic
     # bytes: phase 1 streams the B factors (+x segments from L2), phase 2 the
@@ -501,9 +532,11 @@ def run_ours(a):
         gbs, thr, sample, _ = cpu_sample_gbs(a.n, a.cpu_rows)
         cpu = {"value": gbs, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong" if shard else "weak",
             "vs_baseline": None, "dtype": a.storage, "data": "synthetic",
-            "config": dict(workload(a.n), storage=a.storage, parallelism="replicas" if world > 1 else "1 GPU"),
+            "config": dict(workload(a.n), storage=a.storage, parallelism=("%d row shards, NCCL all-reduce of y" % world) if shard
+                        else ("replicas" if world > 1 else "1 GPU")),
             "clocks": ck,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * a.n, "d2h_bytes_per_step": 8 * a.n,
                     "ms_per_step": e2e_ms},

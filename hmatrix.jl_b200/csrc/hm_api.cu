@@ -360,6 +360,7 @@ int hm_copy(const hm_handle* h, hm_handle** out) {
 int hm_lu(hm_handle* h) {
   if (!h) return fail(HM_ERR_ARG, "NULL handle");
   if (h->factorized) return fail(HM_ERR_STATE, "H-matrix H is already factorized; reuse factorization");
+  if (h->prm.row_hi > h->prm.row_lo) return fail(HM_ERR_UNSUPPORTED, "lu! of a row shard of H");
   DeviceGuard g(h->device);
   return lu_factor(h);
 }

@@ -225,6 +225,28 @@ int build_handle(hm_handle* h, const double* geom, int64_t ncl, const int64_t* c
   }
   enumerate_leaves(h);
 
+  // ---- a shard: only the leaves of rows [row_lo, row_hi) ------------------
+  if (p.row_hi > p.row_lo) {
+    if (p.row_lo < 0 || p.row_hi > n) return fail(HM_ERR_ARG, "row range outside [0, n)");
+    std::vector<Leaf> keep;
+    for (auto& L : h->leaves) {
+      const int64_t a = L.row0, b = L.row0 + L.m;
+      if (a >= p.row_lo && b <= p.row_hi) {
+        h->nodes[L.node].leaf = (int32_t)keep.size();
+        keep.push_back(L);
+      } else if (b > p.row_lo && a < p.row_hi) {
+        return fail(HM_ERR_ARG, "row range [" + std::to_string(p.row_lo) + ", " + std::to_string(p.row_hi) +
+                                    ") cuts the rows [" + std::to_string(a) + ", " + std::to_string(b) +
+                                    ") of a leaf");
+      } else {
+        h->nodes[L.node].leaf = -1;
+      }
+    }
+    h->leaves.swap(keep);
+  } else if (p.row_lo != 0 || p.row_hi != 0) {
+    return fail(HM_ERR_ARG, "row range must satisfy row_lo < row_hi (or both 0)");
+  }
+
   // ---- ranks of the low-rank leaves ---------------------------------------
   std::vector<int64_t> rk_leaf;     // leaf indices of low-rank leaves
   for (int64_t i = 0; i < (int64_t)h->leaves.size(); ++i)

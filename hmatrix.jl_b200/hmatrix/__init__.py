@@ -59,6 +59,7 @@ class Params:
     RankCap: int = 0                      # rank capacity during H-LU (0: automatic)
     LuMode: str = "auto"                  # "auto" | "recursive" (lu! as written) | "tiles"
     εTruncLU: float = 0.0                 # truncation inside H-LU (0: εTrunc, as in the reference)
+    RowRange: tuple = (0, 0)              # build only rows [lo, hi) (a multi-GPU shard); (0, 0): all
 
 
 Hparams = Params()
@@ -101,6 +102,7 @@ def _params_struct(prm: Params, dim: int):
     p.rank_cap = prm.RankCap
     p.lu_mode = {"auto": 0, "recursive": 1, "tiles": 2}[prm.LuMode]
     p.eps_trunc_lu = prm.εTruncLU
+    p.row_lo, p.row_hi = int(prm.RowRange[0]), int(prm.RowRange[1])
     return p
 
 

@@ -45,7 +45,7 @@ class hm_params(C.Structure):
         ("max_block", C.c_int32), ("min_block", C.c_int32), ("cons_method", C.c_int32),
         ("aca_force", C.c_int32), ("storage", C.c_int32), ("device", C.c_int32),
         ("rank_cap", C.c_int32), ("lu_mode", C.c_int32), ("reserved0", C.c_int32),
-        ("eps_trunc_lu", C.c_double), ("reserved", C.c_int32 * 2),
+        ("eps_trunc_lu", C.c_double), ("row_lo", C.c_int32), ("row_hi", C.c_int32),
     ]
 
 

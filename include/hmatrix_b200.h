@@ -87,7 +87,13 @@ typedef struct hm_params {
                              H-LU (0: eps_trunc, as in the reference); a looser
                              value gives a cheaper factorisation that
                              hm_solve_refined brings back to full accuracy */
-    int32_t reserved[2];
+    int32_t row_lo;       /* rows [row_lo, row_hi) of H only (0, 0: all rows):
+                             a shard of a row-partitioned H for multi-GPU use.
+                             The range must not cut a leaf (cut at clusters of
+                             the first admissible level).  H*x of a shard gives
+                             its rows and zeros elsewhere, H'*x its share of
+                             the sum; hm_lu refuses a shard (HM_ERR_UNSUPPORTED) */
+    int32_t row_hi;
 } hm_params;
 
 /* info(H) of src/utils.jl:83-110 plus the byte counts used for rooflines. */

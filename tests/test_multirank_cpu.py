@@ -59,3 +59,76 @@ def test_single_rank_passthrough():
     import bench
     assert bench.job_time(7.0, None, "cpu") == 7.0
     assert bench.job_value(2e9, 1, 10.0) == pytest.approx(200.0)
+
+
+def test_row_splits_keep_leaves_whole():
+    # the shard boundaries of the multi-GPU matvec never cut a leaf of the
+    # partition (aca2 route, identity adjacency), checked on the C oracle's
+    # partition of a 1-D and a 2-D tree
+    import sys
+    import numpy as np
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "hmatrix.jl_b200"))
+    from hmatrix.cluster import construct_cluster
+    from hmatrix.shard import row_splits
+    from oracle import hm_oracle_c as O
+    import ctypes as C
+    for G, mb, minb in ((np.linspace(0, 10, 5000), 512, 64),
+                        (np.random.default_rng(5).uniform(0, 1, (3000, 2)), 256, 32)):
+        c = construct_cluster(G, minb, "bisect")
+        s, e, l, r = (np.ascontiguousarray(a, np.int64) for a in (c.s, c.e, c.left, c.right))
+        L = O.lib()
+        n = int(c.e[0])
+        cnt = L.orc_partition(O._p(s), O._p(e), O._p(l), O._p(r), minb, mb, 0, n, 0, C.c_void_p(0))
+        lv = np.zeros((cnt, 5), np.int64)
+        L.orc_partition(O._p(s), O._p(e), O._p(l), O._p(r), minb, mb, 0, n, cnt, O._p(lv))
+        for world in (2, 3, 4, 8):
+            b = row_splits(c, mb, world)
+            assert b[0] == 0 and b[-1] == n and all(b[i] <= b[i + 1] for i in range(world))
+            for t in b[1:-1]:
+                cut = (lv[:, 1] < t) & (lv[:, 1] + lv[:, 3] > t)
+                assert not cut.any()
+            sizes = np.diff(b)
+            assert sizes.max() - sizes.min() <= 2 * mb
+
+
+def _shard_worker(rank, world, port, out):
+    # the reduction that assembles H*x from the shards, over gloo: each rank
+    # contributes its rows of a dense product and zeros elsewhere
+    import datetime
+    import sys
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "hmatrix.jl_b200"))
+    from hmatrix.shard import reduce_rows
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    rng = np.random.default_rng(0)
+    A = rng.standard_normal((40, 40))
+    x = rng.standard_normal(40)
+    b = [0, 17, 40]
+    y = torch.zeros(40, dtype=torch.float64)
+    y[b[rank]:b[rank + 1]] = torch.tensor(A[b[rank]:b[rank + 1]] @ x)
+    reduce_rows(y, dist)
+    out.put((rank, float(np.abs(y.numpy() - A @ x).max())))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_shard_reduction_two_ranks():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, err in res:
+        assert err <= 1e-12
