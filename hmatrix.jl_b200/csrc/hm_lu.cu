@@ -1148,7 +1148,9 @@ struct RcReq {
   int m, n, kcap;
 };
 
-static void recompress_batch(Ctx& c, const std::vector<RcReq>& reqs, int rmax) {
+// size_to_batch: read the largest core size back and launch for it (one host
+// synchronisation); otherwise launch for rmax.
+static void recompress_batch(Ctx& c, const std::vector<RcReq>& reqs, int rmax, bool size_to_batch = true) {
   if (reqs.empty()) return;
   rmax = std::min(std::max(rmax, 1), RCORE_MAX);
   size_t b = 0;
@@ -1188,14 +1190,17 @@ static void recompress_batch(Ctx& c, const std::vector<RcReq>& reqs, int rmax) {
     LU_LAUNCH_CHECK();
     // size the core launch to the largest core of this batch (ranks are on
     // the device: one small read-back per batch)
-    int32_t* dmax = (int32_t*)dmalloc(c, tmp, sizeof(int32_t));
-    lu_max_int_kernel<<<1, 256, 0, c.st>>>(rr, (int)(e - b), dmax);
-    LU_LAUNCH_CHECK();
-    int32_t hmax = 0;
-    if (cudaMemcpyAsync(&hmax, dmax, sizeof(int32_t), cudaMemcpyDeviceToHost, c.st) != cudaSuccess ||
-        cudaStreamSynchronize(c.st) != cudaSuccess)
-      throw LuError(HM_ERR_CUDA, "core size read-back");
-    const int rlaunch = std::min(rmax, std::max(8, (hmax + 7) / 8 * 8));
+    int rlaunch = rmax;
+    if (size_to_batch) {
+      int32_t* dmax = (int32_t*)dmalloc(c, tmp, sizeof(int32_t));
+      lu_max_int_kernel<<<1, 256, 0, c.st>>>(rr, (int)(e - b), dmax);
+      LU_LAUNCH_CHECK();
+      int32_t hmax = 0;
+      if (cudaMemcpyAsync(&hmax, dmax, sizeof(int32_t), cudaMemcpyDeviceToHost, c.st) != cudaSuccess ||
+          cudaStreamSynchronize(c.st) != cudaSuccess)
+        throw LuError(HM_ERR_CUDA, "core size read-back");
+      rlaunch = std::min(rmax, std::max(8, (hmax + 7) / 8 * 8));
+    }
     int s = launch_core_recompress(dc, (int)(e - b), rlaunch, c.eps_trunc, c.flags, c.st);
     if (s != HM_OK) throw LuError(s, "batched recompression launch");
     b = e;
@@ -1207,6 +1212,31 @@ static void recompress_batch(Ctx& c, const std::vector<RcReq>& reqs, int rmax) {
 // into one [A | -Q] [B | B_kj] pair and recompressed (Q_ij = A_ik W_kj, the
 // panel product of step k).  Job q of the batch is pair (ii, jj) of the
 // trailing tiles with the diagonal skipped; its scratch is a fixed stride.
+// Pair q of the trailing update of step k: mode 0 every pair i != j of the
+// tiles (k, T); mode 1 the pairs of tile row and tile column k+1; mode 2 the
+// pairs among the tiles (k+1, T).
+__device__ __forceinline__ void tile_pair(int T, int k, int mode, int64_t gq, int& i, int& j) {
+  if (mode == 1) {
+    const int n1 = T - k - 2;
+    if (gq < n1) { i = k + 1; j = k + 2 + (int)gq; }
+    else { i = k + 2 + (int)(gq - n1); j = k + 1; }
+    return;
+  }
+  const int base = mode == 2 ? k + 2 : k + 1;
+  const int Tr = T - base;
+  const int ii = (int)(gq / (Tr - 1));
+  int jj = (int)(gq % (Tr - 1));
+  if (jj >= ii) ++jj;
+  i = base + ii;
+  j = base + jj;
+}
+static int64_t tile_pair_count(int T, int k, int mode) {
+  const int64_t Tr = T - k - 1;
+  if (mode == 0) return Tr * (Tr - 1);
+  if (mode == 1) return Tr >= 2 ? 2 * (Tr - 1) : 0;
+  return Tr >= 2 ? (Tr - 1) * (Tr - 2) : 0;
+}
+
 struct TileJobArgs {
   const double* const* Ap;
   const double* const* Bp;
@@ -1222,15 +1252,13 @@ struct TileJobArgs {
   int* flags;
   CoreJob* cj;
   int64_t q0;                // first job of this batch
+  int mode;                  // which pairs (tile_pair)
 };
 __global__ void __launch_bounds__(256) lu_tile_gather_kernel(TileJobArgs a) {
   const int64_t q = blockIdx.x;
   const int64_t gq = a.q0 + q;
-  const int Tr = a.T - a.k - 1;
-  const int ii = (int)(gq / (Tr - 1));
-  int jj = (int)(gq % (Tr - 1));
-  if (jj >= ii) ++jj;
-  const int i = a.k + 1 + ii, j = a.k + 1 + jj;
+  int i, j;
+  tile_pair(a.T, a.k, a.mode, gq, i, j);
   const int mi = a.size[i], nj = a.size[j];
   const double* Qi = a.qbase + (a.start[i] - a.start[a.k + 1]) * a.R;
   double* Aij = const_cast<double*>(a.Ap[i]) + (int64_t)j * a.cap * mi;
@@ -1406,11 +1434,8 @@ static bool tile_structure(const hm_handle* h, std::vector<int32_t>& gcl, std::v
 __global__ void __launch_bounds__(128) lu_tile_core_kernel(TileJobArgs a, int rl, int smax, double eps_trunc) {
   extern __shared__ double sm[];
   const int64_t gq = a.q0 + blockIdx.x;
-  const int Tr = a.T - a.k - 1;
-  const int ii = (int)(gq / (Tr - 1));
-  int jj = (int)(gq % (Tr - 1));
-  if (jj >= ii) ++jj;
-  const int i = a.k + 1 + ii, j = a.k + 1 + jj;
+  int i, j;
+  tile_pair(a.T, a.k, a.mode, gq, i, j);
   const int mi = a.size[i], nj = a.size[j];
   const double* Qij = a.qbase + (a.start[i] - a.start[a.k + 1]) * a.R + (int64_t)(j - a.k - 1) * a.cap * mi;
   double* Aij = const_cast<double*>(a.Ap[i]) + (int64_t)j * a.cap * mi;
@@ -1472,9 +1497,25 @@ __global__ void lu_tile_rank_bound_kernel(const int32_t* __restrict__ kmat, int 
   if (threadIdx.x == 0) *out = a1 + red[0];
 }
 
-static void recompress_tile_pairs(Ctx& c, const TileLU& TL, int k, int64_t R, const double* qbase, int rmax) {
-  const int T = TL.T, Tr = T - k - 1;
-  const int64_t njobs = (int64_t)Tr * (Tr - 1);
+// the launch size of step k's recompression cores: a bound of rank(A_ij) +
+// rank(B_kj) over its pairs, read back once per step
+static int tile_rank_bound(Ctx& c, const TileLU& TL, int k, int rmax) {
+  Blk tmp;
+  tmp.st = c.st;
+  int32_t* dmax = (int32_t*)dmalloc(c, tmp, sizeof(int32_t));
+  lu_tile_rank_bound_kernel<<<1, 256, 0, c.st>>>(TL.kmat, TL.T, k, dmax);
+  LU_LAUNCH_CHECK();
+  int32_t hb = 0;
+  if (cudaMemcpyAsync(&hb, dmax, sizeof(int32_t), cudaMemcpyDeviceToHost, c.st) != cudaSuccess ||
+      cudaStreamSynchronize(c.st) != cudaSuccess)
+    throw LuError(HM_ERR_CUDA, "rank bound read-back");
+  return std::min(std::min(std::max(rmax, 1), RCORE_MAX), std::max(8, (hb + 7) / 8 * 8));
+}
+
+static void recompress_tile_pairs(Ctx& c, const TileLU& TL, int k, int64_t R, const double* qbase, int rmax,
+                                  int mode, int rl) {
+  const int T = TL.T;
+  const int64_t njobs = tile_pair_count(T, k, mode);
   if (njobs <= 0) return;
   rmax = std::min(std::max(rmax, 1), RCORE_MAX);
   int64_t smax = 1;
@@ -1482,15 +1523,7 @@ static void recompress_tile_pairs(Ctx& c, const TileLU& TL, int k, int64_t R, co
   Blk tmp;
   tmp.st = c.st;
   {
-    // fused path: one rank bound per step, the pairs' factors staged in shared memory
-    int32_t* dmax = (int32_t*)dmalloc(c, tmp, sizeof(int32_t));
-    lu_tile_rank_bound_kernel<<<1, 256, 0, c.st>>>(TL.kmat, T, k, dmax);
-    LU_LAUNCH_CHECK();
-    int32_t hb = 0;
-    if (cudaMemcpyAsync(&hb, dmax, sizeof(int32_t), cudaMemcpyDeviceToHost, c.st) != cudaSuccess ||
-        cudaStreamSynchronize(c.st) != cudaSuccess)
-      throw LuError(HM_ERR_CUDA, "rank bound read-back");
-    const int rl = std::min(rmax, std::max(8, (hb + 7) / 8 * 8));
+    // fused path: the pairs' factors staged in shared memory
     const size_t smem = sizeof(double) * ((size_t)3 * rl * rl + (size_t)2 * smax * rl);
     if (smem <= 200 * 1024) {
       if (smem_attr((const void*)lu_tile_core_kernel, 200 * 1024) != cudaSuccess)
@@ -1498,7 +1531,7 @@ static void recompress_tile_pairs(Ctx& c, const TileLU& TL, int k, int64_t R, co
       for (int64_t q0 = 0; q0 < njobs; q0 += INT32_MAX) {
         const int64_t nb = std::min<int64_t>(INT32_MAX, njobs - q0);
         TileJobArgs a{TL.d_Ap, TL.d_Bp, TL.d_start, TL.d_size, TL.kmat, T, c.cap, k, rmax, R, qbase, nullptr, 0,
-                      nullptr, c.flags, nullptr, q0};
+                      nullptr, c.flags, nullptr, q0, mode};
         lu_tile_core_kernel<<<(unsigned)nb, 128, smem, c.st>>>(a, rl, (int)smax, c.eps_trunc);
         LU_LAUNCH_CHECK();
       }
@@ -1515,7 +1548,7 @@ static void recompress_tile_pairs(Ctx& c, const TileLU& TL, int k, int64_t R, co
   for (int64_t q0 = 0; q0 < njobs; q0 += per) {
     const int64_t nb = std::min(per, njobs - q0);
     TileJobArgs a{TL.d_Ap, TL.d_Bp, TL.d_start, TL.d_size, TL.kmat, T, c.cap, k, rmax, R, qbase, scratch, stride,
-                  rr, c.flags, cj, q0};
+                  rr, c.flags, cj, q0, mode};
     lu_tile_gather_kernel<<<(unsigned)nb, 256, 0, c.st>>>(a);
     LU_LAUNCH_CHECK();
     lu_max_int_kernel<<<1, 256, 0, c.st>>>(rr, (int)nb, dmax);
@@ -1530,8 +1563,17 @@ static void recompress_tile_pairs(Ctx& c, const TileLU& TL, int k, int64_t R, co
   }
 }
 
+// Step k's products for the trailing update, kept until the update has run:
+// W = B_ik' A_kj for the whole panels and Q_i = A_ik W for every trailing tile
+// row (freed on the main stream).
+struct StepQ {
+  std::shared_ptr<Blk> hold;
+  double* qbase = nullptr;
+  std::vector<double*> Q;
+};
+
 static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vector<int32_t>& gcl,
-                        const std::vector<int32_t>& dnode) {
+                        const std::vector<int32_t>& dnode, cudaStream_t look, cublasHandle_t look_blas) {
   const int T = (int)gcl.size(), cap = c.cap;
   TL.T = T;
   TL.start.resize(T);
@@ -1597,79 +1639,125 @@ static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vecto
   for (int i = 0; i < T; ++i) TL.diag[i] = build_tree(c, h, dnode[i], ld);
   ld.flush(c);
 
-  for (int k = 0; k < T; ++k) {
+  // Step k: the diagonal tile's LU and the panels (x: the stream they run on),
+  // then the trailing update.  With a look-ahead stream, the LU and panels of
+  // tile k+1 run there as soon as step k has updated tile row and column k+1,
+  // overlapping the rest of step k's update on the main stream.
+  auto panels = [&](Ctx& x, int k, StepQ& out) {
     const int mk = (int)TL.size[k];
     const int R = (T - k - 1) * cap;
-    lu_rec(c, *TL.diag[k]);
-    if (k > 0) laswp(c, View{TL.Ap[k], 1, mk, mk, k * cap}, TL.start[k]);
-    if (R == 0) break;
+    lu_rec(x, *TL.diag[k]);
+    if (k > 0) laswp(x, View{TL.Ap[k], 1, mk, mk, k * cap}, TL.start[k]);
+    if (R == 0) return;
     View Ua{TL.Ai(k, k + 1, cap), 1, mk, mk, R};          // A factors of tiles (k, j>k)
     View Lb{TL.Bj(k + 1, k, cap), 1, mk, mk, R};          // B factors of tiles (i>k, k)
-    laswp(c, Ua, TL.start[k]);
-    mfs(c, *TL.diag[k], Ua, true, true);                  // L_kk^{-1} P_k A_kj
-    mfs(c, *TL.diag[k], vtr(Lb), false, false);           // B_ik' U_kk^{-1}
-    Blk tmp;
-    tmp.st = c.st;
-    double* W = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)R * R);
+    laswp(x, Ua, TL.start[k]);
+    mfs(x, *TL.diag[k], Ua, true, true);                  // L_kk^{-1} P_k A_kj
+    mfs(x, *TL.diag[k], vtr(Lb), false, false);           // B_ik' U_kk^{-1}
+    out.hold = std::make_shared<Blk>();
+    out.hold->st = c.st;                                  // freed after the main stream used it
+    Blk& hold = *out.hold;
+    double* W = (double*)dmalloc(x, hold, sizeof(double) * (size_t)R * R);
     View Wv{W, 1, R, R, R};
-    gemm(c, Wv, vtr(Lb), Ua, 1.0, 0.0);                   // W_ij = B_ik' A_kj
+    gemm(x, Wv, vtr(Lb), Ua, 1.0, 0.0);                   // W_ij = B_ik' A_kj
     // Q_i = A_ik W_i,:   (m_i x R) for every trailing tile row i
-    std::vector<double*> Q(T, nullptr);
-    {
-      int64_t qtot = 0;
-      for (int i = k + 1; i < T; ++i) qtot += TL.size[i] * (int64_t)R;
-      double* qbase = (double*)dmalloc(c, tmp, sizeof(double) * (size_t)qtot);
-      int64_t qo = 0;
-      for (int i = k + 1; i < T; ++i) { Q[i] = qbase + qo; qo += TL.size[i] * (int64_t)R; }
-      // tiles of equal height: one batched cuBLAS product per height
-      std::map<int, std::vector<int>> by_m;
-      for (int i = k + 1; i < T; ++i) by_m[(int)TL.size[i]].push_back(i);
-      std::vector<GemmJob> gq;
-      for (auto& kv : by_m) {
-        const int mi = kv.first;
-        const std::vector<int>& rows = kv.second;
-        if (c.blas && (double)mi * R * cap * rows.size() >= 4.0e6) {
-          std::vector<const double*> pa, pb;
-          std::vector<double*> pc;
-          for (int i : rows) {
-            pa.push_back(TL.Ai(i, k, cap));
-            pb.push_back(W + (int64_t)(i - k - 1) * cap);
-            pc.push_back(Q[i]);
-          }
-          const double** da = (const double**)dmalloc(c, tmp, sizeof(void*) * rows.size());
-          const double** db = (const double**)dmalloc(c, tmp, sizeof(void*) * rows.size());
-          double** dc = (double**)dmalloc(c, tmp, sizeof(void*) * rows.size());
-          if (cudaMemcpyAsync(da, pa.data(), sizeof(void*) * rows.size(), cudaMemcpyHostToDevice, c.st) ||
-              cudaMemcpyAsync(db, pb.data(), sizeof(void*) * rows.size(), cudaMemcpyHostToDevice, c.st) ||
-              cudaMemcpyAsync(dc, pc.data(), sizeof(void*) * rows.size(), cudaMemcpyHostToDevice, c.st))
-            throw LuError(HM_ERR_CUDA, "pointer upload");
-          const double one = 1.0, zero = 0.0;
-          if (cublasDgemmBatched(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, mi, R, cap, &one, da, mi, db, R, &zero, dc, mi,
-                                 (int)rows.size()) != CUBLAS_STATUS_SUCCESS)
-            throw LuError(HM_ERR_CUDA, "cublasDgemmBatched");
-        } else {
-          for (int i : rows) {
-            GemmJob g{};
-            g.A = View{TL.Ai(i, k, cap), 1, mi, mi, cap};
-            g.B = vsub(Wv, (i - k - 1) * cap, 0, cap, R);
-            g.C = View{Q[i], 1, mi, mi, R};
-            g.alpha = 1.0; g.beta = 0.0;
-            gq.push_back(g);
-          }
+    std::vector<double*>& Q = out.Q;
+    Q.assign(T, nullptr);
+    int64_t qtot = 0;
+    for (int i = k + 1; i < T; ++i) qtot += TL.size[i] * (int64_t)R;
+    out.qbase = (double*)dmalloc(x, hold, sizeof(double) * (size_t)qtot);
+    int64_t qo = 0;
+    for (int i = k + 1; i < T; ++i) { Q[i] = out.qbase + qo; qo += TL.size[i] * (int64_t)R; }
+    // tiles of equal height: one batched cuBLAS product per height
+    std::map<int, std::vector<int>> by_m;
+    for (int i = k + 1; i < T; ++i) by_m[(int)TL.size[i]].push_back(i);
+    std::vector<GemmJob> gq;
+    for (auto& kv : by_m) {
+      const int mi = kv.first;
+      const std::vector<int>& rows = kv.second;
+      if (x.blas && (double)mi * R * cap * rows.size() >= 4.0e6) {
+        std::vector<const double*> pa, pb;
+        std::vector<double*> pc;
+        for (int i : rows) {
+          pa.push_back(TL.Ai(i, k, cap));
+          pb.push_back(W + (int64_t)(i - k - 1) * cap);
+          pc.push_back(Q[i]);
+        }
+        const double** da = (const double**)dmalloc(x, hold, sizeof(void*) * rows.size());
+        const double** db = (const double**)dmalloc(x, hold, sizeof(void*) * rows.size());
+        double** dc = (double**)dmalloc(x, hold, sizeof(void*) * rows.size());
+        if (cudaMemcpyAsync(da, pa.data(), sizeof(void*) * rows.size(), cudaMemcpyHostToDevice, x.st) ||
+            cudaMemcpyAsync(db, pb.data(), sizeof(void*) * rows.size(), cudaMemcpyHostToDevice, x.st) ||
+            cudaMemcpyAsync(dc, pc.data(), sizeof(void*) * rows.size(), cudaMemcpyHostToDevice, x.st))
+          throw LuError(HM_ERR_CUDA, "pointer upload");
+        const double one = 1.0, zero = 0.0;
+        if (cublasDgemmBatched(x.blas, CUBLAS_OP_N, CUBLAS_OP_N, mi, R, cap, &one, da, mi, db, R, &zero, dc, mi,
+                               (int)rows.size()) != CUBLAS_STATUS_SUCCESS)
+          throw LuError(HM_ERR_CUDA, "cublasDgemmBatched");
+      } else {
+        for (int i : rows) {
+          GemmJob g{};
+          g.A = View{TL.Ai(i, k, cap), 1, mi, mi, cap};
+          g.B = vsub(Wv, (i - k - 1) * cap, 0, cap, R);
+          g.C = View{Q[i], 1, mi, mi, R};
+          g.alpha = 1.0; g.beta = 0.0;
+          gq.push_back(g);
         }
       }
-      gemm_batch(c, gq);
     }
+    gemm_batch(x, gq);
+  };
+  // updates of the trailing diagonal tiles i in [i0, i1) (H-structured targets)
+  auto diag_updates = [&](int k, const StepQ& sq, int i0, int i1) {
     std::vector<RcReq> rj;
     std::vector<GemmJob> gd;
-    for (int i = k + 1; i < T; ++i) {                      // diagonal tiles: H-structured targets
+    for (int i = i0; i < i1; ++i) {
       const int mi = (int)TL.size[i];
-      const double* Qii = Q[i] + (int64_t)(i - k - 1) * cap * mi;
+      const double* Qii = sq.Q[i] + (int64_t)(i - k - 1) * cap * mi;
       tile_add_lowrank(*TL.diag[i], 0, 0, Qii, mi, TL.Bj(k, i, cap), mi, TL.kmat + k * T + i, cap, -1.0, gd, rj);
     }
     gemm_batch(c, gd);
-    recompress_batch(c, rj, 2 * cap);                      // low-rank leaves of the diagonal tiles
-    recompress_tile_pairs(c, TL, k, R, Q[k + 1], 2 * cap);  // the off-diagonal tiles
+    recompress_batch(c, rj, 2 * cap, false);              // no read-back: keeps the host ahead
+  };
+  Ctx cl = c;
+  cl.st = look;
+  cl.blas = look_blas;
+  cudaEvent_t ev_up = nullptr, ev_dn = nullptr;
+  if (look && (cudaEventCreateWithFlags(&ev_up, cudaEventDisableTiming) != cudaSuccess ||
+               cudaEventCreateWithFlags(&ev_dn, cudaEventDisableTiming) != cudaSuccess))
+    throw LuError(HM_ERR_CUDA, "look-ahead events");
+  struct EvGuard {
+    cudaEvent_t a, b;
+    cudaStream_t s;
+    ~EvGuard() {
+      if (s) cudaStreamSynchronize(s);
+      if (a) cudaEventDestroy(a);
+      if (b) cudaEventDestroy(b);
+    }
+  } evg{ev_up, ev_dn, look};
+  StepQ cur;
+  panels(c, 0, cur);
+  for (int k = 0; k < T; ++k) {
+    const int R = (T - k - 1) * cap;
+    if (R == 0) break;
+    const int rl = tile_rank_bound(c, TL, k, 2 * cap);
+    StepQ next;
+    if (look) {
+      diag_updates(k, cur, k + 1, k + 2);
+      recompress_tile_pairs(c, TL, k, R, cur.qbase, 2 * cap, 1, rl);   // tile row and column k+1
+      if (cudaEventRecord(ev_up, c.st) != cudaSuccess || cudaStreamWaitEvent(look, ev_up, 0) != cudaSuccess)
+        throw LuError(HM_ERR_CUDA, "look-ahead wait");
+      panels(cl, k + 1, next);
+      if (cudaEventRecord(ev_dn, look) != cudaSuccess) throw LuError(HM_ERR_CUDA, "look-ahead record");
+      recompress_tile_pairs(c, TL, k, R, cur.qbase, 2 * cap, 2, rl);   // the rest
+      diag_updates(k, cur, k + 2, T);
+      if (cudaStreamWaitEvent(c.st, ev_dn, 0) != cudaSuccess) throw LuError(HM_ERR_CUDA, "look-ahead join");
+    } else {
+      diag_updates(k, cur, k + 1, T);
+      recompress_tile_pairs(c, TL, k, R, cur.qbase, 2 * cap, 0, rl);
+      panels(c, k + 1, next);
+    }
+    cur = std::move(next);
   }
 }
 
@@ -2125,17 +2213,53 @@ struct LuState {
   cudaStream_t st = nullptr;
   cublasHandle_t blas = nullptr;
   void* blas_ws = nullptr;
+  // look-ahead stream of the tile schedule and its cuBLAS handle (blocks made
+  // there keep it as their stream, so it lives as long as the factors)
+  cudaStream_t look = nullptr;
+  cublasHandle_t look_blas = nullptr;
+  void* look_ws = nullptr;
   std::vector<std::unique_ptr<SolvePlan>> plans;
   ~LuState() {
     if (!plans.empty()) cudaDeviceSynchronize();
     plans.clear();
+    if (look) cudaStreamSynchronize(look);
     root.reset();
     tile.reset();
     if (P) cudaFreeAsync(P, st);
     if (flags) cudaFreeAsync(flags, st);
     if (st) cudaStreamSynchronize(st);
+    if (look) {
+      cudaStreamSynchronize(look);
+      cudaStreamDestroy(look);
+    }
     if (blas) cublasDestroy(blas);
     if (blas_ws) cudaFree(blas_ws);
+    if (look_blas) cublasDestroy(look_blas);
+    if (look_ws) cudaFree(look_ws);
+  }
+  // a second stream with its own cuBLAS handle and workspace (nullptr if
+  // either cannot be made: the schedule then runs on one stream)
+  void make_look() {
+    if (look) return;
+    // high priority: its small kernels are scheduled between the blocks of the
+    // main stream's large recompression launches instead of after them
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (cudaStreamCreateWithPriority(&look, cudaStreamNonBlocking, greatest) != cudaSuccess) {
+      cudaGetLastError();
+      look = nullptr;
+      return;
+    }
+    if (cublasCreate(&look_blas) != CUBLAS_STATUS_SUCCESS) {
+      look_blas = nullptr;
+      return;
+    }
+    if (cudaMalloc(&look_ws, BLAS_WS) != cudaSuccess) {
+      cudaGetLastError();
+      look_ws = nullptr;
+    }
+    cublasSetStream(look_blas, look);
+    if (look_ws) cublasSetWorkspace(look_blas, look_ws, BLAS_WS);
   }
   // cuBLAS on stream s (created on first use).  The handle gets a fixed
   // workspace so that a captured product allocates nothing; cublasSetStream
@@ -2233,7 +2357,8 @@ int lu_factor(hm_handle* h) {
     if (mode == 2 && !tiled) throw LuError(HM_ERR_UNSUPPORTED, "the partition has no tile level");
     if (tiled) {
       S->tile.reset(new TileLU());
-      tile_factor(c, h, *S->tile, gcl, dnode);
+      S->make_look();
+      tile_factor(c, h, *S->tile, gcl, dnode, S->look_blas ? S->look : nullptr, S->look_blas);
     } else {
       S->root = build_from_handle(c, h, 0);
       lu_rec(c, *S->root);
