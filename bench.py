@@ -410,16 +410,21 @@ def batched_problems(count, seed=3, nmin=2 ** 10, nmax=2 ** 16):
     return out
 
 
-def batch_leg(count, torch, nthreads=0, budget_gb=90.0):
+def batch_leg(count, torch, nthreads=0, budget_gb=90.0, rank=0, world=1, dist=None):
     """All problems factored (lu!) and solved with FP64 refinement to a
     relative residual <= 1e-10 through the batched entry points, in waves
     whose factor memory (about 2.5 n^2 bytes a problem) fits the budget.
     Timed: factorisation + refined solve of every problem (host right-hand
-    sides in, solutions out); construction is not timed."""
+    sides in, solutions out); construction is not timed.  With world > 1 the
+    problems are split over the ranks by predicted cost (no exchange between
+    ranks); the job time is the max over ranks."""
     import hmatrix as hm
+    from hmatrix.shard import problem_cost, split_problems
     probs = batched_problems(count)
+    mine = split_problems([problem_cost(len(p[0]), 256) for p in probs], world)[rank]
     waves, cur, acc = [], [], 0.0
-    for i, (x, _, _) in enumerate(probs):
+    for i in mine:
+        x = probs[i][0]
         need = 2.5 * len(x) ** 2 / 1e9
         if cur and acc + need > budget_gb:
             waves.append(cur)
@@ -432,9 +437,13 @@ def batch_leg(count, torch, nthreads=0, budget_gb=90.0):
                       "n_range": [int(min(len(p[0]) for p in probs)), int(max(len(p[0]) for p in probs))],
                       "kernel": "1/(1+((x-y)/l)^2) + delta_xy", "MaxBlock": 256, "MinBlock": 32, "MaxRank": 12,
                       "aca_tol": 1e-10, "target_relres": 1e-10, "tree": "median bisection", "waves": len(waves),
-                      "host_threads": nthreads or "auto"}}
+                      "host_threads": nthreads or "auto",
+                      "split": ("%d ranks by predicted cost, no exchange" % world) if world > 1 else "1 GPU"}}
+    dev = "cuda" if dist is not None and dist.get_backend() == "nccl" else "cpu"
     for name, epslu in (("fp64", 0.0), ("mixed", 1e-6)):
         t_all, worst, steps = 0.0, 0.0, 0
+        if dist is not None:
+            dist.barrier()
         for w in waves:
             Hs, ys = [], []
             for i in w:
@@ -453,6 +462,9 @@ def batch_leg(count, torch, nthreads=0, budget_gb=90.0):
             steps = max(steps, int(it.max()))
             del Hs, xs
             torch.cuda.empty_cache()
+        t_all = job_time(t_all * 1e3, dist, dev) * 1e-3
+        worst = job_time(worst, dist, dev)              # max over ranks
+        steps = int(job_time(float(steps), dist, dev))
         out[name] = {"total_s": t_all, "max_relres": worst, "max_refine_steps": steps,
                      "eps_trunc_lu": epslu or 1e-10}
     out["mixed_speedup"] = out["fp64"]["total_s"] / out["mixed"]["total_s"]
@@ -528,10 +540,10 @@ def run_ours(a):
         torch.cuda.empty_cache()
         lu = lu_solve_leg(a.lu_n, torch)
     batch = None
-    if a.batch > 0 and world == 1:
+    if a.batch > 0:
         H = None
         torch.cuda.empty_cache()
-        batch = batch_leg(a.batch, torch, a.batch_nthreads)
+        batch = batch_leg(a.batch, torch, a.batch_nthreads, rank=rank, world=world, dist=dist)
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()

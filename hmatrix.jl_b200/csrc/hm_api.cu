@@ -56,8 +56,10 @@ int check_params(const hm_params* p) {
     return fail(HM_ERR_ARG, "kernel parameter must be > 0");
   if (p->max_rank < 1 || p->max_rank > 64) return fail(HM_ERR_ARG, "MaxRank must be in [1, 64]");
   if (p->min_block < 1) return fail(HM_ERR_ARG, "MinBlock must be >= 1");
-  if (p->cons_method != HM_CONS_ACA2 && p->cons_method != HM_CONS_SVD)
-    return fail(HM_ERR_ARG, "ConsMethod must be aca2 or svd (bbfmm/separate are not on this path)");
+  if (p->cons_method != HM_CONS_ACA2 && p->cons_method != HM_CONS_SVD && p->cons_method != HM_CONS_BBFMM)
+    return fail(HM_ERR_ARG, "ConsMethod must be aca2, svd or bbfmm (separate needs user closures)");
+  if (p->cons_method == HM_CONS_BBFMM && p->dim > 2)
+    return fail(HM_ERR_UNSUPPORTED, "bbfmm construction takes 1-D or 2-D geometry (deps/src/lowrank.cpp:186-222)");
   if (p->storage != HM_F64 && p->storage != HM_F32 && p->storage != HM_BF16)
     return fail(HM_ERR_ARG, "storage must be HM_F64, HM_F32 or HM_BF16");
   if (!(p->eps_trunc >= 0.0) || !(p->eps_comp >= 0.0)) return fail(HM_ERR_ARG, "tolerances must be >= 0");

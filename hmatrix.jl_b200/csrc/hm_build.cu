@@ -96,7 +96,8 @@ int classify(const hm_handle* h, const NbSet& nb, int32_t s, int32_t t) {
     return T_DENSE;
   if (m > p.max_block || n > p.max_block) return T_H;
   if (h->cl_s[s] == h->cl_s[t] && h->cl_e[s] == h->cl_e[t]) return T_H;  // s == t
-  if (p.cons_method == HM_CONS_ACA2) return nb.neighbours(h, s, t) ? T_H : T_RK;
+  // aca2 and bbfmm: admissible iff not neighbours (cluster.jl:68-75, 86-97)
+  if (p.cons_method == HM_CONS_ACA2 || p.cons_method == HM_CONS_BBFMM) return nb.neighbours(h, s, t) ? T_H : T_RK;
   return -1;
 }
 
@@ -259,6 +260,9 @@ int build_handle(hm_handle* h, const double* geom, int64_t ncl, const int64_t* c
     std::vector<int32_t> ranks;
     HM_TRY(aca2_ranks(h, rk_leaf, ranks));
     for (size_t i = 0; i < rk_leaf.size(); ++i) h->leaves[rk_leaf[i]].k = ranks[i];
+  } else if (p.cons_method == HM_CONS_BBFMM) {
+    for (int64_t li : rk_leaf)
+      h->leaves[li].k = bbfmm_rank(h->leaves[li].m, h->leaves[li].n, (int)h->dim, p.max_rank);
   } else {
     for (int64_t li : rk_leaf) {
       int32_t node = h->leaves[li].node;
@@ -295,6 +299,8 @@ int build_handle(hm_handle* h, const double* geom, int64_t ncl, const int64_t* c
   }
   if (p.cons_method == HM_CONS_ACA2) {
     HM_TRY(aca2_write(h, rk_leaf));
+  } else if (p.cons_method == HM_CONS_BBFMM) {
+    HM_TRY(bbfmm_write(h, rk_leaf));
   } else {
     HM_TRY(svd_store.write_pool(h, rk_leaf));
   }

@@ -49,21 +49,21 @@ struct KernelDesc {
 // Geometry is column-major n x dim.  The arithmetic order matches the FP64
 // oracle exactly (no FMA contraction), so rational kernels are bit-identical
 // to the CPU restatement of kernel_full (src/cluster.jl:258-275).
-__device__ __forceinline__ double kernel_eval(const KernelDesc& kd,
-                                              const double* __restrict__ geom,
-                                              int64_t n, int64_t i, int64_t j) {
+// kernel_eval_xy: k(x, y) for points whose coordinate q is x[q * sx], y[q * sy].
+__device__ __forceinline__ double kernel_eval_xy(const KernelDesc& kd, const double* __restrict__ x,
+                                                 int64_t sx, const double* __restrict__ y, int64_t sy) {
   double s = 0.0;
   if ((kd.kind == HM_KERNEL_CAUCHY && kd.p != 1.0) || kd.kind == HM_KERNEL_CAUCHY_DP) {
 #pragma unroll 3
     for (int q = 0; q < kd.dim; ++q) {
-      double d = __ddiv_rn(__dsub_rn(geom[i + q * n], geom[j + q * n]), kd.p);
+      double d = __ddiv_rn(__dsub_rn(x[q * sx], y[q * sy]), kd.p);
       double t = __dmul_rn(d, d);
       s = (q == 0) ? t : __dadd_rn(s, t);
     }
   } else {
 #pragma unroll 3
     for (int q = 0; q < kd.dim; ++q) {
-      double d = __dsub_rn(geom[i + q * n], geom[j + q * n]);
+      double d = __dsub_rn(x[q * sx], y[q * sy]);
       double t = __dmul_rn(d, d);
       s = (q == 0) ? t : __dadd_rn(s, t);
     }
@@ -86,6 +86,12 @@ __device__ __forceinline__ double kernel_eval(const KernelDesc& kd,
     v = __ddiv_rn(1.0, __dadd_rn(1.0, s));
   }
   return v;
+}
+
+__device__ __forceinline__ double kernel_eval(const KernelDesc& kd,
+                                              const double* __restrict__ geom,
+                                              int64_t n, int64_t i, int64_t j) {
+  return kernel_eval_xy(kd, geom + i, n, geom + j, n);
 }
 
 // ---------------------------------------------------------------------------

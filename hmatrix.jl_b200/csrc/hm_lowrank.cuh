@@ -69,6 +69,10 @@ int svd_compress_candidates(hm_handle* h, const std::vector<int64_t>& r0,
                             SvdCandidateStore& store, const std::vector<int32_t>& nodes);
 int aca2_ranks(hm_handle* h, const std::vector<int64_t>& rk_leaf, std::vector<int32_t>& ranks);
 int aca2_write(hm_handle* h, const std::vector<int64_t>& rk_leaf);
+// Chebyshev-interpolation ("bbfmm") leaves: the rank of an m x n leaf, and
+// the factors of every low-rank leaf written into the pool
+int bbfmm_rank(int64_t m, int64_t n, int dim, int max_rank);
+int bbfmm_write(hm_handle* h, const std::vector<int64_t>& rk_leaf);
 
 // One recompression problem for the batched QR+SVD core kernel.  A (m x r,
 // column stride lda) and B (n x r, stride ldb) are FP64 device buffers that

@@ -91,8 +91,10 @@ def _params_struct(prm: Params, dim: int):
         p.cons_method = _lib.HM_CONS_ACA2
     elif prm.ConsMethod == "svd":
         p.cons_method = _lib.HM_CONS_SVD
+    elif prm.ConsMethod == "bbfmm":
+        p.cons_method = _lib.HM_CONS_BBFMM
     else:
-        raise HmError(_lib.HM_ERR_ARG, "ConsMethod %r is not on the device path (use 'aca2' or 'svd')"
+        raise HmError(_lib.HM_ERR_ARG, "ConsMethod %r is not on the device path (use 'aca2', 'svd' or 'bbfmm')"
                       % prm.ConsMethod)
     if prm.CompMethod != "svd":
         raise HmError(_lib.HM_ERR_ARG, "CompMethod %r: only 'svd' works in the reference" % prm.CompMethod)

@@ -17,7 +17,7 @@ HM_ERR_ARG, HM_ERR_CUDA, HM_ERR_OOM, HM_ERR_STATE = 1, 2, 3, 4
 HM_ERR_SINGULAR, HM_ERR_RANK, HM_ERR_NONFINITE, HM_ERR_UNSUPPORTED, HM_ERR_TIMEOUT = 5, 6, 7, 8, 9
 HM_KERNEL_CAUCHY, HM_KERNEL_INVQUAD, HM_KERNEL_GAUSS = 1, 2, 3
 HM_KERNEL_CAUCHY_DP, HM_KERNEL_INVQUAD_DP, HM_KERNEL_GAUSS_DP = 4, 5, 6
-HM_CONS_ACA2, HM_CONS_SVD = 1, 2
+HM_CONS_ACA2, HM_CONS_SVD, HM_CONS_BBFMM = 1, 2, 3
 HM_F64, HM_F32, HM_BF16 = 0, 1, 2
 HM_FLAG_DEVICE_PTRS = 1
 HM_FLAG_TRANS = 2

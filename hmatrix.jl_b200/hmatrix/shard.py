@@ -1,4 +1,5 @@
-"""Row-sharded H-matvec over several GPUs (one process per GPU).
+"""Multi-GPU work split (one process per GPU): row-sharded H-matvec, and
+independent problems of a batch spread over the ranks.
 
 Every rank builds the same cluster tree (deterministic), owns a contiguous
 range of rows and builds only the leaves of those rows (``Params.RowRange``):
@@ -72,3 +73,28 @@ class ShardedHmat:
     def matvec(self, x, dist=None, group=None):
         """H*x on every rank (x: the full vector, a CUDA float64 tensor)."""
         return reduce_rows(self.H.matvec(x), dist, group)
+
+
+def problem_cost(n, max_block):
+    """Predicted relative cost of ``lu!`` + refined solve of one problem of n
+    points whose tile level has T = ceil(n / max_block) tiles: the right-looking
+    tile elimination recompresses about T^3 / 3 off-diagonal tiles, and each of
+    its T steps carries a fixed launch latency worth about 64 tile updates."""
+    T = max(1, -(-int(n) // int(max_block)))
+    return 64.0 * T + T ** 3 / 3.0
+
+
+def split_problems(costs, world):
+    """Independent problems over ``world`` ranks, no exchange between them:
+    longest predicted cost first, each to the rank with the least work so far
+    (ties to the lowest rank).  Returns one sorted index list per rank; every
+    index appears exactly once, and the most loaded rank carries at most the
+    mean load plus the largest single cost."""
+    costs = np.asarray(costs, dtype=np.float64)
+    load = np.zeros(world)
+    out = [[] for _ in range(world)]
+    for i in np.argsort(-costs, kind="stable"):
+        r = int(np.argmin(load))
+        out[r].append(int(i))
+        load[r] += costs[i]
+    return [sorted(o) for o in out]

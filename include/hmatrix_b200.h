@@ -52,6 +52,8 @@ extern "C" {
 /* ---- construction methods (Hparams.ConsMethod) --------------------------- */
 #define HM_CONS_ACA2       1   /* partially pivoted ACA, src/hlu.jl:59-111    */
 #define HM_CONS_SVD        2   /* dense block + truncated SVD, cluster.jl:99  */
+#define HM_CONS_BBFMM      3   /* Chebyshev interpolation, hlu.jl:20-29,113-132;
+                                  deps/src/lowrank.cpp:186-222 (1-D and 2-D)   */
 
 /* ---- storage precision of the matvec copy of the factors ----------------- */
 #define HM_F64             0

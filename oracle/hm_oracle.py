@@ -15,6 +15,7 @@ Hmatrix.jl for the hot path, following the reference files line by line
 * dense kernel blocks ``FullMat`` ... src/cluster.jl:45,258-275
 * ``compress`` / ``rank_truncate`` .. src/hlu.jl:144-190
 * ``aca2`` (d-D form) ............... src/hlu.jl:59-111
+* ``bbfmm`` Chebyshev interpolation . src/hlu.jl:20-29,113-132, deps/src/lowrank.cpp:24-222
 * fully pivoted ACA ................. deps/src/ACA_FullyPivoted.cpp:9-236
 * H-matvec .......................... src/harithm.jl:317-371
 * H-add / recompression ............. src/harithm.jl:4-159,374-420
@@ -409,6 +410,77 @@ def aca2(f, X, Y, Rrank, εComp):
     return A, B
 
 
+def chebyshev_points(r, a, b):
+    """``Chebyshev_points(n, a, b)`` / ``Interpolation`` (deps/src/lowrank.cpp:26-44):
+    cos(pi (2i+1) / (2r)) on [-1, 1], mapped as u (b - a) / 2 + (a + b) / 2,
+    with libm's cos and the same operation order."""
+    u = np.array([math.cos(math.pi * (2.0 * i + 1.0) / (2.0 * r)) for i in range(r)])
+    return u * (b - a) / 2.0 + (a + b) / 2.0
+
+
+def lagrange_matrix(X, cheb):
+    """``Interpolation::ComputeMatrix`` (deps/src/lowrank.cpp:48-61):
+    P(i, j) = prod_{k != j} (X_i - c_k) / (c_j - c_k), multiplied in k order."""
+    X = np.asarray(X, dtype=np.float64)
+    r = len(cheb)
+    P = np.ones((len(X), r))
+    for j in range(r):
+        for k in range(r):
+            if k != j:
+                P[:, j] *= (X - cheb[k]) / (cheb[j] - cheb[k])
+    return P
+
+
+def bbfmm1d(f, X, Y, r):
+    """``bbfmm1D`` (deps/src/lowrank.cpp:186-200, src/hlu.jl:113-121):
+    U = P_X S (m x r), V = P_Y (n x r), S_ij = f(cX_i, cY_j), nodes on
+    [min X, max X] and [min Y, max Y]."""
+    X = np.asarray(X, dtype=np.float64).reshape(-1)
+    Y = np.asarray(Y, dtype=np.float64).reshape(-1)
+    cx = chebyshev_points(r, X.min(), X.max())
+    cy = chebyshev_points(r, Y.min(), Y.max())
+    S = f(cx.reshape(-1, 1), cy.reshape(-1, 1))
+    return lagrange_matrix(X, cx) @ S, lagrange_matrix(Y, cy)
+
+
+def _interp_2d(X, r):
+    """``Interpolation_2d`` (deps/src/lowrank.cpp:100-136): nodes (cx_i, cy_j)
+    at row i r + j, and the matrix with column i r + j = Lx_i * Ly_j."""
+    cx = chebyshev_points(r, X[:, 0].min(), X[:, 0].max())
+    cy = chebyshev_points(r, X[:, 1].min(), X[:, 1].max())
+    nodes = np.stack([np.repeat(cx, r), np.tile(cy, r)], axis=1)
+    Lx, Ly = lagrange_matrix(X[:, 0], cx), lagrange_matrix(X[:, 1], cy)
+    P = (Lx[:, :, None] * Ly[:, None, :]).reshape(len(X), r * r)
+    return nodes, P
+
+
+def bbfmm2d(f, X, Y, r):
+    """``bbfmm2D`` / ``Compute_lowrank`` (deps/src/lowrank.cpp:139-222,
+    src/hlu.jl:123-132): U = P_X S (m x r^2), V = P_Y (n x r^2),
+    S(a, b) = f(node a of X, node b of Y)."""
+    X = np.asarray(X, dtype=np.float64).reshape(len(X), 2)
+    Y = np.asarray(Y, dtype=np.float64).reshape(len(Y), 2)
+    nx, PX = _interp_2d(X, r)
+    ny, PY = _interp_2d(Y, r)
+    return PX @ f(nx, ny), PY
+
+
+def bbfmm(f, X, Y, Rrank):
+    """``bbfmm`` (src/hlu.jl:20-29).  1-D geometry takes the ``bbfmm1d``
+    branch (the reference's n x 1 cluster points reach ``bbfmm2d`` and read
+    past the end of X, deps/src/lowrank.cpp:207-208); 2-D lowers Rrank to
+    floor(sqrt(max(m, n))) when Rrank^2 exceeds max(m, n)."""
+    X = np.asarray(X, dtype=np.float64).reshape(len(X), -1)
+    Y = np.asarray(Y, dtype=np.float64).reshape(len(Y), -1)
+    if X.shape[1] == 1:
+        return bbfmm1d(f, X, Y, Rrank)
+    if X.shape[1] != 2:
+        raise NotImplementedError("bbfmm2D reads two coordinates (deps/src/lowrank.cpp:203-211)")
+    if Rrank ** 2 > max(len(X), len(Y)):
+        Rrank = int(math.floor(math.sqrt(max(len(X), len(Y)))))
+    return bbfmm2d(f, X, Y, Rrank)
+
+
 def aca_fully_pivoted(A, epsilon, min_rank=1):
     """deps/src/ACA_FullyPivoted.cpp:9-151 (the ``rank==0`` branch).
 
@@ -505,6 +577,12 @@ def build_hmat(c, prm: Params, nb):
                     H.is_rk, H.is_h = False, True
             else:
                 H.is_h = True
+        elif prm.ConsMethod == "bbfmm":
+            if not nb(s, t):
+                H.is_rk = True
+                U, V = bbfmm(f, s.X, t.X, prm.MaxRank)
+            else:
+                H.is_h = True
         elif prm.ConsMethod == "svd":
             A = FullMat(f, s.X, t.X)
             U, V = compress(A, prm)
@@ -514,7 +592,7 @@ def build_hmat(c, prm: Params, nb):
                 H.is_h = True
         else:
             raise NotImplementedError(
-                "ConsMethod %r is outside the hot path (bbfmm / separate)" % prm.ConsMethod)
+                "ConsMethod %r is outside the hot path (separate needs user closures)" % prm.ConsMethod)
 
         if H.is_full:
             H.C = FullMat(f, s.X, t.X)

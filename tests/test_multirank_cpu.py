@@ -132,3 +132,73 @@ def test_shard_reduction_two_ranks():
         assert p.exitcode == 0
     for rank, err in res:
         assert err <= 1e-12
+
+
+def test_split_problems_cover_and_balance():
+    # the batched uneven problems over 1..8 ranks: every problem on exactly one
+    # rank, the most loaded rank within the LPT bound (mean + largest cost)
+    import sys
+    import numpy as np
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    sys.path.insert(0, os.path.join(root, "hmatrix.jl_b200"))
+    import bench
+    from hmatrix.shard import problem_cost, split_problems
+    probs = bench.batched_problems(256)
+    costs = np.array([problem_cost(len(p[0]), 256) for p in probs])
+    assert problem_cost(256, 256) < problem_cost(257, 256) < problem_cost(65536, 256)
+    for world in (1, 2, 3, 4, 8):
+        parts = split_problems(costs, world)
+        assert len(parts) == world
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(probs)))
+        loads = np.array([costs[p].sum() for p in parts])
+        assert loads.max() <= costs.sum() / world + costs.max() + 1e-9
+        if world > 1:
+            assert loads.max() <= 1.05 * costs.sum() / world
+    # fewer problems than ranks: the extra ranks get none
+    parts = split_problems([5.0, 1.0], 4)
+    assert parts == [[0], [1], [], []]
+
+
+def _batch_worker(rank, world, port, out):
+    # each rank takes its share of the batch with no exchange; only the
+    # counts, the job time (max) and the worst residual (max) are reduced
+    import datetime
+    import sys
+    import torch
+    import torch.distributed as dist
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    sys.path.insert(0, os.path.join(root, "hmatrix.jl_b200"))
+    import bench
+    from hmatrix.shard import problem_cost, split_problems
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    probs = bench.batched_problems(32)
+    mine = split_problems([problem_cost(len(p[0]), 256) for p in probs], world)[rank]
+    cnt = torch.tensor([float(len(mine)), float(sum(len(probs[i][0]) for i in mine))], dtype=torch.float64)
+    dist.all_reduce(cnt)
+    ms = bench.job_time([3.0, 5.0][rank], dist, "cpu")
+    worst = bench.job_time([1e-12, 4e-11][rank], dist, "cpu")
+    out.put((rank, int(cnt[0]), int(cnt[1]), ms, worst, sum(len(p[0]) for p in probs)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_batch_split_two_ranks():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_batch_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, count, sum_n, ms, worst, total_n in res:
+        assert count == 32 and sum_n == total_n
+        assert ms == 5.0 and worst == 4e-11

@@ -118,3 +118,68 @@ def test_golden_fixtures_match_oracle():
     assert np.array_equal(np.asarray(O.block_list(H), np.int64), g["blocks5"])
     y = g["y"]
     assert np.allclose(O.matvec(H, y), g["Hy5"], rtol=1e-13, atol=0)
+
+
+# --- bbfmm (deps/src/lowrank.cpp:24-222, src/hlu.jl:20-29,113-132) ---------
+# The reference's C++ needs Eigen (absent), so the restatement is pinned by
+# the identities Chebyshev interpolation must satisfy.
+
+def test_bbfmm_nodes_and_lagrange_identity():
+    from oracle import hm_oracle as O
+    for r in (1, 2, 5, 16):
+        c = O.chebyshev_points(r, -1.0, 1.0)
+        assert np.allclose(c, np.cos(np.pi * (2 * np.arange(r) + 1) / (2 * r)), rtol=0, atol=1e-15)
+        c = O.chebyshev_points(r, 3.0, 7.0)
+        assert np.all((c > 3.0) & (c < 7.0))
+        # L_j(c_i) = delta_ij exactly: a zero factor off the diagonal, x/x on it
+        assert np.array_equal(O.lagrange_matrix(c, c), np.eye(r))
+
+
+def test_bbfmm_reproduces_polynomials():
+    # a kernel of degree < r in each coordinate is interpolated exactly
+    from oracle import hm_oracle as O
+    rng = np.random.default_rng(0)
+    f1 = lambda X, Y: (1.0 + X[:, 0][:, None] * Y[:, 0][None, :]) ** 3
+    X, Y = np.sort(rng.uniform(0, 1, 70)), np.sort(rng.uniform(2, 3, 50))
+    U, V = O.bbfmm(f1, X, Y, 4)
+    assert U.shape == (70, 4) and V.shape == (50, 4)
+    A = f1(X.reshape(-1, 1), Y.reshape(-1, 1))
+    assert np.abs(U @ V.T - A).max() <= 1e-12 * np.abs(A).max()
+    f2 = lambda X, Y: (1.0 + X @ Y.T) ** 2
+    X2, Y2 = rng.uniform(0, 1, (90, 2)), rng.uniform(2, 3, (80, 2))
+    U, V = O.bbfmm(f2, X2, Y2, 3)
+    assert U.shape == (90, 9) and V.shape == (80, 9)
+    A = f2(X2, Y2)
+    assert np.abs(U @ V.T - A).max() <= 1e-12 * np.abs(A).max()
+
+
+def test_bbfmm_converges_and_rank_rule():
+    from oracle import hm_oracle as O
+    rng = np.random.default_rng(1)
+    f = O.kernel_cauchy()
+    X, Y = np.sort(rng.uniform(0, 1, 64)), np.sort(rng.uniform(3, 4, 64))
+    A = f(X.reshape(-1, 1), Y.reshape(-1, 1))
+    errs = []
+    for r in (2, 4, 8, 12):
+        U, V = O.bbfmm(f, X, Y, r)
+        errs.append(np.abs(U @ V.T - A).max() / np.abs(A).max())
+    assert all(errs[i + 1] < errs[i] for i in range(3)) and errs[-1] < 1e-9
+    # 2-D: r lowered to floor(sqrt(max(m, n))) when r^2 > max(m, n) (hlu.jl:24-26)
+    X2, Y2 = rng.uniform(0, 1, (40, 2)), rng.uniform(3, 4, (30, 2))
+    U, V = O.bbfmm(f, X2, Y2, 16)
+    assert U.shape == (40, 36) and V.shape == (30, 36)        # floor(sqrt(40)) = 6
+    U, V = O.bbfmm(f, X2, Y2, 5)
+    assert U.shape == (40, 25)
+
+
+def test_bbfmm_newhmat_2d_accuracy():
+    # test/cluster.jl:9's bar on the bbfmm route (its default ConsMethod) in 2-D
+    from oracle import hm_oracle as O
+    G = np.random.default_rng(2).uniform(0, 1, (1200, 2))
+    prm = O.Params(Geom=G, Kernel=O.kernel_invquad(100.0), MaxBlock=300, MinBlock=32, MaxRank=6,
+                   ConsMethod="bbfmm", Tree="bisect")
+    c, H = O.NewHmat(prm)
+    A = O.FullMat(prm.Kernel, c.X, c.X)
+    lv = np.asarray(O.block_list(H))
+    assert (lv[:, 0] == 1).any()
+    assert np.abs(O.to_fmat(H) - A).max() < 1e-8
