@@ -85,8 +85,11 @@ __global__ void xcopy_kernel(const double* __restrict__ x, int64_t n, TX* __rest
 // ---------------------------------------------------------------------------
 // phase 1: z = F1' x_seg, one warp per low-rank leaf
 // ---------------------------------------------------------------------------
+#ifndef HM_P1_MINB
+#define HM_P1_MINB 1
+#endif
 template <typename T>
-__global__ void __launch_bounds__(256) mv_phase1_kernel(const P1Desc* __restrict__ d, int64_t nd,
+__global__ void __launch_bounds__(256, HM_P1_MINB) mv_phase1_kernel(const P1Desc* __restrict__ d, int64_t nd,
                                                         const T* __restrict__ pool,
                                                         const typename MvT<T>::X* __restrict__ xs,
                                                         int64_t xs_stride, double* __restrict__ z) {
@@ -145,8 +148,13 @@ __global__ void __launch_bounds__(256) mv_phase1_kernel(const P1Desc* __restrict
 // multiple of 4 elements and 16 bytes, padding rows hold zeros).
 // ---------------------------------------------------------------------------
 constexpr int P2_NB = 32;      // descriptors staged per round
-constexpr int P2_EMAX = 1024;  // expanded (leaf, column) entries per sub-round
-constexpr int P2_WARPS = MV_WROWS / 128;
+#ifndef HM_P2_SPLIT
+#define HM_P2_SPLIT 4
+#endif
+constexpr int P2_SPLIT = HM_P2_SPLIT;              // CTAs per window
+constexpr int P2_CROWS = MV_WROWS / P2_SPLIT;      // rows of one CTA
+constexpr int P2_WARPS = P2_CROWS / 128;           // 32 lanes x 4 rows a warp
+constexpr int P2_EMAX = 1024 / P2_SPLIT;           // expanded (leaf, column) entries per sub-round
 constexpr uint64_t P2_DENSE_FLAG = 1ull << 63;
 
 // 4 consecutive rows of one column are loaded as raw words and converted to
@@ -225,8 +233,9 @@ __global__ void __launch_bounds__(P2_WARPS * 32) mv_phase2_kernel(const MvWin* _
   __shared__ uint32_t e_rs[P2_EMAX];
   __shared__ double e_z[P2_EMAX];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const MvWin W = win[blockIdx.x];
-  const int base = 4 * (warp * 32 + lane);       // first of this lane's rows in the window
+  const MvWin W = win[blockIdx.x / P2_SPLIT];
+  const int h0 = (int)(blockIdx.x % P2_SPLIT) * P2_CROWS;   // this CTA's rows of the window
+  const int base = h0 + 4 * (warp * 32 + lane);  // first of this lane's rows in the window
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   for (uint32_t b0 = W.begin; b0 < W.end; b0 += P2_NB) {
     const int nb = (int)min((uint32_t)P2_NB, W.end - b0);
@@ -235,7 +244,9 @@ __global__ void __launch_bounds__(P2_WARPS * 32) mv_phase2_kernel(const MvWin* _
       int cnt = 0;
       if (lane < nb) {
         sd[lane] = d[b0 + lane];
-        cnt = (int)sd[lane].cnt;
+        // only leaves with rows in this CTA's part of the window are expanded
+        const int r0 = sd[lane].row_off, r1 = r0 + (int)sd[lane].m;
+        cnt = (r1 > h0 && r0 < h0 + P2_CROWS) ? (int)sd[lane].cnt : 0;
       }
       int incl = cnt;
 #pragma unroll
@@ -460,13 +471,19 @@ static int matvec_t(hm_handle* h, const double* d_x, double* d_y, int trans, cud
   if (P.np1 > 0) {
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
-    int64_t blocks = std::min<int64_t>((P.np1 + 7) / 8, (int64_t)nsm * 8);
+    // one wave of resident CTAs: the warps stride over equal-sized leaves and
+    // finish together (a grid of several partial waves leaves a tail)
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mv_phase1_kernel<T>, 256, 0) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    int64_t blocks = std::min<int64_t>((P.np1 + 7) / 8, (int64_t)nsm * per_sm);
     mv_phase1_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(P.d_p1, P.np1, (const T*)h->d_rk, xs, stride, h->d_z);
   }
   if (ev) HM_CUDA_TRY(cudaEventRecord(ev[2], st));
   // dense leaves are FP64 with FP64 factors and FP32 otherwise
   using TD = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
-  mv_phase2_kernel<T, TD><<<P.nwin, P2_WARPS * 32, 0, st>>>(P.d_win, P.d_p2, (const T*)h->d_rk,
+  mv_phase2_kernel<T, TD><<<(unsigned)(P.nwin * P2_SPLIT), P2_WARPS * 32, 0, st>>>(P.d_win, P.d_p2, (const T*)h->d_rk,
                                                             (const TD*)h->d_dense, h->d_z, d_x, d_y);
   if (ev) HM_CUDA_TRY(cudaEventRecord(ev[3], st));
   HM_CUDA_TRY(cudaGetLastError());
