@@ -359,6 +359,33 @@ int hm_copy(const hm_handle* h, hm_handle** out) {
   return copy_handle(h, out);
 }
 
+int hm_save(const hm_handle* h, const char* path, const void* user, int64_t user_bytes) {
+  if (!h || !path) return fail(HM_ERR_ARG, "NULL argument");
+  DeviceGuard g(h->device);
+  cudaStreamSynchronize(h->stream);
+  return save_handle(h, path, user, user_bytes);
+}
+
+int hm_load(const char* path, int32_t device, hm_handle** out) {
+  if (!path || !out) return fail(HM_ERR_ARG, "NULL argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(HM_ERR_CUDA, "no CUDA device: the H-matrix path has no CPU fallback");
+  if (device < 0 || device >= ndev) return fail(HM_ERR_ARG, "invalid device ordinal");
+  DeviceGuard g(device);
+  try {
+    return load_handle(path, device, check_params, out);
+  } catch (const std::bad_alloc&) {
+    return fail(HM_ERR_OOM, "load: host allocation");
+  }
+}
+
+int hm_load_user(const char* path, void* user, int64_t cap, int64_t* user_bytes) {
+  if (!path) return fail(HM_ERR_ARG, "NULL argument");
+  return load_user(path, user, cap, user_bytes);
+}
+
 int hm_lu(hm_handle* h) {
   if (!h) return fail(HM_ERR_ARG, "NULL handle");
   if (h->factorized) return fail(HM_ERR_STATE, "H-matrix H is already factorized; reuse factorization");

@@ -383,6 +383,45 @@ int build_matvec_plans(hm_handle* h) {
   return HM_OK;
 }
 
+// A handle read back from a file: the cluster tree, block tree and leaf list
+// are checked before anything is derived from them (every index in range,
+// every leaf inside the matrix and on its own clusters, node and leaf lists
+// pointing at each other), then the pools and matvec plans are laid out as
+// construction lays them out.
+int restore_structure(hm_handle* h) {
+  const int64_t ncl = (int64_t)h->cl_s.size();
+  if ((int64_t)h->cl_e.size() != ncl || (int64_t)h->cl_left.size() != ncl || (int64_t)h->cl_right.size() != ncl)
+    return fail(HM_ERR_ARG, "file: inconsistent cluster arrays");
+  HM_TRY(validate_tree(h, ncl));
+  const int64_t nn = (int64_t)h->nodes.size(), nl = (int64_t)h->leaves.size();
+  if (nn < 1 || nn > ((int64_t)1 << 31) || nl > nn) return fail(HM_ERR_ARG, "file: invalid block tree size");
+  for (int64_t i = 0; i < nn; ++i) {
+    const Node& d = h->nodes[i];
+    if (d.s < 0 || d.s >= ncl || d.t < 0 || d.t >= ncl) return fail(HM_ERR_ARG, "file: node cluster out of range");
+    if (d.type == T_H) {
+      for (int c = 0; c < 4; ++c)
+        if (d.child[c] <= i || d.child[c] >= nn) return fail(HM_ERR_ARG, "file: node child out of range");
+    } else if (d.type == T_DENSE || d.type == T_RK) {
+      if (d.leaf >= nl || (d.leaf >= 0 && h->leaves[d.leaf].node != i))
+        return fail(HM_ERR_ARG, "file: node and leaf lists disagree");
+    } else {
+      return fail(HM_ERR_ARG, "file: invalid node type");
+    }
+  }
+  for (int64_t i = 0; i < nl; ++i) {
+    const Leaf& L = h->leaves[i];
+    if (L.node < 0 || L.node >= nn || h->nodes[L.node].leaf != i || h->nodes[L.node].type != L.type)
+      return fail(HM_ERR_ARG, "file: leaf " + std::to_string(i) + " does not match its node");
+    if (L.s != h->nodes[L.node].s || L.t != h->nodes[L.node].t)
+      return fail(HM_ERR_ARG, "file: leaf clusters differ from its node's");
+    if (L.row0 != h->cl_s[L.s] || L.col0 != h->cl_s[L.t] || L.m != csize(h, L.s) || L.n != csize(h, L.t))
+      return fail(HM_ERR_ARG, "file: leaf extent differs from its clusters");
+    if (L.type == T_RK ? (L.k < 0 || L.k > MV_KMAX) : L.k != 0)
+      return fail(HM_ERR_ARG, "file: invalid leaf rank");
+  }
+  return build_matvec_plans(h);
+}
+
 void free_handle_data(hm_handle* h) {
   auto fr = [](void* p) { if (p) cudaFree(p); };
   fr(h->d_geom);

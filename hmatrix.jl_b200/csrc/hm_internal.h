@@ -247,6 +247,11 @@ int to_dense(const hm_handle* h, double* d_out);   // device output n*n
 int apply_shift(hm_handle* h, double lambda);
 int apply_scale(hm_handle* h, double u);
 int copy_handle(const hm_handle* h, hm_handle** out);
+int restore_structure(hm_handle* h);
+// file export / import (hm_io.cu)
+int save_handle(const hm_handle* h, const char* path, const void* user, int64_t user_bytes);
+int load_user(const char* path, void* user, int64_t cap, int64_t* user_bytes);
+int load_handle(const char* path, int device, int (*validate)(const hm_params*), hm_handle** out);
 void free_handle_data(hm_handle* h);
 void lu_describe(const hm_handle* h, int64_t* tiles, int64_t* cap);
 

@@ -14,7 +14,7 @@ namespace hm {
 
 constexpr int ACA_MAX_EXTENT = 2048;   // largest block side for device aca2
 constexpr int RCORE_MAX = 96;          // largest core of the QR+SVD recompression
-constexpr int MV_KMAX = 255;           // largest rank a leaf may carry
+constexpr int MV_KMAX = 4096;          // largest rank a leaf may carry (bbfmm 2-D: 64^2)
 
 // ---------------------------------------------------------------------------
 // warp / block reductions (fixed order: results are reproducible run to run)

@@ -17,6 +17,7 @@ reference.  All arithmetic runs in the CUDA library; there is no CPU path.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass
 from typing import Optional
 
@@ -30,7 +31,7 @@ from .kernels import Cauchy, CauchyDP, Gauss, GaussDP, InvQuad, InvQuadDP, Kerne
 __all__ = [
     "Hparams", "Params", "NewHmat", "FullMat", "Hmat", "lu", "lu_", "getl", "getu", "info",
     "Cauchy", "InvQuad", "Gauss", "Kernel", "Cluster", "construct_cluster", "HmError",
-    "aca_wrapper", "F64", "F32", "BF16", "new_on_cluster", "CauchyDP", "InvQuadDP", "GaussDP",
+    "aca_wrapper", "F64", "F32", "BF16", "new_on_cluster", "load", "CauchyDP", "InvQuadDP", "GaussDP",
     "lu_batch", "lu_batch_", "solve_batch", "solve_refined_batch", "matvec_batch", "gmres", "bicgstab",
 ]
 
@@ -221,6 +222,18 @@ class Hmat:
         check(lib().hm_copy(self._h, C.byref(out)))
         return Hmat(out.value, self.n, self.c)
 
+    def save(self, path):
+        """Write the (unfactorised) H-matrix to ``path``; the cluster tree and
+        permutation of ``self.c`` go into the file's user block."""
+        import io
+        blob = b""
+        if self.c is not None:
+            buf = io.BytesIO()
+            np.savez(buf, X=self.c.X, P=self.c.P, s=self.c.s, e=self.c.e, left=self.c.left, right=self.c.right)
+            blob = buf.getvalue()
+        cb = C.create_string_buffer(blob, len(blob)) if blob else None
+        check(lib().hm_save(self._h, os.fsencode(path), C.cast(cb, C.c_void_p) if cb else None, len(blob)))
+
     def add_identity(self, lam):
         """``lam*I + H`` (src/harithm.jl:457-473), returning a new H."""
         H = self.copy()
@@ -337,6 +350,27 @@ def new_on_cluster(prm: Params, c: Cluster):
                        _ptr(c.right), 0 if nb is None else len(nb),
                        None if nb is None else _ptr(np.ascontiguousarray(nb)), C.byref(out)))
     return Hmat(out.value, n, c)
+
+
+def load(path, device=0):
+    """An H-matrix written by :meth:`Hmat.save`, rebuilt on ``device``;
+    returns (c, H) like :func:`NewHmat`."""
+    import io
+    from .cluster import Cluster
+    p = os.fsencode(path)
+    ub = C.c_int64(0)
+    check(lib().hm_load_user(p, None, 0, C.byref(ub)))
+    c = None
+    if ub.value > 0:
+        buf = C.create_string_buffer(ub.value)
+        check(lib().hm_load_user(p, C.cast(buf, C.c_void_p), ub.value, C.byref(ub)))
+        z = np.load(io.BytesIO(buf.raw), allow_pickle=False)
+        c = Cluster(z["X"], z["P"], z["s"], z["e"], z["left"], z["right"])
+    out = C.c_void_p()
+    check(lib().hm_load(p, int(device), C.byref(out)))
+    info = _lib.hm_info_t()
+    check(lib().hm_info(out, C.byref(info)))
+    return c, Hmat(out.value, int(info.n), c)
 
 
 def lu(H: Hmat):

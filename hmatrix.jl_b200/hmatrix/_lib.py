@@ -25,13 +25,14 @@ HM_FLAG_TRANS = 2
 STATUS_NAMES = {
     1: "HM_ERR_ARG", 2: "HM_ERR_CUDA", 3: "HM_ERR_OOM", 4: "HM_ERR_STATE", 5: "HM_ERR_SINGULAR",
     6: "HM_ERR_RANK", 7: "HM_ERR_NONFINITE", 8: "HM_ERR_UNSUPPORTED", 9: "HM_ERR_TIMEOUT",
+    10: "HM_ERR_IO",
 }
 
 # every symbol include/hmatrix_b200.h declares
 EXPORTED = [
     "hm_version", "hm_last_error", "hm_default_params", "hm_new", "hm_destroy", "hm_info",
     "hm_leaves", "hm_leaf_factors", "hm_to_dense", "hm_matvec", "hm_matvec_profile", "hm_exact_rows",
-    "hm_add_identity", "hm_scale", "hm_copy", "hm_lu", "hm_lu_perm", "hm_solve", "hm_solve_refined",
+    "hm_add_identity", "hm_scale", "hm_copy", "hm_save", "hm_load", "hm_load_user", "hm_lu", "hm_lu_perm", "hm_solve", "hm_solve_refined",
     "hm_batch_lu", "hm_batch_solve", "hm_batch_solve_refined", "hm_batch_matvec",
     "aca_wrapper",
     "aca_wrapper_noalloc",
@@ -95,6 +96,9 @@ def lib():
     L.hm_add_identity.argtypes = [vp, C.c_double]
     L.hm_scale.argtypes = [vp, C.c_double]
     L.hm_copy.argtypes = [vp, C.POINTER(vp)]
+    L.hm_save.argtypes = [vp, C.c_char_p, vp, C.c_int64]
+    L.hm_load.argtypes = [C.c_char_p, C.c_int32, C.POINTER(vp)]
+    L.hm_load_user.argtypes = [C.c_char_p, vp, C.c_int64, p64]
     L.hm_lu.argtypes = [vp]
     L.hm_lu_perm.argtypes = [vp, vp]
     L.hm_solve.argtypes = [vp, vp, vp, C.c_int64, C.c_uint32, vp]

@@ -37,6 +37,7 @@ extern "C" {
 #define HM_ERR_NONFINITE   7   /* NaN/Inf met where a finite value is needed */
 #define HM_ERR_UNSUPPORTED 8   /* valid request outside what is implemented  */
 #define HM_ERR_TIMEOUT     9   /* a bounded device wait gave up              */
+#define HM_ERR_IO         10   /* a file could not be opened, read or written */
 
 /* ---- kernels (Hparams.Kernel has to be one of these on the device) ----- */
 #define HM_KERNEL_CAUCHY   1   /* 1/(1 + |x-y|^2/p^2)      p = kparam (ell)   */
@@ -191,6 +192,20 @@ int hm_scale(hm_handle* h, double u);
 
 /* copy(H) (src/utils.jl:130-159) */
 int hm_copy(const hm_handle* h, hm_handle** out);
+
+/* Export / import of a built (unfactorised) H-matrix: parameters, cluster
+ * tree, block tree, geometry and factor pools in one binary file, so that a
+ * construction is paid once.  No counterpart in the reference (its REQUIRE
+ * lists JLD2, unused).  hm_save refuses a factorised handle (HM_ERR_STATE);
+ * `user` (user_bytes, may be 0) is stored alongside for the caller (the host
+ * mirror keeps the cluster permutation there).  hm_load rebuilds the handle
+ * on `device` after checking every index of the file's structure; a file from
+ * another build, a truncated or altered file is refused (HM_ERR_ARG /
+ * HM_ERR_IO).  hm_load_user reads only the user block: *user_bytes receives
+ * its size, and min(cap, size) bytes are copied to user when it is not NULL. */
+int hm_save(const hm_handle* h, const char* path, const void* user, int64_t user_bytes);
+int hm_load(const char* path, int32_t device, hm_handle** out);
+int hm_load_user(const char* path, void* user, int64_t cap, int64_t* user_bytes);
 
 /* lu!(H) (src/hlu.jl:465-515): factorise in place with pivoting inside each
  * diagonal leaf.  HM_ERR_STATE if already factorised (src/hlu.jl:466-468). */

@@ -51,11 +51,11 @@ def test_bbfmm_1d_vs_oracle():
     assert np.abs(H.to_dense() - A).max() < 1e-5          # 10 Chebyshev nodes
 
 
-@pytest.mark.parametrize("max_rank,max_block", [(6, 300), (16, 128)])
-def test_bbfmm_2d_vs_oracle(max_rank, max_block):
+@pytest.mark.parametrize("max_rank,max_block,n", [(6, 300, 1500), (16, 128, 1500), (16, 400, 3000)])
+def test_bbfmm_2d_vs_oracle(max_rank, max_block, n):
     import hmatrix as hm
     from oracle import hm_oracle as O
-    G = np.random.default_rng(2).uniform(0, 1, (1500, 2))
+    G = np.random.default_rng(2).uniform(0, 1, (n, 2))
     c, H = hm.NewHmat(hm.Params(Geom=G, Kernel=hm.InvQuad(100.0), MaxBlock=max_block, MinBlock=32,
                                 MaxRank=max_rank, ConsMethod="bbfmm", Tree="bisect"))
     oc, OH = O.NewHmat(O.Params(Geom=G, Kernel=O.kernel_invquad(100.0), MaxBlock=max_block, MinBlock=32,
@@ -64,8 +64,10 @@ def test_bbfmm_2d_vs_oracle(max_rank, max_block):
     ranks = set(lv[lv[:, 0] == 1, 5])
     if max_rank == 6:
         assert ranks == {36}
-    else:                                   # r lowered to floor(sqrt(max(m, n))) < 16
+    elif max_block == 128:                  # r lowered to floor(sqrt(max(m, n))) < 16
         assert max(ranks) < 256 and all(int(round(np.sqrt(k))) ** 2 == k for k in ranks)
+    else:                                   # the reference's default MaxRank: rank 256 leaves
+        assert 256 in ranks
     A = O.FullMat(O.kernel_invquad(100.0), oc.X, oc.X)
     assert np.abs(H.to_dense() - A).max() < 1e-8
 
