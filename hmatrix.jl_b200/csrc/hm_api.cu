@@ -359,6 +359,21 @@ int hm_copy(const hm_handle* h, hm_handle** out) {
   return copy_handle(h, out);
 }
 
+int hm_coarsen(const hm_handle* h, hm_handle** out) {
+  if (!h || !out) return fail(HM_ERR_ARG, "NULL argument");
+  *out = nullptr;
+  DeviceGuard g(h->device);
+  return coarsen_handle(h, out);
+}
+
+int hm_add(const hm_handle* a, const hm_handle* b, double scalar, hm_handle** out) {
+  if (!a || !b || !out) return fail(HM_ERR_ARG, "NULL argument");
+  *out = nullptr;
+  if (a->device != b->device) return fail(HM_ERR_UNSUPPORTED, "hadd: the H-matrices live on different devices");
+  DeviceGuard g(a->device);
+  return add_handles(a, b, scalar, out);
+}
+
 int hm_save(const hm_handle* h, const char* path, const void* user, int64_t user_bytes) {
   if (!h || !path) return fail(HM_ERR_ARG, "NULL argument");
   DeviceGuard g(h->device);

@@ -248,6 +248,9 @@ int apply_shift(hm_handle* h, double lambda);
 int apply_scale(hm_handle* h, double u);
 int copy_handle(const hm_handle* h, hm_handle** out);
 int restore_structure(hm_handle* h);
+// leaf-format-changing arithmetic (hm_harith.cu)
+int coarsen_handle(const hm_handle* h, hm_handle** out);
+int add_handles(const hm_handle* a, const hm_handle* b, double scalar, hm_handle** out);
 // file export / import (hm_io.cu)
 int save_handle(const hm_handle* h, const char* path, const void* user, int64_t user_bytes);
 int load_user(const char* path, void* user, int64_t cap, int64_t* user_bytes);

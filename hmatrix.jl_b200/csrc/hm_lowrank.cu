@@ -269,6 +269,13 @@ __global__ void __launch_bounds__(512) aca_fp_kernel(const AcaFpJob* __restrict_
 
 __global__ void __launch_bounds__(512) aca_fp_one_kernel(AcaFpJob J) { aca_fp_body(J); }
 
+int launch_aca_fp(const AcaFpJob* d_jobs, int njobs, cudaStream_t st) {
+  if (njobs <= 0) return HM_OK;
+  aca_fp_kernel<<<njobs, 512, 0, st>>>(d_jobs);
+  HM_CUDA_TRY(cudaGetLastError());
+  return HM_OK;
+}
+
 int launch_aca_fp_one(const AcaFpJob& J, cudaStream_t st) {
   aca_fp_one_kernel<<<1, 512, 0, st>>>(J);
   HM_CUDA_TRY(cudaGetLastError());

@@ -104,6 +104,7 @@ struct AcaFpJob {
   double eps_trunc;
 };
 int launch_aca_fp_one(const AcaFpJob& J, cudaStream_t st);
+int launch_aca_fp(const AcaFpJob* d_jobs, int njobs, cudaStream_t st);   // one CTA per job
 int launch_core_one(const CoreJob& J, double eps_trunc, int* d_flags, cudaStream_t st);
 // launch the batched recompression; status of rank overflow/nonfinite is
 // OR-ed into *d_flags (bit 0: rank > kcap, bit 1: non-finite).

@@ -31,7 +31,7 @@ from .kernels import Cauchy, CauchyDP, Gauss, GaussDP, InvQuad, InvQuadDP, Kerne
 __all__ = [
     "Hparams", "Params", "NewHmat", "FullMat", "Hmat", "lu", "lu_", "getl", "getu", "info",
     "Cauchy", "InvQuad", "Gauss", "Kernel", "Cluster", "construct_cluster", "HmError",
-    "aca_wrapper", "F64", "F32", "BF16", "new_on_cluster", "load", "CauchyDP", "InvQuadDP", "GaussDP",
+    "aca_wrapper", "F64", "F32", "BF16", "new_on_cluster", "load", "coarsening", "CauchyDP", "InvQuadDP", "GaussDP",
     "lu_batch", "lu_batch_", "solve_batch", "solve_refined_batch", "matvec_batch", "gmres", "bicgstab",
 ]
 
@@ -246,13 +246,29 @@ class Hmat:
         check(lib().hm_scale(H._h, float(u)))
         return H
 
+    def hadd(self, other, scalar=1.0):
+        """``self + scalar*other`` for two H-matrices on the same block
+        partition (``hadd``/``hmat_add!``, src/harithm.jl:4-159, 374-420):
+        a new H-matrix in the formats of ``self``."""
+        out = C.c_void_p()
+        check(lib().hm_add(self._h, other._h, float(scalar), C.byref(out)))
+        return Hmat(out.value, self.n, self.c)
+
     def __add__(self, other):
-        from numbers import Number
         if isinstance(other, _Identity):
             return self.add_identity(other.lam)
+        if isinstance(other, Hmat):
+            return self.hadd(other, 1.0)                 # src/harithm.jl:158
         raise TypeError("H + %r is outside the hot path" % type(other))
 
     __radd__ = __add__
+
+    def __sub__(self, other):
+        if isinstance(other, Hmat):
+            return self.hadd(other, -1.0)                # src/harithm.jl:159
+        if isinstance(other, _Identity):
+            return self.add_identity(-other.lam)
+        raise TypeError("H - %r is outside the hot path" % type(other))
 
     def __neg__(self):
         return self.scaled(-1.0)
@@ -371,6 +387,14 @@ def load(path, device=0):
     info = _lib.hm_info_t()
     check(lib().hm_info(out, C.byref(info)))
     return c, Hmat(out.value, int(info.n), c)
+
+
+def coarsening(H: Hmat):
+    """``coarsening(H)`` (src/utils.jl:29-59): a copy in which every dense leaf
+    off the diagonal with truncated SVD rank <= MaxRank becomes low-rank."""
+    out = C.c_void_p()
+    check(lib().hm_coarsen(H._h, C.byref(out)))
+    return Hmat(out.value, H.n, H.c)
 
 
 def lu(H: Hmat):

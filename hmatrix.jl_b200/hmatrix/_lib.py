@@ -32,7 +32,7 @@ STATUS_NAMES = {
 EXPORTED = [
     "hm_version", "hm_last_error", "hm_default_params", "hm_new", "hm_destroy", "hm_info",
     "hm_leaves", "hm_leaf_factors", "hm_to_dense", "hm_matvec", "hm_matvec_profile", "hm_exact_rows",
-    "hm_add_identity", "hm_scale", "hm_copy", "hm_save", "hm_load", "hm_load_user", "hm_lu", "hm_lu_perm", "hm_solve", "hm_solve_refined",
+    "hm_add_identity", "hm_scale", "hm_copy", "hm_coarsen", "hm_add", "hm_save", "hm_load", "hm_load_user", "hm_lu", "hm_lu_perm", "hm_solve", "hm_solve_refined",
     "hm_batch_lu", "hm_batch_solve", "hm_batch_solve_refined", "hm_batch_matvec",
     "aca_wrapper",
     "aca_wrapper_noalloc",
@@ -96,6 +96,8 @@ def lib():
     L.hm_add_identity.argtypes = [vp, C.c_double]
     L.hm_scale.argtypes = [vp, C.c_double]
     L.hm_copy.argtypes = [vp, C.POINTER(vp)]
+    L.hm_coarsen.argtypes = [vp, C.POINTER(vp)]
+    L.hm_add.argtypes = [vp, vp, C.c_double, C.POINTER(vp)]
     L.hm_save.argtypes = [vp, C.c_char_p, vp, C.c_int64]
     L.hm_load.argtypes = [C.c_char_p, C.c_int32, C.POINTER(vp)]
     L.hm_load_user.argtypes = [C.c_char_p, vp, C.c_int64, p64]

@@ -193,6 +193,21 @@ int hm_scale(hm_handle* h, double u);
 /* copy(H) (src/utils.jl:130-159) */
 int hm_copy(const hm_handle* h, hm_handle** out);
 
+/* coarsening(H) (src/utils.jl:29-59): a new H-matrix in which every dense
+ * leaf off the diagonal whose truncated SVD rank (S/S[1] > eps_trunc) is at
+ * most MaxRank is stored as that low-rank pair.  HM_ERR_STATE on a
+ * factorised handle. */
+int hm_coarsen(const hm_handle* h, hm_handle** out);
+
+/* a + scalar*b (hadd / hmat_add!, src/harithm.jl:4-159, 374-420; a - b is
+ * scalar = -1) as a new H-matrix, for two H-matrices on the same block
+ * partition (leaf formats may differ; the format of a is kept, low-rank sums
+ * recompressed with eps_trunc).  Different partitions or storage precisions
+ * are refused (HM_ERR_UNSUPPORTED), as is a low-rank sum whose ranks add up
+ * to more than 96.  The reference's H*H operator (src/harithm.jl:315) calls
+ * itself; its hmul serves lu! and is built inside hm_lu. */
+int hm_add(const hm_handle* a, const hm_handle* b, double scalar, hm_handle** out);
+
 /* Export / import of a built (unfactorised) H-matrix: parameters, cluster
  * tree, block tree, geometry and factor pools in one binary file, so that a
  * construction is paid once.  No counterpart in the reference (its REQUIRE

@@ -19,6 +19,7 @@ Hmatrix.jl for the hot path, following the reference files line by line
 * fully pivoted ACA ................. deps/src/ACA_FullyPivoted.cpp:9-236
 * H-matvec .......................... src/harithm.jl:317-371
 * H-add / recompression ............. src/harithm.jl:4-159,374-420
+* ``coarsening`` .................... src/utils.jl:29-59
 * H x H product ``hmul`` ............ src/harithm.jl:162-315
 * shifts / scaling .................. src/harithm.jl:456-502
 * copy / densify / ``info`` ......... src/utils.jl:83-192
@@ -902,10 +903,37 @@ def hmat_add(a, b, scalar, prm):
                 hmat_add(a.children[i][j], b.children[i][j], scalar, prm)
 
 
-def hadd(a, b, prm):
+def hadd(a, b, prm, scalar=1.0):
+    """``hadd`` (src/harithm.jl:153-157), and ``a - b`` with scalar = -1."""
     c = hmat_copy(a)
-    hmat_add(c, b, 1.0, prm)
+    hmat_add(c, b, scalar, prm)
     return c
+
+
+def coarsening(H, prm):
+    """``coarsening`` (src/utils.jl:29-59): every dense leaf whose row and
+    column clusters differ becomes U_k, V_k S_k when its truncated SVD rank
+    k = findlast(S/S[1] > εTrunc) is at most MaxRank.  A block with S[1] = 0
+    stays dense (the reference divides by it and fails there)."""
+    G = hmat_copy(H)
+
+    def helper(h):
+        if h.is_full and not h.s.same(h.t):
+            U, S, Vt = np.linalg.svd(h.C, full_matrices=False)
+            if S[0] == 0:
+                return
+            k = rank_truncate(S, prm.εTrunc)
+            if k <= prm.MaxRank:
+                h.A = U[:, :k].copy()
+                h.B = (S[:k, None] * Vt[:k, :]).T.copy()
+                h.C = None
+                h.is_rk, h.is_full = True, False
+        elif h.is_h:
+            for i in range(2):
+                for j in range(2):
+                    helper(h.children[i][j])
+    helper(G)
+    return G
 
 
 # ----------------------------------------------------------------------------

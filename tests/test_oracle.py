@@ -183,3 +183,52 @@ def test_bbfmm_newhmat_2d_accuracy():
     lv = np.asarray(O.block_list(H))
     assert (lv[:, 0] == 1).any()
     assert np.abs(O.to_fmat(H) - A).max() < 1e-8
+
+
+# --- coarsening and H + H (src/utils.jl:29-59, src/harithm.jl:4-159,374-420) --
+
+def _readme(O, max_rank, kernel=None):
+    prm = O.Params(Geom=np.linspace(0, 10, 2000), Kernel=kernel or O.kernel_cauchy(), MaxBlock=500,
+                   MinBlock=64, MaxRank=max_rank, ConsMethod="svd")
+    c, H = O.NewHmat(prm)
+    return prm, c, H
+
+
+def test_coarsening_oracle():
+    from oracle import hm_oracle as O
+    prm, c, H = _readme(O, 5)
+    G = O.coarsening(H, prm)
+    b0, b1 = np.asarray(O.block_list(H)), np.asarray(O.block_list(G))
+    assert np.array_equal(b0[:, 1:5], b1[:, 1:5])                 # same partition
+    conv = (b0[:, 0] == 0) & (b1[:, 0] == 1)
+    assert conv.sum() > 0 and (b1[conv, 5] <= 5).all()
+    diag = (b0[:, 1] == b0[:, 2]) & (b0[:, 3] == b0[:, 4])
+    assert not (conv & diag).any()                                # diagonal leaves stay dense
+    A = O.FullMat(O.kernel_cauchy(), c.X, c.X)
+    assert np.abs(O.to_fmat(G) - A).max() < 1e-8                  # test/cluster.jl:9's bar
+    assert O.info(G)[3] < O.info(H)[3] or O.info(G)[3] <= O.info(H)[3]
+
+
+def test_hadd_oracle():
+    from oracle import hm_oracle as O
+    # aca2 route: the partition depends on the geometry only, so two kernels share it
+    kw = dict(Geom=np.linspace(0, 10, 1500), MaxBlock=300, MinBlock=32, MaxRank=16, ConsMethod="aca2",
+              Tree="bisect")
+    _, A1 = O.NewHmat(O.Params(Kernel=O.kernel_cauchy(), **kw))
+    _, A2 = O.NewHmat(O.Params(Kernel=O.kernel_invquad(3.0), **kw))
+    assert np.array_equal(np.asarray(O.block_list(A1))[:, :5], np.asarray(O.block_list(A2))[:, :5])
+    prm, c, H1 = _readme(O, 5)
+    S = O.hadd(A1, A2, prm)
+    D = O.to_fmat(A1) + O.to_fmat(A2)
+    assert np.abs(O.to_fmat(S) - D).max() <= 1e-9 * np.abs(D).max()
+    H2 = O.scale(0.7, H1)
+    S = O.hadd(H1, H2, prm)
+    D = O.to_fmat(H1) + O.to_fmat(H2)
+    assert np.abs(O.to_fmat(S) - D).max() <= 1e-9 * np.abs(D).max()
+    Z = O.hadd(H1, H1, prm, -1.0)
+    assert np.abs(O.to_fmat(Z)).max() <= 1e-13
+    # mixed formats: a coarsened copy against the original
+    G = O.coarsening(H1, prm)
+    for a, b in ((H1, G), (G, H1)):
+        M = O.hadd(a, b, prm)
+        assert np.abs(O.to_fmat(M) - 2 * O.to_fmat(H1)).max() <= 1e-8
