@@ -360,7 +360,8 @@ def lu_solve_leg(n, torch):
     (n points on [0,10], 1/(1+(x-y)^2) + delta_xy, MaxBlock 256, MinBlock 32,
     MaxRank 12, one N(0,1) right-hand side): the FP64 factorisation as in the
     reference (eps_trunc 1e-10) against a cheaper low-accuracy factorisation
-    (eps_trunc 1e-6 inside the LU), both refined with the FP64 H-matvec to a
+    (eps_trunc 1e-3 inside the LU: the fastest total of a sweep over 1e-6 .. 1e-2
+    at this size), both refined with the FP64 H-matvec to a
     relative residual <= 1e-10."""
     import hmatrix as hm
     out = {"config": {"n": n, "kernel": "1/(1+(x-y)^2) + delta_xy", "MaxBlock": 256, "MinBlock": 32,
@@ -375,7 +376,7 @@ def lu_solve_leg(n, torch):
     wH.lu_()
     wH.solve_refined(np.ones(4096), tol=1e-10, max_iter=5)
     del wH
-    for name, epslu in (("fp64", 0.0), ("mixed", 1e-6)):
+    for name, epslu in (("fp64", 0.0), ("mixed", 1e-3)):
         prm = hm.Params(Geom=np.linspace(0, 10, n), Kernel=hm.Cauchy(1.0), MaxBlock=256, MinBlock=32,
                         MaxRank=12, ConsMethod="aca2", εComp=1e-10, Tree="bisect", Shift=1.0, εTruncLU=epslu,
                         Device=torch.cuda.current_device())
