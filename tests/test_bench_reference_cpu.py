@@ -1,0 +1,35 @@
+"""The reference arm of bench.py (`--impl reference`) on the CPU: the C
+restatement of aca2 + hmat_matvec! timed on a bounded band of rows, printed as
+the same JSON line as the GPU arm with impl = "reference"; ranks other than 0
+exit without work."""
+import json
+import os
+import subprocess
+import sys
+
+from conftest import ROOT
+
+ARGS = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--n", "65536",
+        "--cpu-rows", "512", "--steps", "1", "--warmup", "0"]
+
+
+def test_reference_line_contract():
+    out = subprocess.run(ARGS, cwd=ROOT, capture_output=True, text=True, timeout=600, check=True)
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == bench.UNIT
+    assert d["value"] > 0 and d["higher_is_better"] is True and d["n_gpus"] == 1
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert d["config"]["n"] == 65536 and d["config"]["workload"]
+
+
+def test_reference_other_ranks_silent():
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2")
+    out = subprocess.run(ARGS, cwd=ROOT, capture_output=True, text=True, timeout=600, env=env)
+    assert out.returncode == 0
+    assert not [l for l in out.stdout.splitlines() if l.startswith("{")]
