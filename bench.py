@@ -396,6 +396,59 @@ def lu_solve_leg(n, torch):
     return out
 
 
+LU_CPU_N = 8192          # bounded size of the CPU H-LU sample (the oracle takes ~3 s there)
+
+
+def lu_params(n):
+    """Parameters of the H-LU legs: n points on [0,10], MaxBlock 256, MinBlock 32,
+    MaxRank 12, aca2 at 1e-10, median-bisection tree (kernel and shift apart)."""
+    return dict(Geom=np.linspace(0, 10, n), MaxBlock=256, MinBlock=32, MaxRank=12, ConsMethod="aca2",
+                εComp=1e-10, Tree="bisect")
+
+
+def oracle_lu_sample(n):
+    """The reference's lu! and \\ (src/hlu.jl:465-562) as restated in FP64 numpy by
+    the oracle, timed on the host cores (numpy's BLAS on every thread) on the LU
+    leg's matrix at a bounded size n: 1/(1+(x-y)^2) + I, no refinement."""
+    import os
+    from oracle import hm_oracle as O
+    y = np.random.default_rng(3).standard_normal(n)
+    prm = O.Params(Kernel=O.kernel_cauchy(), **lu_params(n))
+    _, H = O.NewHmat(prm)
+    H = O.add_identity(H, 1.0)
+    t0 = time.perf_counter()
+    L = O.lu(H, prm)
+    t1 = time.perf_counter()
+    x = O.solve(L, y)
+    t2 = time.perf_counter()
+    rr = float(np.linalg.norm(O.matvec(H, x) - y) / np.linalg.norm(y))
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except Exception:
+        cores = os.cpu_count() or 1
+    return {"n": n, "lu_s": t1 - t0, "solve_s": t2 - t1, "total_s": t2 - t0, "relres": rr, "cores": cores,
+            "kind": "port", "sample": "lu! + \\ of the FP64 oracle (numpy/BLAS) at n=%d" % n}
+
+
+def lu_cpu_beside_gpu(n, torch):
+    """The CPU sample of oracle_lu_sample next to the GPU's FP64 lu(H) + H\\y of the
+    same matrix (no refinement on either side)."""
+    import hmatrix as hm
+    cpu = oracle_lu_sample(n)
+    y = np.random.default_rng(3).standard_normal(n)
+    _, H = hm.NewHmat(hm.Params(Kernel=hm.Cauchy(1.0), Shift=1.0, Device=torch.cuda.current_device(),
+                                **lu_params(n)))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L = hm.lu(H)
+    t1 = time.perf_counter()
+    x = L.solve(y)
+    t2 = time.perf_counter()
+    rr = float(np.linalg.norm(H * x - y) / np.linalg.norm(y))
+    gpu = {"n": n, "lu_s": t1 - t0, "solve_s": t2 - t1, "total_s": t2 - t0, "relres": rr}
+    return {"cpu": cpu, "gpu": gpu, "gpu_speedup": cpu["total_s"] / gpu["total_s"]}
+
+
 def batched_problems(count, seed=3, nmin=2 ** 10, nmax=2 ** 16):
     """The batched uneven 1-D problems: n = round(2^U(log2 nmin, log2 nmax)),
     points sorted U[0, L] with L ~ U[5, 20], K = 1/(1+((x-y)/l)^2) + delta_xy
@@ -540,6 +593,11 @@ def run_ours(a):
         H = None
         torch.cuda.empty_cache()
         lu = lu_solve_leg(a.lu_n, torch)
+        if not a.no_cpu:
+            try:
+                lu["cpu_baseline"] = lu_cpu_beside_gpu(LU_CPU_N, torch)
+            except Exception as e:          # the CPU sample never costs the bench line
+                lu["cpu_baseline"] = {"error": repr(e)[:300]}
     batch = None
     if a.batch > 0:
         H = None

@@ -33,3 +33,13 @@ def test_reference_other_ranks_silent():
     out = subprocess.run(ARGS, cwd=ROOT, capture_output=True, text=True, timeout=600, env=env)
     assert out.returncode == 0
     assert not [l for l in out.stdout.splitlines() if l.startswith("{")]
+
+
+def test_oracle_lu_sample_contract():
+    # the CPU H-LU sample set beside the GPU's in the bench's LU leg
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "hmatrix.jl_b200"))
+    import bench
+    d = bench.oracle_lu_sample(2048)
+    assert d["n"] == 2048 and d["kind"] == "port" and d["cores"] >= 1
+    assert d["lu_s"] > 0 and d["total_s"] >= d["lu_s"] and d["relres"] < 1e-8
