@@ -156,13 +156,13 @@ def traffic_per_byte():
 # --------------------------------------------------------------------------
 # CPU baseline: the C restatement of aca2 + hmat_matvec! on a band of rows
 # --------------------------------------------------------------------------
-def cpu_sample_gbs(n, rows, target_s=12.0, max_reps=200):
+def cpu_sample_gbs(n, rows, target_s=12.0, max_reps=200, nthreads=0):
     from hmatrix.cluster import construct_cluster
     from oracle.hm_oracle_c import Sample
     c = construct_cluster(np.linspace(0, 10, n), 64, "bisect")
     tree = {"s": c.s, "e": c.e, "left": c.left, "right": c.right}
     r0 = n // 2 - rows // 2
-    S = Sample(1, 1.0, c.X, tree, 64, 512, 16, 1e-8, r0, r0 + rows)
+    S = Sample(1, 1.0, c.X, tree, 64, 512, 16, 1e-8, r0, r0 + rows, nthreads=nthreads)
     x = np.random.default_rng(1).standard_normal(n)
     S.matvec(x)
     t0 = time.perf_counter()
@@ -611,6 +611,11 @@ def run_ours(a):
     if not a.no_cpu and world == 1:
         gbs, thr, sample, _ = cpu_sample_gbs(a.n, a.cpu_rows)
         cpu = {"value": gbs, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample}
+        try:                                # the reference's own mode: one thread
+            g1, _, s1, _ = cpu_sample_gbs(a.n, a.cpu_rows, target_s=4.0, nthreads=1)
+            cpu["single_thread"] = {"value": g1, "unit": UNIT, "cores": 1, "sample": s1}
+        except Exception as e:
+            cpu["single_thread"] = {"error": repr(e)[:300]}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "strong" if shard else "weak",
