@@ -232,3 +232,27 @@ def test_hadd_oracle():
     for a, b in ((H1, G), (G, H1)):
         M = O.hadd(a, b, prm)
         assert np.abs(O.to_fmat(M) - 2 * O.to_fmat(H1)).max() <= 1e-8
+
+
+def test_c_restatement_matches_python_oracle():
+    # the C restatement of the partition, aca2 and hmat_matvec! (the CPU baseline
+    # of bench.py) against the Python oracle: same leaves and ranks, same product
+    import sys
+    import os
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "hmatrix.jl_b200"))
+    from oracle import hm_oracle as O
+    from oracle.hm_oracle_c import Sample
+    from hmatrix.cluster import construct_cluster
+    n = 4096
+    G = np.linspace(0, 10, n)
+    c = construct_cluster(G, 64, "bisect")
+    S = Sample(1, 1.0, c.X, {"s": c.s, "e": c.e, "left": c.left, "right": c.right}, 64, 512, 16, 1e-8, 0, n)
+    _, OH = O.NewHmat(O.Params(Geom=G, Kernel=O.kernel_cauchy(), MaxBlock=512, MinBlock=64, MaxRank=16,
+                               ConsMethod="aca2", εComp=1e-8, Tree="bisect"))
+    ref = np.asarray(O.block_list(OH), np.int64)
+    assert np.array_equal(S.lv, ref[:, :5])
+    assert np.array_equal(np.where(S.lv[:, 0] == 1, S.rank, 0), ref[:, 5])
+    x = np.random.default_rng(1).standard_normal(n)
+    yo = O.matvec(OH, x)
+    assert np.linalg.norm(S.matvec(x) - yo) <= 1e-13 * np.linalg.norm(yo)
