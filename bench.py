@@ -12,8 +12,11 @@ needed between steps.  `e2e` is the same metric through hm_matvec with host
 (pinned) buffers, the 8 MB host->device copy of x and device->host copy of y
 inside the timed region.
 
-Multi-GPU: every rank builds and multiplies its own replica (independent
-H-matrices, no exchange), weak scaling; the job time is the max over ranks.
+Multi-GPU (--gpus N): one H of n = 2^20 row-sharded over the ranks (strong
+scaling): every rank builds and multiplies only its rows (shards balanced by
+the bytes they stream), and one NCCL all-gather of the row shards leaves the
+full H*x on every rank each step; the job time is the max over ranks.
+--replicas runs N independent copies instead (weak scaling).
 
 --impl reference times the reference algorithm's CPU path (the C restatement
 of hmat_matvec! in oracle/, FP64, all host threads) on a bounded sample of
@@ -185,7 +188,8 @@ def run_reference(a):
     gbs, thr, sample, dt = cpu_sample_gbs(a.n, a.cpu_rows, target_s=max(2.0, 0.5 * a.steps))
     # each step: one matvec of the sample (bounded), reported as GB/s
     line = {"metric": METRIC, "value": gbs, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "warmup": a.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak" if a.replicas else "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload(a.n),
             "impl": "reference",
             "cpu_baseline": {"value": gbs, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample},
@@ -207,6 +211,7 @@ def build(n, storage, shard=None):
     if shard is not None:
         from hmatrix.shard import ShardedHmat
         S = ShardedHmat(prm, shard[0], shard[1])
+        S.H.shard = S
         return S.c, S.H, time.perf_counter() - t0
     c, H = hm.NewHmat(prm)
     return c, H, time.perf_counter() - t0
@@ -242,10 +247,12 @@ def measure(H, a, torch, dist, world, shard=False):
     sp = C.c_void_p(st.cuda_stream or 1)   # torch's default stream is cudaStreamLegacy
     flags = _lib.HM_FLAG_DEVICE_PTRS
 
+    from hmatrix.shard import gather_rows
+
     def step():
         _lib.check(L.hm_matvec(H._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), 1, 0, flags, sp))
         if shard:                            # every rank's rows -> the full H*x on every rank
-            dist.all_reduce(y)
+            gather_rows(y, H.shard.splits, H.shard.rank, dist)
 
     for _ in range(a.warmup):
         step()
@@ -289,7 +296,7 @@ def measure(H, a, torch, dist, world, shard=False):
             return
         xd.copy_(xh, non_blocking=True)
         _lib.check(L.hm_matvec(H._h, C.c_void_p(xd.data_ptr()), C.c_void_p(yd.data_ptr()), 1, 0, flags, sp))
-        dist.all_reduce(yd)
+        gather_rows(yd, H.shard.splits, H.shard.rank, dist)
         yh.copy_(yd, non_blocking=True)
         torch.cuda.synchronize()
     for _ in range(2):
@@ -618,9 +625,9 @@ def run_ours(a):
             cpu["single_thread"] = {"error": repr(e)[:300]}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "strong" if shard else "weak",
+            "scaling": "weak" if a.replicas else "strong",
             "vs_baseline": None, "dtype": a.storage, "data": "synthetic",
-            "config": dict(workload(a.n), storage=a.storage, parallelism=("%d row shards, NCCL all-reduce of y" % world) if shard
+            "config": dict(workload(a.n), storage=a.storage, parallelism=("%d row shards, NCCL all-gather of y" % world) if shard
                         else ("replicas" if world > 1 else "1 GPU")),
             "clocks": ck,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * a.n, "d2h_bytes_per_step": 8 * a.n,

@@ -1,6 +1,7 @@
 // C ABI of libhmatb200 (declared in include/hmatrix_b200.h).
 #include "hm_internal.h"
 
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -15,6 +16,10 @@ static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
 int fail(int code, const std::string& msg) {
   g_last_error = msg;
+  // a failed runtime call (an allocation that did not fit, for one) leaves its
+  // code as the thread's pending CUDA error; clear it, so that the next
+  // entry point's launch check does not report it a second time
+  if (code == HM_ERR_OOM || code == HM_ERR_CUDA) (void)cudaGetLastError();
   return code;
 }
 
@@ -52,8 +57,11 @@ int check_params(const hm_params* p) {
   if (p->kernel < HM_KERNEL_CAUCHY || p->kernel > HM_KERNEL_GAUSS_DP)
     return fail(HM_ERR_ARG, "unknown kernel id " + std::to_string(p->kernel) +
                                 "; Hparams.Kernel must map to HM_KERNEL_*");
-  if (!(p->kparam > 0.0) && p->kernel != HM_KERNEL_INVQUAD && p->kernel != HM_KERNEL_INVQUAD_DP)
-    return fail(HM_ERR_ARG, "kernel parameter must be > 0");
+  // > 0 for every kernel: 1/(c + |x-y|^2) with c <= 0 is infinite or negative
+  // where points meet, and the others divide by their parameter
+  if (!(p->kparam > 0.0) || !std::isfinite(p->kparam))
+    return fail(HM_ERR_ARG, "kernel parameter must be finite and > 0");
+  if (!std::isfinite(p->shift)) return fail(HM_ERR_NONFINITE, "shift is not finite");
   if (p->max_rank < 1 || p->max_rank > 64) return fail(HM_ERR_ARG, "MaxRank must be in [1, 64]");
   if (p->min_block < 1) return fail(HM_ERR_ARG, "MinBlock must be >= 1");
   if (p->cons_method != HM_CONS_ACA2 && p->cons_method != HM_CONS_SVD && p->cons_method != HM_CONS_BBFMM)
@@ -173,6 +181,12 @@ int hm_new(const hm_params* p, int64_t n, const double* geom, int64_t ncluster, 
   HM_TRY(check_params(p));
   if (n < 1 || !geom || ncluster < 1 || !cl_s || !cl_e || !cl_left || !cl_right)
     return fail(HM_ERR_ARG, "invalid geometry or cluster arrays");
+  // a NaN or infinite coordinate would make every kernel value of its row and
+  // column non-finite; refuse it before anything reaches the device
+  for (int64_t i = 0; i < n * (int64_t)p->dim; ++i)
+    if (!std::isfinite(geom[i]))
+      return fail(HM_ERR_NONFINITE, "geometry: coordinate " + std::to_string(i / n) + " of point " +
+                                        std::to_string(i % n) + " is not finite");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(HM_ERR_CUDA, "no CUDA device: the H-matrix path has no CPU fallback");
@@ -236,6 +250,30 @@ int hm_info(const hm_handle* h, hm_info_t* o) {
   o->n_row_groups = h->fwd.nwin;
   o->factorized = h->factorized ? 1 : 0;
   if (h->lu) lu_describe(h, &o->lu_tiles, &o->lu_rank_cap);
+  return HM_OK;
+}
+
+int hm_partition(const hm_params* p, int64_t n, int64_t ncluster, const int64_t* cl_s, const int64_t* cl_e,
+                 const int64_t* cl_left, const int64_t* cl_right, int64_t n_nb, const int64_t* nb_pairs,
+                 int64_t cap, int64_t* out, int64_t* count) {
+  HM_TRY(check_params(p));
+  if (!count || n < 1 || ncluster < 1 || !cl_s || !cl_e || !cl_left || !cl_right)
+    return fail(HM_ERR_ARG, "invalid cluster arrays");
+  hm_handle h;
+  h.prm = *p;
+  if (h.prm.max_block == -1) h.prm.max_block = (int32_t)(n / 4);   // src/cluster.jl:37-39
+  h.n = n;
+  h.dim = p->dim;
+  HM_TRY(partition_only(&h, ncluster, cl_s, cl_e, cl_left, cl_right, n_nb, nb_pairs));
+  *count = (int64_t)h.leaves.size();
+  if (!out) return HM_OK;
+  if (cap < *count) return fail(HM_ERR_ARG, "leaf buffer too small");
+  for (size_t i = 0; i < h.leaves.size(); ++i) {
+    const Leaf& L = h.leaves[i];
+    int64_t* o = out + 5 * i;
+    o[0] = L.type == T_DENSE ? 0 : 1;
+    o[1] = L.row0; o[2] = L.col0; o[3] = L.m; o[4] = L.n;
+  }
   return HM_OK;
 }
 

@@ -132,6 +132,56 @@ void enumerate_leaves(hm_handle* h) {
   }
 }
 
+int make_nbset(int64_t ncl, int64_t n_nb, const int64_t* nb_pairs, NbSet& nb) {
+  nb.ncl = ncl;
+  if (nb_pairs != nullptr) {
+    nb.identity = false;
+    nb.pairs.reserve((size_t)n_nb * 2);
+    for (int64_t i = 0; i < n_nb; ++i) {
+      int64_t a = nb_pairs[2 * i], b = nb_pairs[2 * i + 1];
+      if (a < 0 || b < 0 || a >= ncl || b >= ncl) return fail(HM_ERR_ARG, "neighbour pair out of range");
+      nb.pairs.insert((uint64_t)a * (uint64_t)ncl + (uint64_t)b);
+    }
+  }
+  return HM_OK;
+}
+
+// The block tree level by level (src/cluster.jl:48-133), then the leaves in
+// the reference's order.  decide(undecided) settles the "svd" route's
+// candidates (their type needs a compression); the other routes have none.
+template <typename Decide>
+int partition_levels(hm_handle* h, const NbSet& nb, Decide decide) {
+  h->nodes.clear();
+  h->nodes.push_back(Node{T_H, 0, 0, {-1, -1, -1, -1}, -1});
+  std::vector<int32_t> level{0};
+  while (!level.empty()) {
+    std::vector<int32_t> undecided;
+    for (int32_t id : level) {
+      int ty = classify(h, nb, h->nodes[id].s, h->nodes[id].t);
+      if (ty < 0) undecided.push_back(id);
+      else h->nodes[id].type = (int8_t)ty;
+    }
+    if (!undecided.empty()) HM_TRY(decide(undecided));
+    std::vector<int32_t> next;
+    for (int32_t id : level) {
+      if (h->nodes[id].type != T_H) continue;
+      int32_t s = h->nodes[id].s, t = h->nodes[id].t;
+      int32_t sl = (int32_t)h->cl_left[s], sr = (int32_t)h->cl_right[s];
+      int32_t tl = (int32_t)h->cl_left[t], tr = (int32_t)h->cl_right[t];
+      int32_t cs[4][2] = {{sl, tl}, {sl, tr}, {sr, tl}, {sr, tr}};
+      for (int c = 0; c < 4; ++c) {
+        int32_t cid = (int32_t)h->nodes.size();
+        h->nodes.push_back(Node{T_H, cs[c][0], cs[c][1], {-1, -1, -1, -1}, -1});
+        h->nodes[id].child[c] = cid;
+        next.push_back(cid);
+      }
+    }
+    level.swap(next);
+  }
+  enumerate_leaves(h);
+  return HM_OK;
+}
+
 template <typename T>
 int upload(T** dptr, const std::vector<T>& v, cudaStream_t st) {
   if (v.empty()) { *dptr = nullptr; return HM_OK; }
@@ -166,65 +216,30 @@ int build_handle(hm_handle* h, const double* geom, int64_t ncl, const int64_t* c
   HM_TRY(validate_tree(h, ncl));
 
   NbSet nb;
-  nb.ncl = ncl;
-  if (nb_pairs != nullptr) {
-    nb.identity = false;
-    nb.pairs.reserve((size_t)n_nb * 2);
-    for (int64_t i = 0; i < n_nb; ++i) {
-      int64_t a = nb_pairs[2 * i], b = nb_pairs[2 * i + 1];
-      if (a < 0 || b < 0 || a >= ncl || b >= ncl) return fail(HM_ERR_ARG, "neighbour pair out of range");
-      nb.pairs.insert((uint64_t)a * (uint64_t)ncl + (uint64_t)b);
-    }
-  }
+  HM_TRY(make_nbset(ncl, n_nb, nb_pairs, nb));
 
   HM_CUDA_TRY(cudaMalloc((void**)&h->d_geom, sizeof(double) * n * h->dim));
   HM_CUDA_TRY(cudaMemcpyAsync(h->d_geom, geom, sizeof(double) * n * h->dim, cudaMemcpyHostToDevice,
                               h->stream));
 
   // ---- partition, level by level ------------------------------------------
-  h->nodes.clear();
-  h->nodes.push_back(Node{T_H, 0, 0, {-1, -1, -1, -1}, -1});
-  std::vector<int32_t> level{0};
   SvdCandidateStore svd_store;   // factors of "svd"-route low-rank leaves
-  while (!level.empty()) {
-    std::vector<int32_t> undecided;
-    for (int32_t id : level) {
-      int ty = classify(h, nb, h->nodes[id].s, h->nodes[id].t);
-      if (ty < 0) undecided.push_back(id);
-      else h->nodes[id].type = (int8_t)ty;
+  HM_TRY(partition_levels(h, nb, [&](const std::vector<int32_t>& undecided) -> int {
+    // "svd" route: dense block + compress + (rank <= MaxRank) (cluster.jl:99-107)
+    std::vector<int64_t> r0, c0;
+    std::vector<int32_t> mm, nn;
+    for (int32_t id : undecided) {
+      r0.push_back(h->cl_s[h->nodes[id].s]);
+      c0.push_back(h->cl_s[h->nodes[id].t]);
+      mm.push_back((int32_t)csize(h, h->nodes[id].s));
+      nn.push_back((int32_t)csize(h, h->nodes[id].t));
     }
-    if (!undecided.empty()) {
-      // "svd" route: dense block + compress + (rank <= MaxRank) (cluster.jl:99-107)
-      std::vector<int64_t> r0, c0;
-      std::vector<int32_t> mm, nn;
-      for (int32_t id : undecided) {
-        r0.push_back(h->cl_s[h->nodes[id].s]);
-        c0.push_back(h->cl_s[h->nodes[id].t]);
-        mm.push_back((int32_t)csize(h, h->nodes[id].s));
-        nn.push_back((int32_t)csize(h, h->nodes[id].t));
-      }
-      std::vector<int32_t> ranks;
-      HM_TRY(svd_compress_candidates(h, r0, c0, mm, nn, ranks, svd_store, undecided));
-      for (size_t i = 0; i < undecided.size(); ++i)
-        h->nodes[undecided[i]].type = (ranks[i] <= p.max_rank) ? T_RK : T_H;
-    }
-    std::vector<int32_t> next;
-    for (int32_t id : level) {
-      if (h->nodes[id].type != T_H) continue;
-      int32_t s = h->nodes[id].s, t = h->nodes[id].t;
-      int32_t sl = (int32_t)h->cl_left[s], sr = (int32_t)h->cl_right[s];
-      int32_t tl = (int32_t)h->cl_left[t], tr = (int32_t)h->cl_right[t];
-      int32_t cs[4][2] = {{sl, tl}, {sl, tr}, {sr, tl}, {sr, tr}};
-      for (int c = 0; c < 4; ++c) {
-        int32_t cid = (int32_t)h->nodes.size();
-        h->nodes.push_back(Node{T_H, cs[c][0], cs[c][1], {-1, -1, -1, -1}, -1});
-        h->nodes[id].child[c] = cid;
-        next.push_back(cid);
-      }
-    }
-    level.swap(next);
-  }
-  enumerate_leaves(h);
+    std::vector<int32_t> ranks;
+    HM_TRY(svd_compress_candidates(h, r0, c0, mm, nn, ranks, svd_store, undecided));
+    for (size_t i = 0; i < undecided.size(); ++i)
+      h->nodes[undecided[i]].type = (ranks[i] <= p.max_rank) ? T_RK : T_H;
+    return HM_OK;
+  }));
 
   // ---- a shard: only the leaves of rows [row_lo, row_hi) ------------------
   if (p.row_hi > p.row_lo) {
@@ -307,6 +322,23 @@ int build_handle(hm_handle* h, const double* geom, int64_t ncl, const int64_t* c
   (void)eb;
   HM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return HM_OK;
+}
+
+// The leaves of the block partition alone, on the host (no device is used):
+// the aca2 and bbfmm routes decide every block from the tree and the
+// adjacency; the svd route needs a compression per candidate and is refused.
+int partition_only(hm_handle* h, int64_t ncl, const int64_t* cl_s, const int64_t* cl_e, const int64_t* cl_left,
+                   const int64_t* cl_right, int64_t n_nb, const int64_t* nb_pairs) {
+  h->cl_s.assign(cl_s, cl_s + ncl);
+  h->cl_e.assign(cl_e, cl_e + ncl);
+  h->cl_left.assign(cl_left, cl_left + ncl);
+  h->cl_right.assign(cl_right, cl_right + ncl);
+  HM_TRY(validate_tree(h, ncl));
+  NbSet nb;
+  HM_TRY(make_nbset(ncl, n_nb, nb_pairs, nb));
+  return partition_levels(h, nb, [](const std::vector<int32_t>&) -> int {
+    return fail(HM_ERR_UNSUPPORTED, "the svd route decides its blocks by compressing them on the device");
+  });
 }
 
 // ---------------------------------------------------------------------------

@@ -240,6 +240,8 @@ int build_handle(hm_handle* h, const double* geom, int64_t ncluster,
                  const int64_t* cl_s, const int64_t* cl_e, const int64_t* cl_left,
                  const int64_t* cl_right, int64_t n_nb, const int64_t* nb_pairs);
 int build_matvec_plans(hm_handle* h);
+int partition_only(hm_handle* h, int64_t ncl, const int64_t* cl_s, const int64_t* cl_e, const int64_t* cl_left,
+                   const int64_t* cl_right, int64_t n_nb, const int64_t* nb_pairs);
 int build_mv_descriptors(hm_handle* h, const std::vector<int64_t>& order, int trans);
 void free_mv_plan(MvPlan& p);
 int leaf_factors_f64(const hm_handle* h, int64_t leaf, double* A, double* B);

@@ -488,6 +488,10 @@ __global__ void pack_rk_kernel(const double* __restrict__ A, const double* __res
 int SvdCandidateStore::write_pool(hm_handle* h, const std::vector<int64_t>& rk_leaf) const {
   const int eb = elem_bytes(h->storage);
   double* dA = nullptr;
+  struct Guard {
+    double** p;
+    ~Guard() { if (*p) cudaFree(*p); }
+  } guard{&dA};
   size_t cap = 0;
   for (int64_t li : rk_leaf) {
     const Leaf& L = h->leaves[li];
@@ -498,6 +502,7 @@ int SvdCandidateStore::write_pool(hm_handle* h, const std::vector<int64_t>& rk_l
     size_t need = (f.A.size() + f.B.size()) * sizeof(double);
     if (need > cap) {
       if (dA) cudaFree(dA);
+      dA = nullptr;
       HM_CUDA_TRY(cudaMalloc(&dA, need));
       cap = need;
     }
@@ -508,7 +513,6 @@ int SvdCandidateStore::write_pool(hm_handle* h, const std::vector<int64_t>& rk_l
     HM_CUDA_TRY(cudaGetLastError());
     HM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   }
-  if (dA) cudaFree(dA);
   return HM_OK;
 }
 
@@ -521,6 +525,11 @@ int aca_fp_host(const double* A, double* U, double* V, int m, int n, double eps,
   double *dR = nullptr, *dU = nullptr, *dV = nullptr;
   int32_t* dk = nullptr;
   AcaFpJob* dj = nullptr;
+  // every return below, early error returns included, frees what was allocated
+  struct Guard {
+    void** p[5];
+    ~Guard() { for (void** q : p) if (*q) cudaFree(*q); }
+  } guard{{(void**)&dR, (void**)&dU, (void**)&dV, (void**)&dk, (void**)&dj}};
   HM_CUDA_TRY(cudaMalloc(&dR, 8ull * m * n));
   HM_CUDA_TRY(cudaMalloc(&dU, 8ull * m * cap));
   HM_CUDA_TRY(cudaMalloc(&dV, 8ull * n * cap));
@@ -558,7 +567,6 @@ int aca_fp_host(const double* A, double* U, double* V, int m, int n, double eps,
     HM_CUDA_TRY(cudaMemcpy(U, dU, 8ull * m * M, cudaMemcpyDeviceToHost));
     HM_CUDA_TRY(cudaMemcpy(V, dV, 8ull * n * M, cudaMemcpyDeviceToHost));
   }
-  cudaFree(dR); cudaFree(dU); cudaFree(dV); cudaFree(dk); cudaFree(dj);
   *out_rank = r;
   return HM_OK;
 }

@@ -200,8 +200,9 @@ __global__ void __launch_bounds__(32) lu_getrf_small_kernel(View C, int64_t* __r
       if (a > best) { best = a; bi = i; bv = S[i + j * LD]; }
     }
     warp_argmax(best, bi, bv);
-    if (lane == 0 && !(bv != 0.0)) atomicOr(flags, 4);
-    const int p = (int)bi;
+    if (lane == 0 && !(bv != 0.0)) atomicOr(flags, bi == INT64_MAX ? 6 : 4);
+    // every candidate NaN: no maximum was found; keep the row (flagged above)
+    const int p = bi == INT64_MAX ? j : (int)bi;
     if (p != j) {
       for (int c = lane; c < m; c += 32) {
         const double t = S[j + c * LD];
@@ -252,8 +253,9 @@ __global__ void __launch_bounds__(256) lu_getrf_kernel(View C, int64_t* __restri
       }
       warp_argmax(best, bi, bv);
       if (threadIdx.x == 0) {
-        s_piv = (int)bi;
-        if (!(bv != 0.0)) atomicOr(flags, 4);        // exactly zero (or NaN) pivot
+        // every candidate NaN: no maximum was found; keep the row
+        s_piv = bi == INT64_MAX ? j : (int)bi;
+        if (!(bv != 0.0)) atomicOr(flags, bi == INT64_MAX ? 6 : 4);   // exactly zero (or NaN) pivot
       }
     }
     __syncthreads();

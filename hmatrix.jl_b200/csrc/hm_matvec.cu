@@ -6,7 +6,11 @@
 //          with 16-byte loads and writes z = F1' x_seg (k values) to z[].
 // Phase 2: one CTA per window of 1024 output rows; each lane owns 4 rows and
 //          accumulates sum_r F2[:,r] z_r over the low-rank leaves and C x_seg
-//          over the dense leaves that cover its rows, in FP64, and stores y.
+//          over the dense leaves that cover its rows, and stores y.
+// FP64 factors are accumulated in FP64.  FP32 and BF16 factors are
+// multiplied and summed in FP32 over the few vectors (phase 1) or entries
+// (phase 2) a lane has in flight, and those FP32 partial sums are added in
+// FP64: one conversion per group instead of one per element.
 // The input is staged as 16-byte aligned shifted copies so that every
 // x-segment load in phase 1 is a vector load, whatever the segment start.
 #include "hm_internal.h"
@@ -41,11 +45,12 @@ template <> struct MvT<float> {
   struct XV { float4 a; };
   __device__ static R ld(const float* p) { return __ldcs(reinterpret_cast<const float4*>(p)); }
   __device__ static XV ldx(const float* p) { return XV{__ldg(reinterpret_cast<const float4*>(p))}; }
-  __device__ static double dot(const R& f, const XV& x, double s) {
-    s = fma((double)f.x, (double)x.a.x, s);
-    s = fma((double)f.y, (double)x.a.y, s);
-    s = fma((double)f.z, (double)x.a.z, s);
-    return fma((double)f.w, (double)x.a.w, s);
+  // FP32 partial sum of one vector (the caller folds it into its FP64 sum)
+  __device__ static float dotf(const R& f, const XV& x, float s) {
+    s = fmaf(f.x, x.a.x, s);
+    s = fmaf(f.y, x.a.y, s);
+    s = fmaf(f.z, x.a.z, s);
+    return fmaf(f.w, x.a.w, s);
   }
 };
 __device__ __forceinline__ float bf_lo(uint32_t w) { return __uint_as_float(w << 16); }
@@ -59,15 +64,16 @@ template <> struct MvT<__nv_bfloat16> {
   __device__ static XV ldx(const float* p) {
     return XV{__ldg(reinterpret_cast<const float4*>(p)), __ldg(reinterpret_cast<const float4*>(p) + 1)};
   }
-  __device__ static double dot(const R& f, const XV& x, double s) {
-    s = fma((double)bf_lo(f.x), (double)x.a.x, s);
-    s = fma((double)bf_hi(f.x), (double)x.a.y, s);
-    s = fma((double)bf_lo(f.y), (double)x.a.z, s);
-    s = fma((double)bf_hi(f.y), (double)x.a.w, s);
-    s = fma((double)bf_lo(f.z), (double)x.b.x, s);
-    s = fma((double)bf_hi(f.z), (double)x.b.y, s);
-    s = fma((double)bf_lo(f.w), (double)x.b.z, s);
-    return fma((double)bf_hi(f.w), (double)x.b.w, s);
+  // BF16 -> FP32 is a shift of the bits; FP32 partial sum of one vector
+  __device__ static float dotf(const R& f, const XV& x, float s) {
+    s = fmaf(bf_lo(f.x), x.a.x, s);
+    s = fmaf(bf_hi(f.x), x.a.y, s);
+    s = fmaf(bf_lo(f.y), x.a.z, s);
+    s = fmaf(bf_hi(f.y), x.a.w, s);
+    s = fmaf(bf_lo(f.z), x.b.x, s);
+    s = fmaf(bf_hi(f.z), x.b.y, s);
+    s = fmaf(bf_lo(f.w), x.b.z, s);
+    return fmaf(bf_hi(f.w), x.b.w, s);
   }
 };
 
@@ -123,12 +129,27 @@ __global__ void __launch_bounds__(256, HM_P1_MINB) mv_phase1_kernel(const P1Desc
             xv[u] = Tr::ldx(xb + (int64_t)v * VW);
           }
         }
+        if constexpr (std::is_same<T, double>::value) {
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-          if (v0 + 32 * u < nvec) {
-            s0 = Tr::dot(a[u], xv[u], s0);
-            s1 = Tr::dot(c[u], xv[u], s1);
+          for (int u = 0; u < U; ++u) {
+            if (v0 + 32 * u < nvec) {
+              s0 = Tr::dot(a[u], xv[u], s0);
+              s1 = Tr::dot(c[u], xv[u], s1);
+            }
           }
+        } else {
+          // FP32 products and partial sums over the U vectors in flight (16
+          // elements a lane), folded into the FP64 sums once per group
+          float f0 = 0.f, f1 = 0.f;
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            if (v0 + 32 * u < nvec) {
+              f0 = Tr::dotf(a[u], xv[u], f0);
+              f1 = Tr::dotf(c[u], xv[u], f1);
+            }
+          }
+          s0 += (double)f0;
+          s1 += (double)f1;
         }
       }
       s0 = warp_sum(s0);
@@ -184,6 +205,7 @@ template <> struct Row4<float> {                // dense leaves: float
     if (q == 0) r.x = v; else if (q == 1) r.y = v; else if (q == 2) r.z = v; else r.w = v;
   }
   __device__ static void cvt(const Raw& r, bool, double (&v)[4]) { v[0] = r.x; v[1] = r.y; v[2] = r.z; v[3] = r.w; }
+  __device__ static void cvtf(const Raw& r, bool, float (&v)[4]) { v[0] = r.x; v[1] = r.y; v[2] = r.z; v[3] = r.w; }
 };
 template <> struct Row4<__nv_bfloat16> {        // dense leaves: float (raw float bits)
   static constexpr int U = 8;
@@ -208,6 +230,14 @@ template <> struct Row4<__nv_bfloat16> {        // dense leaves: float (raw floa
     else r.y = (r.y & 0x0000ffffu) | (b << 16);
   }
   __device__ static void cvt(const Raw& r, bool dense, double (&v)[4]) {
+    if (dense) {
+      v[0] = __uint_as_float(r.x); v[1] = __uint_as_float(r.y);
+      v[2] = __uint_as_float(r.z); v[3] = __uint_as_float(r.w);
+    } else {
+      v[0] = bf_lo(r.x); v[1] = bf_hi(r.x); v[2] = bf_lo(r.y); v[3] = bf_hi(r.y);
+    }
+  }
+  __device__ static void cvtf(const Raw& r, bool dense, float (&v)[4]) {
     if (dense) {
       v[0] = __uint_as_float(r.x); v[1] = __uint_as_float(r.y);
       v[2] = __uint_as_float(r.z); v[3] = __uint_as_float(r.w);
@@ -324,12 +354,28 @@ __global__ void __launch_bounds__(P2_WARPS * 32) mv_phase2_kernel(const MvWin* _
             }
           }
         }
+        if constexpr (std::is_same<T, double>::value) {
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-          double v[4];
-          Row4<T>::cvt(raw[u], isd[u], v);
+          for (int u = 0; u < U; ++u) {
+            double v[4];
+            Row4<T>::cvt(raw[u], isd[u], v);
 #pragma unroll
-          for (int q = 0; q < 4; ++q) acc[q] = fma(v[q], zz[u], acc[q]);
+            for (int q = 0; q < 4; ++q) acc[q] = fma(v[q], zz[u], acc[q]);
+          }
+        } else {
+          // FP32 products and partial sums over the U entries in flight,
+          // folded into the FP64 row sums once per group
+          float part[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            float v[4];
+            Row4<T>::cvtf(raw[u], isd[u], v);
+            const float zf = (float)zz[u];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) part[q] = fmaf(v[q], zf, part[q]);
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[q] += (double)part[q];
         }
       }
     }

@@ -21,7 +21,10 @@
 //    same time) race on the array and must be serialised by the caller;
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress while that device is current; make that first call
-//    before any stream capture begins.
+//    before any stream capture begins.  The address is kept until the process
+//    exits, so a cudaDeviceReset on that device ends the use of this entry
+//    point;
+//  * each call copies the rank back to the host and waits for its stream.
 #include "hm_internal.h"
 #include "hm_lowrank.cuh"
 

@@ -342,6 +342,9 @@ def NewHmat(prm: Params = None):
     if X.ndim == 1:
         X = X.reshape(-1, 1)
     n, d = X.shape
+    if not np.all(np.isfinite(X)):
+        # the library refuses such geometry too; KMeans would fail first here
+        raise HmError(_lib.HM_ERR_NONFINITE, "Hparams.Geom holds a non-finite coordinate")
     if prm.MaxBlock == -1:
         prm.MaxBlock = n // 4                          # src/cluster.jl:37-39
     c = construct_cluster(X, prm.MinBlock, prm.Tree)

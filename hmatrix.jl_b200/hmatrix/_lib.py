@@ -30,7 +30,7 @@ STATUS_NAMES = {
 
 # every symbol include/hmatrix_b200.h declares
 EXPORTED = [
-    "hm_version", "hm_last_error", "hm_default_params", "hm_new", "hm_destroy", "hm_info",
+    "hm_version", "hm_last_error", "hm_default_params", "hm_new", "hm_partition", "hm_destroy", "hm_info",
     "hm_leaves", "hm_leaf_factors", "hm_to_dense", "hm_matvec", "hm_matvec_profile", "hm_exact_rows",
     "hm_add_identity", "hm_scale", "hm_copy", "hm_coarsen", "hm_add", "hm_save", "hm_load", "hm_load_user", "hm_lu", "hm_lu_perm", "hm_solve", "hm_solve_refined",
     "hm_batch_lu", "hm_batch_solve", "hm_batch_solve_refined", "hm_batch_matvec",
@@ -85,6 +85,8 @@ def lib():
     L.hm_default_params.argtypes = [C.POINTER(hm_params)]
     L.hm_new.argtypes = [C.POINTER(hm_params), C.c_int64, vp, C.c_int64, vp, vp, vp, vp, C.c_int64, vp,
                          C.POINTER(vp)]
+    L.hm_partition.argtypes = [C.POINTER(hm_params), C.c_int64, C.c_int64, vp, vp, vp, vp, C.c_int64, vp,
+                               C.c_int64, vp, p64]
     L.hm_destroy.argtypes = [vp]
     L.hm_info.argtypes = [vp, C.POINTER(hm_info_t)]
     L.hm_leaves.argtypes = [vp, C.c_int64, vp, p64]

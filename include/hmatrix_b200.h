@@ -145,6 +145,17 @@ int hm_new(const hm_params* p, int64_t n, const double* geom,
            const int64_t* cl_left, const int64_t* cl_right,
            int64_t n_nb, const int64_t* nb_pairs, hm_handle** out);
 
+/* The block partition of NewHmat alone (src/cluster.jl:48-133), computed on
+ * the host without a device: for leaf i in the reference's order,
+ * out[5i..5i+4] = (type 0 dense / 1 low-rank, row0, col0, m, n); *count
+ * receives the number of leaves (out may be NULL to ask for it).  Arguments
+ * as for hm_new.  The "svd" route decides its blocks by compressing them and
+ * is refused (HM_ERR_UNSUPPORTED).  Used to balance row shards over GPUs by
+ * the bytes they will store; no counterpart in the reference. */
+int hm_partition(const hm_params* p, int64_t n, int64_t ncluster, const int64_t* cl_s, const int64_t* cl_e,
+                 const int64_t* cl_left, const int64_t* cl_right, int64_t n_nb, const int64_t* nb_pairs,
+                 int64_t cap, int64_t* out, int64_t* count);
+
 /* free a handle */
 int hm_destroy(hm_handle* h);
 
@@ -286,12 +297,16 @@ int aca_wrapper(double* AA, double* UU, double* VV, int m, int n,
  * synchronisation an allocation implies).  No counterpart in the reference.
  * A (m x n), UU (m x min(m,n,rank+1)) and VV (n x min(m,n,rank+1)) are device
  * pointers on the current device, column-major; the result equals
- * aca_wrapper's and the untruncated rank is returned (negative status on
- * error).  The residual lives in a fixed device array of 2^18 - 32 doubles
- * shared by all calls: m*n + m + n must not exceed that (HM_ERR_ARG
- * otherwise), calls that overlap on the GPU race, and the first call on a
- * device (which looks the array up) should come before any stream capture.
- * stream: a cudaStream_t or NULL for the legacy default stream. */
+ * aca_wrapper's and the untruncated rank (at most min(m,n)) is returned
+ * (negative status on error).  The residual lives in a fixed device array of
+ * 2^18 - 32 doubles shared by all calls: m*n + m + n must not exceed that
+ * (HM_ERR_ARG otherwise), calls that overlap on the GPU race, and the first
+ * call on a device (which looks the array up) should come before any stream
+ * capture.  Each call reads the rank back to the host, so it returns only
+ * once `stream` has finished its work.  The looked-up address is kept until
+ * the process exits: do not use this entry point on a device across a
+ * cudaDeviceReset.  stream: a cudaStream_t or NULL for the legacy default
+ * stream. */
 int aca_wrapper_noalloc(const double* AA, double* UU, double* VV, int m, int n,
                         double epsilon, int rank, void* stream);
 

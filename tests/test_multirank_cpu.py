@@ -1,8 +1,12 @@
-"""The multi-GPU path of bench.py on CPU: world_size 2 over gloo.
+"""The multi-GPU paths on CPU: world_size 2 over gloo.
 
-`bench.py --gpus N` runs one replica of the H-matrix per rank (independent
-H-matrices, no exchange in the data path); the only collective is the max over
-ranks of the per-rank time, and the whole-job value counts every rank's bytes.
+`bench.py --gpus N` row-shards one H-matrix over the ranks (strong scaling):
+each rank multiplies its own rows and one all-gather of the row shards leaves
+H*x on every rank; the job time is the max over ranks.  `--replicas` runs N
+independent copies instead (weak scaling), and `--batch` splits independent
+problems over the ranks with no exchange.  These tests cover the timing
+reductions, the shard boundaries (never inside a leaf, balanced by bytes),
+the all-gather assembly and the problem split.
 """
 import os
 import socket
@@ -93,8 +97,9 @@ def test_row_splits_keep_leaves_whole():
 
 
 def _shard_worker(rank, world, port, out):
-    # the reduction that assembles H*x from the shards, over gloo: each rank
-    # contributes its rows of a dense product and zeros elsewhere
+    # the all-gather that assembles H*x from the shards, over gloo: each rank
+    # holds its rows of a dense product (garbage elsewhere), shards of unequal
+    # length, one vector and one block of 3 columns
     import datetime
     import sys
     import numpy as np
@@ -102,18 +107,21 @@ def _shard_worker(rank, world, port, out):
     import torch.distributed as dist
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     sys.path.insert(0, os.path.join(root, "hmatrix.jl_b200"))
-    from hmatrix.shard import reduce_rows
+    from hmatrix.shard import gather_rows
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     rng = np.random.default_rng(0)
     A = rng.standard_normal((40, 40))
-    x = rng.standard_normal(40)
+    x = rng.standard_normal((40, 3))
     b = [0, 17, 40]
-    y = torch.zeros(40, dtype=torch.float64)
-    y[b[rank]:b[rank + 1]] = torch.tensor(A[b[rank]:b[rank + 1]] @ x)
-    reduce_rows(y, dist)
-    out.put((rank, float(np.abs(y.numpy() - A @ x).max())))
+    err = 0.0
+    for X in (x[:, 0], x):
+        y = torch.full((40,) + X.shape[1:], float(rank + 7), dtype=torch.float64)
+        y[b[rank]:b[rank + 1]] = torch.tensor(A[b[rank]:b[rank + 1]] @ X)
+        gather_rows(y, b, rank, dist)
+        err = max(err, float(np.abs(y.numpy() - A @ X).max()))
+    out.put((rank, err))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -132,6 +140,59 @@ def test_shard_reduction_two_ranks():
         assert p.exitcode == 0
     for rank, err in res:
         assert err <= 1e-12
+
+
+def test_host_partition_matches_oracle():
+    # hm_partition (the library's host-side partition, no device) lists the
+    # same leaves in the same order as the oracle's partition of __c1
+    import sys
+    import numpy as np
+    import ctypes as C
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "hmatrix.jl_b200"))
+    import hmatrix as hm
+    from hmatrix.cluster import construct_cluster
+    from hmatrix.shard import partition_leaves
+    from oracle import hm_oracle_c as O
+    for G, mb, minb, tree in ((np.linspace(0, 10, 5000), 512, 64, "bisect"),
+                              (np.linspace(0, 10, 3000), 512, 64, "kmeans"),
+                              (np.random.default_rng(5).uniform(0, 1, (3000, 2)), 256, 32, "bisect")):
+        c = construct_cluster(G, minb, tree)
+        prm = hm.Params(Geom=G, Kernel=hm.Cauchy(1.0), MaxBlock=mb, MinBlock=minb, ConsMethod="aca2")
+        got = partition_leaves(prm, c)
+        s, e, l, r = (np.ascontiguousarray(a, np.int64) for a in (c.s, c.e, c.left, c.right))
+        L = O.lib()
+        n = int(c.e[0])
+        cnt = L.orc_partition(O._p(s), O._p(e), O._p(l), O._p(r), minb, mb, 0, n, 0, C.c_void_p(0))
+        lv = np.zeros((cnt, 5), np.int64)
+        L.orc_partition(O._p(s), O._p(e), O._p(l), O._p(r), minb, mb, 0, n, cnt, O._p(lv))
+        assert np.array_equal(got, lv)
+
+
+def test_byte_balanced_splits():
+    # on a 2-D tree the byte-balanced cut points give shards whose streamed
+    # bytes are closer to equal than the row-balanced ones, and never cut a leaf
+    import sys
+    import numpy as np
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "hmatrix.jl_b200"))
+    import hmatrix as hm
+    from hmatrix.cluster import construct_cluster
+    from hmatrix.shard import partition_leaves, row_bytes, row_splits
+    G = np.random.default_rng(7).uniform(0, 1, (20000, 2))
+    G[:6000] *= 0.2                                   # a dense corner: uneven rows
+    c = construct_cluster(G, 32, "bisect")
+    prm = hm.Params(Geom=G, Kernel=hm.Cauchy(1.0), MaxBlock=256, MinBlock=32, ConsMethod="aca2")
+    lv = partition_leaves(prm, c)
+    w = row_bytes(lv, 20000)
+    cw = np.concatenate([[0.0], np.cumsum(w)])
+    for world in (2, 4, 8):
+        br = row_splits(c, 256, world)
+        bb = row_splits(c, 256, world, w)
+        spread = lambda b: max(cw[b[i + 1]] - cw[b[i]] for i in range(world)) / (cw[-1] / world)
+        assert spread(bb) <= spread(br) + 1e-12
+        for t in bb[1:-1]:
+            assert not ((lv[:, 1] < t) & (lv[:, 1] + lv[:, 3] > t)).any()
 
 
 def test_split_problems_cover_and_balance():

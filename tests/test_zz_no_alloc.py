@@ -20,6 +20,10 @@ pytestmark = pytest.mark.gpu
 TOL = dict(rtol=1e-12, atol=1e-14)
 
 
+def _eps(A):
+    return 1e-3 if A.shape == (20, 20) else 1e-9
+
+
 def _noalloc(A, rank):
     import torch
     from hmatrix import _lib
@@ -30,8 +34,7 @@ def _noalloc(A, rank):
     dV = torch.full((keep * n,), np.nan, device="cuda", dtype=torch.float64)
     stream = torch.cuda.current_stream().cuda_stream or 1
     R = _lib.lib().aca_wrapper_noalloc(C.c_void_p(dA.data_ptr()), C.c_void_p(dU.data_ptr()),
-                                       C.c_void_p(dV.data_ptr()), m, n, 1e-3 if A.shape == (20, 20) else 1e-9,
-                                       rank, C.c_void_p(stream))
+                                       C.c_void_p(dV.data_ptr()), m, n, _eps(A), rank, C.c_void_p(stream))
     if R < 0:
         raise RuntimeError(_lib.last_error())
     M = min(R, rank + 1)
@@ -42,7 +45,7 @@ def _noalloc(A, rank):
 
 def _reference(A, rank):
     import hmatrix as hm
-    return hm.aca_wrapper(A, 1e-3 if A.shape == (20, 20) else 1e-9, rank)
+    return hm.aca_wrapper(A, _eps(A), rank)
 
 
 def _cases():
@@ -63,6 +66,34 @@ def test_noalloc_matches_allocating_entry_point_twice():
             assert R == Rr
             assert U.shape == Ur.shape and V.shape == Vr.shape
             assert np.allclose(U, Ur, **TOL) and np.allclose(V, Vr, **TOL)
+
+
+def _edge_cases():
+    rng = np.random.default_rng(12)
+    fat_nan = rng.standard_normal((40, 70))
+    fat_nan[7, 11] = np.nan
+    thin_nan = rng.standard_normal((90, 30))
+    thin_nan[50, 3] = np.nan
+    lowrank = rng.standard_normal((60, 4)) @ rng.standard_normal((4, 50))
+    return [
+        ("zero, fat", np.zeros((30, 50)), 4),          # every pivot below machine epsilon
+        ("zero, thin", np.zeros((50, 30)), 4),
+        ("NaN, fat", fat_nan, 6),                      # full-rank fallback, ACA_FullyPivoted.cpp:122-147
+        ("NaN, thin", thin_nan, 6),
+        ("rank 0", lowrank, 0),                        # only the first term is kept
+    ]
+
+
+@pytest.mark.parametrize("name,A,rank", _edge_cases(), ids=[c[0] for c in _edge_cases()])
+def test_noalloc_edge_cases_match_allocating_entry_point(name, A, rank):
+    # the sub-epsilon pivot branch (unit column, zero row), the NaN fallback
+    # (written on the device here, on the host by aca_wrapper) and rank = 0
+    Ur, Vr, Rr = _reference(A, rank)
+    for _ in range(2):
+        U, V, R = _noalloc(A, rank)
+        assert R == Rr, (name, R, Rr)
+        assert U.shape == Ur.shape and V.shape == Vr.shape
+        assert np.allclose(U, Ur, equal_nan=True, **TOL) and np.allclose(V, Vr, equal_nan=True, **TOL), name
 
 
 def test_noalloc_rejects_oversize():
