@@ -324,9 +324,11 @@ int hm_matvec(hm_handle* h, const double* X, double* Y, int64_t ncols, int32_t t
   cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
   const int64_t n = h->n;
   // one column: the single-vector kernels; a block: every factor streamed once per column block
+  // (FP32/BF16 factors: on the tensor cores unless HM_FLAG_MV_SIMT)
+  const bool simt = (flags & HM_FLAG_MV_SIMT) != 0;
   auto run = [&](const double* dx, double* dy) -> int {
     if (ncols == 1) return matvec_device(h, dx, dy, trans ? 1 : 0, st);
-    return matvec_multi_device(h, dx, dy, ncols, trans ? 1 : 0, st);
+    return matvec_multi_device(h, dx, dy, ncols, trans ? 1 : 0, st, simt);
   };
   if (ncols == 0) return HM_OK;
   if (flags & HM_FLAG_DEVICE_PTRS) return run(X, Y);
@@ -336,7 +338,20 @@ int hm_matvec(hm_handle* h, const double* X, double* Y, int64_t ncols, int32_t t
   HM_TRY(run(io.ptr, io.ptr + n * ncols));
   HM_CUDA_TRY(cudaMemcpyAsync(Y, io.ptr + n * ncols, sizeof(double) * n * ncols, cudaMemcpyDeviceToHost, st));
   HM_CUDA_TRY(cudaStreamSynchronize(st));
-  return HM_OK;
+  return tc_status(h, st);
+}
+
+int hm_tc_selftest(int32_t kind, int32_t a_mn, int32_t nc, const float* A, const float* B, float* D) {
+  if (!A || !B || !D) return fail(HM_ERR_ARG, "invalid argument");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(HM_ERR_CUDA, "no CUDA device");
+  return tc_selftest(kind, a_mn, nc, A, B, D);
+}
+
+int hm_status(hm_handle* h, void* stream) {
+  if (!h) return fail(HM_ERR_ARG, "invalid argument");
+  DeviceGuard g(h->device);
+  return tc_status(h, stream ? (cudaStream_t)stream : h->stream);
 }
 
 int hm_matvec_profile(hm_handle* h, const double* X, double* Y, int32_t trans, void* stream, float* ms) {

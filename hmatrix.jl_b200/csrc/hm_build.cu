@@ -464,6 +464,13 @@ void free_handle_data(hm_handle* h) {
   fr(h->d_io);
   fr(h->d_z);
   fr(h->d_xm);
+  fr(h->d_tc);
+  fr(h->d_tc_err);
+  free_tc_plan(h->tc_fwd);
+  free_tc_plan(h->tc_bwd);
+  h->d_tc = nullptr;
+  h->d_tc_err = nullptr;
+  h->tc_bytes = 0;
   free_mv_plan(h->fwd);
   free_mv_plan(h->bwd);
   h->d_geom = nullptr;

@@ -168,6 +168,7 @@ struct MvPlan {
 };
 
 struct LuState;            // H-LU data (hm_lu.cu)
+struct TcPlan;             // tensor-core multi-RHS matvec plan (hm_matvec_tc.cu)
 
 }  // namespace hm
 
@@ -209,6 +210,11 @@ struct hm_handle {
   size_t io_bytes = 0;
   void* d_xm = nullptr;            // multi-RHS matvec: row-major input block + phase-1 results
   size_t xm_bytes = 0;
+  hm::TcPlan* tc_fwd = nullptr;    // tensor-core multi-RHS plans (FP32/BF16 factors), built on first use
+  hm::TcPlan* tc_bwd = nullptr;
+  void* d_tc = nullptr;            // their X and Z tiles
+  size_t tc_bytes = 0;
+  int* d_tc_err = nullptr;         // error word of their bounded waits
 
   hm::LuState* lu = nullptr;       // set once factorised
   bool factorized = false;
@@ -265,7 +271,13 @@ int matvec_device(hm_handle* h, const double* d_x, double* d_y, int trans, cudaS
                   cudaEvent_t* ev = nullptr);
 // Y = H X (trans 0) or H' X (trans 1) for an n x ncols column-major block,
 // factors streamed once per column block (hm_matvec_multi.cu)
-int matvec_multi_device(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st);
+int matvec_multi_device(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st,
+                        bool simt = false);
+// the low-rank part of Y = H X on the tensor cores, added into Y (hm_matvec_tc.cu)
+int matvec_multi_tc(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st);
+int tc_status(hm_handle* h, cudaStream_t st);
+int tc_selftest(int kind, int a_mn, int nc, const float* A, const float* B, float* D);
+void free_tc_plan(TcPlan*& p);
 int exact_rows_device(hm_handle* h, const int64_t* d_rows, int64_t nrows,
                       const double* d_x, double* d_y, cudaStream_t st);
 

@@ -265,7 +265,9 @@ template <int CB> struct M2Cfg {
   static constexpr int EMAX = CB >= 16 ? 256 : 512;   // entries per sub-round (z rows in shared memory)
 };
 
-template <typename T, typename TD, int CB>
+// DENSE_ONLY: the dense leaves alone (the low-rank part is added afterwards
+// by the tensor-core kernels)
+template <typename T, typename TD, int CB, bool DENSE_ONLY = false>
 __global__ void __launch_bounds__(M2_THREADS) mvm_phase2_kernel(const MvWin* __restrict__ win,
                                                                 const P2Desc* __restrict__ d,
                                                                 const T* __restrict__ rk, const TD* __restrict__ dn,
@@ -302,6 +304,7 @@ __global__ void __launch_bounds__(M2_THREADS) mvm_phase2_kernel(const MvWin* __r
         const int r0 = sd[lane].row_off, r1 = r0 + (int)sd[lane].m;
         const int h0 = (int)(wh & 1) * (2 * M2_THREADS);
         cnt = (r1 > h0 && r0 < h0 + 2 * M2_THREADS) ? (int)sd[lane].cnt : 0;
+        if (DENSE_ONLY && sd[lane].type == P2_RK) cnt = 0;
       }
       int incl = cnt;
 #pragma unroll
@@ -445,14 +448,16 @@ static int ensure_sorted_p1(MvPlan& P) {
 }
 
 template <typename T, int CB>
-int launch_multi(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st) {
+int launch_multi(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st,
+                 bool dense_only = false) {
   using TD = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
   MvPlan& P = trans ? h->bwd : h->fwd;
-  HM_TRY(ensure_sorted_p1(P));
+  if (!dense_only) HM_TRY(ensure_sorted_p1(P));
   const int ld = (int)pad_to(ncols, CB);
   const int ncb = ld / CB;
   const size_t xr_bytes = sizeof(double) * (size_t)(h->n + 2) * ld;
-  const size_t zr_bytes = sizeof(double) * (size_t)std::max<int64_t>(h->zlen, 1) * ld;
+  // the dense-only pass needs no phase-1 results
+  const size_t zr_bytes = dense_only ? 0 : sizeof(double) * (size_t)std::max<int64_t>(h->zlen, 1) * ld;
   if (h->xm_bytes < xr_bytes + zr_bytes) {
     if (h->d_xm) cudaFree(h->d_xm);
     h->d_xm = nullptr;
@@ -469,6 +474,14 @@ int launch_multi(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, in
     const unsigned g = (unsigned)std::min<int64_t>((tot + 255) / 256, (int64_t)nsm * 16);
     mvm_xr_kernel<<<g, 256, 0, st>>>(d_x, h->n, h->n, (int)ncols, xr, ld);
   }
+  const int64_t nblk = (int64_t)P.nwin * 2 * ncb;
+  if (nblk > (int64_t)INT32_MAX) return fail(HM_ERR_UNSUPPORTED, "too many phase-2 blocks");
+  if (dense_only) {
+    mvm_phase2_kernel<T, TD, CB, true><<<(unsigned)nblk, M2_THREADS, 0, st>>>(
+        P.d_win, P.d_p2, (const T*)h->d_rk, (const TD*)h->d_dense, zr, xr, ld, ncb, d_y, h->n, (int)ncols);
+    HM_CUDA_TRY(cudaGetLastError());
+    return HM_OK;
+  }
   const size_t seg_smem = sizeof(double) * (size_t)P.maxlen1 * (CB + 2);
   if (P.np1 > 0 && seg_smem <= 96 * 1024 && P.nt1 * ncb <= (int64_t)INT32_MAX) {
     HM_CUDA_TRY(smem_attr((const void*)mvm_phase1_seg_kernel<T, CB>, 96 * 1024));
@@ -480,8 +493,6 @@ int launch_multi(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, in
     mvm_phase1_kernel<T, CB><<<(unsigned)blocks, 256, 0, st>>>(P.d_p1s, P.d_g1s, P.ng1, (const T*)h->d_rk, xr, ld,
                                                               ncb, zr);
   }
-  const int64_t nblk = (int64_t)P.nwin * 2 * ncb;
-  if (nblk > (int64_t)INT32_MAX) return fail(HM_ERR_UNSUPPORTED, "too many phase-2 blocks");
   mvm_phase2_kernel<T, TD, CB><<<(unsigned)nblk, M2_THREADS, 0, st>>>(
       P.d_win, P.d_p2, (const T*)h->d_rk, (const TD*)h->d_dense, zr, xr, ld, ncb, d_y, h->n, (int)ncols);
   HM_CUDA_TRY(cudaGetLastError());
@@ -489,21 +500,33 @@ int launch_multi(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, in
 }
 
 template <typename T>
-int multi_t(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st) {
-  if (ncols <= 4) return launch_multi<T, 4>(h, d_x, d_y, ncols, trans, st);
-  if (ncols <= 8) return launch_multi<T, 8>(h, d_x, d_y, ncols, trans, st);
-  return launch_multi<T, 16>(h, d_x, d_y, ncols, trans, st);
+int multi_t(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st,
+            bool dense_only = false) {
+  if (ncols <= 4) return launch_multi<T, 4>(h, d_x, d_y, ncols, trans, st, dense_only);
+  if (ncols <= 8) return launch_multi<T, 8>(h, d_x, d_y, ncols, trans, st, dense_only);
+  return launch_multi<T, 16>(h, d_x, d_y, ncols, trans, st, dense_only);
 }
 
 }  // namespace
 
-int matvec_multi_device(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st) {
+// FP64 factors (no tensor-core kind for FP64), or simt: the CUDA-core block
+// kernels for the whole product.  FP32/BF16 factors: the dense leaves on the
+// CUDA cores (they write every row of Y), then the low-rank part on the
+// tensor cores (added into Y).
+int matvec_multi_device(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st,
+                        bool simt) {
   if (ncols <= 0) return HM_OK;
   if ((h->n + 2) * pad_to(ncols, 16) > (int64_t)1 << 40) return fail(HM_ERR_UNSUPPORTED, "right-hand side block too large");
   switch (h->storage) {
     case HM_F64: return multi_t<double>(h, d_x, d_y, ncols, trans, st);
-    case HM_F32: return multi_t<float>(h, d_x, d_y, ncols, trans, st);
-    default: return multi_t<__nv_bfloat16>(h, d_x, d_y, ncols, trans, st);
+    case HM_F32:
+      if (simt) return multi_t<float>(h, d_x, d_y, ncols, trans, st);
+      HM_TRY(multi_t<float>(h, d_x, d_y, ncols, trans, st, true));
+      return matvec_multi_tc(h, d_x, d_y, ncols, trans, st);
+    default:
+      if (simt) return multi_t<__nv_bfloat16>(h, d_x, d_y, ncols, trans, st);
+      HM_TRY(multi_t<__nv_bfloat16>(h, d_x, d_y, ncols, trans, st, true));
+      return matvec_multi_tc(h, d_x, d_y, ncols, trans, st);
   }
 }
 

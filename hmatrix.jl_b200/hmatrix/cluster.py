@@ -5,8 +5,9 @@ random_state=0)`` (label 0 becomes the left child, both children keep the
 increasing index order of ``findall``), assigns ids in the pre-order of the
 downward pass and a cluster is a leaf once ``N <= MinBlock``.  ``method=
 "bisect"`` replaces KMeans by a median split of the widest coordinate, which
-is deterministic and fast at n = 2^20 (thousands of KMeans calls take
-minutes there).
+is deterministic and fast at n = 2^20.  The KMeans tree of a large n spends
+minutes in thousands of KMeans calls; below its top levels the subtrees are
+independent and go to a pool of host processes.
 """
 from __future__ import annotations
 
@@ -50,14 +51,32 @@ def _split_bisect(X):
     return np.sort(order[:h]), np.sort(order[h:])
 
 
-def construct_cluster(Geom, Nleaf, method="kmeans"):
-    """Build the cluster tree; returns a :class:`Cluster` root."""
+def construct_cluster(Geom, Nleaf, method="kmeans", workers=None):
+    """Build the cluster tree; returns a :class:`Cluster` root.
+
+    ``workers``: host processes for the KMeans tree (None: up to 16 when n is
+    above 32768, else 1).  Every split is the same single-threaded KMeans call
+    whichever process makes it, so the tree does not depend on ``workers``."""
     X = np.asarray(Geom, dtype=np.float64)
     if X.ndim == 1:
         X = X.reshape(-1, 1)
     n = X.shape[0]
     if method == "bisect" and X.shape[1] == 1 and n > 1 and np.all(np.diff(X[:, 0]) >= 0):
         return _bisect_sorted_1d(X, Nleaf)
+    if method == "kmeans":
+        if workers is None:
+            import os
+            workers = min(16, os.cpu_count() or 1) if n > 32768 else 1
+        if workers > 1:
+            return _kmeans_parallel(X, Nleaf, workers)
+    s, e, left, right, perm = _build_tree(X, Nleaf, method)
+    return Cluster(X[perm], perm, s, e, left, right)
+
+
+def _build_tree(X, Nleaf, method):
+    """The downward pass of src/cluster.jl:223-240 on X: flattened arrays in
+    pre-order (ids 0..) and the permutation."""
+    n = X.shape[0]
     split = _split_kmeans if method == "kmeans" else _split_bisect
     s, e, left, right = [], [], [], []
     leaves_P = []
@@ -81,6 +100,69 @@ def construct_cluster(Geom, Nleaf, method="kmeans"):
     perm = np.empty(n, np.int64)
     for start, P in leaves_P:
         perm[start:start + len(P)] = P
+    return (np.asarray(s, np.int64), np.asarray(e, np.int64), np.asarray(left, np.int64),
+            np.asarray(right, np.int64), perm)
+
+
+def _subtree_job(args):
+    X, Nleaf = args
+    return _build_tree(X, Nleaf, "kmeans")
+
+
+def _kmeans_parallel(X, Nleaf, workers):
+    """The KMeans tree with the subtrees below the top levels built in a pool
+    of host processes (spawned: safe after CUDA is initialised), then spliced
+    into the pre-order of the whole tree."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    n = X.shape[0]
+    # top levels on this process: split the largest pending cluster until there
+    # are enough subtrees to keep the pool busy
+    # node: [P (indices into X), children or None, subtree slot or None]
+    root = [np.arange(n), None, None]
+    pending = [root]
+    target = 4 * workers
+    while len(pending) < target:
+        pending.sort(key=lambda nd: -len(nd[0]))
+        nd = pending[0]
+        if len(nd[0]) <= Nleaf or len(nd[0]) < 4096:
+            break
+        P1, P2 = _split_kmeans(X[nd[0]])
+        a, b = [nd[0][P1], None, None], [nd[0][P2], None, None]
+        nd[1] = (a, b)
+        pending = pending[1:] + [a, b]
+    jobs = [nd for nd in pending if len(nd[0]) > Nleaf]
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        futs = [ex.submit(_subtree_job, (X[nd[0]], Nleaf)) for nd in jobs]
+        for nd, f in zip(jobs, futs):
+            nd[2] = f.result()
+    s, e, left, right = [], [], [], []
+    perm = np.empty(n, np.int64)
+
+    def emit(nd, start, parent, side):
+        cid = len(s)
+        if nd[1] is None and nd[2] is not None:          # a subtree built by a worker
+            ss, ee, ll, rr, pp = nd[2]
+            s.extend((ss + start).tolist())
+            e.extend((ee + start).tolist())
+            left.extend(np.where(ll >= 0, ll + cid, -1).tolist())
+            right.extend(np.where(rr >= 0, rr + cid, -1).tolist())
+            perm[start:start + len(pp)] = nd[0][pp]
+        else:
+            s.append(start)
+            e.append(start + len(nd[0]))
+            left.append(-1)
+            right.append(-1)
+            if nd[1] is None:                             # a leaf cluster
+                perm[start:start + len(nd[0])] = nd[0]
+        if parent >= 0:
+            (left if side == 0 else right)[parent] = cid
+        if nd[1] is not None:
+            a, b = nd[1]
+            emit(a, start, cid, 0)
+            emit(b, start + len(a[0]), cid, 1)
+
+    emit(root, 0, -1, 0)
     return Cluster(X[perm], perm, np.asarray(s, np.int64), np.asarray(e, np.int64),
                    np.asarray(left, np.int64), np.asarray(right, np.int64))
 

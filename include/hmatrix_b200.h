@@ -64,6 +64,9 @@ extern "C" {
 /* ---- flags ------------------------------------------------------------- */
 #define HM_FLAG_DEVICE_PTRS 1u
 #define HM_FLAG_TRANS       2u   /* hm_solve / hm_solve_refined: solve with H' */
+#define HM_FLAG_MV_SIMT     4u   /* hm_matvec, several columns, FP32/BF16 factors:
+                                    the CUDA-core block kernels instead of the
+                                    tensor cores                                */
 
 /* Mirror of the reference's global Params (src/utils.jl:8-24) restricted
  * to the fields the hot path reads, plus the device kernel description. */
@@ -177,11 +180,31 @@ int hm_to_dense(const hm_handle* h, double* out, uint32_t flags);
 
 /* H*V and H'*V (src/harithm.jl:317-329, 243-260): Y = H*X (trans=0) or
  * Y = H'*X (trans=1); X, Y are n x ncols column-major doubles.  The device
- * kernel streams the stored factors once per call (single RHS) in the
- * handle's storage precision and accumulates in FP64.  stream: a
- * cudaStream_t or NULL for the handle's own stream. */
+ * kernels stream the stored factors once per call in the handle's storage
+ * precision (several columns: once per block of columns).  FP64 factors
+ * accumulate in FP64; FP32 and BF16 factors are multiplied in FP32 (one
+ * column) or on the tensor cores (several columns: three TF32 products per
+ * term for FP32 factors, two BF16 products for BF16 factors) with FP32 partial
+ * sums added in FP64.  stream: a cudaStream_t or NULL for the handle's own
+ * stream.  With host pointers the call is synchronous and reports a
+ * tensor-core pipeline timeout (HM_ERR_TIMEOUT); hm_status reads it after
+ * device-pointer calls. */
 int hm_matvec(hm_handle* h, const double* X, double* Y, int64_t ncols,
               int32_t trans, uint32_t flags, void* stream);
+
+/* Waits for `stream` (NULL: the handle's stream) and reports, once, whether a
+ * bounded wait inside the tensor-core kernels gave up since the last check
+ * (HM_ERR_TIMEOUT; the results of that call are not valid).  No counterpart in
+ * the reference. */
+int hm_status(hm_handle* h, void* stream);
+
+/* Self-test of the tensor-core operand layouts of the multi-RHS matvec, on
+ * the current device: D = A B' for A 128 x KC and B 2nc x KC (row-major
+ * FP32 host arrays, KC = 16 for kind 0 = TF32, 32 for kind 1 = BF16, whose
+ * inputs must be exact BF16 values), with A staged in the kernels' K-major
+ * (a_mn = 0) or M-major (a_mn = 1) tile layout; D is 128 x 2nc row-major,
+ * nc = 16 or 64.  No counterpart in the reference. */
+int hm_tc_selftest(int32_t kind, int32_t a_mn, int32_t nc, const float* A, const float* B, float* D);
 
 /* One single-RHS matvec on device pointers with CUDA events between its three
  * launches; ms[0..2] = x staging, phase 1 (z = B'x per low-rank leaf), phase 2
