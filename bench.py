@@ -49,8 +49,11 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1 << 20)
     ap.add_argument("--storage", default="f64", choices=["f64", "f32", "bf16"])
-    ap.add_argument("--extra-precisions", action="store_true",
-                    help="also measure FP32 and BF16 factor storage")
+    ap.add_argument("--no-precisions", action="store_true",
+                    help="skip the FP32 / BF16 factor legs (single RHS and tensor-core multi-RHS)")
+    ap.add_argument("--no-kmeans", action="store_true", help="skip the matvec on the reference's KMeans tree")
+    ap.add_argument("--no-c4", action="store_true", help="skip the gradient (adjoint) leg")
+    ap.add_argument("--c4-n", type=int, default=1 << 17, help="size of the gradient leg")
     ap.add_argument("--cpu-rows", type=int, default=4096, help="rows of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-lu", action="store_true", help="skip the H-LU + solve leg")
@@ -59,8 +62,8 @@ def parse():
                     help="column counts of the multi-RHS matvec leg (comma separated; empty to skip)")
     ap.add_argument("--replicas", action="store_true",
                     help="with --gpus N > 1: N independent copies of H instead of row shards of one H")
-    ap.add_argument("--batch", type=int, default=0,
-                    help="also run the batched uneven H-LU + solve leg with this many problems (256 in full)")
+    ap.add_argument("--batch", type=int, default=256,
+                    help="problems of the batched uneven H-LU + solve leg (0: skip)")
     ap.add_argument("--batch-nthreads", type=int, default=0, help="host threads of the batched calls (0: auto)")
     return ap.parse_args()
 
@@ -315,12 +318,14 @@ def measure(H, a, torch, dist, world, shard=False):
     return ms, ph, ck, e2e_ms, rel
 
 
-def multi_rhs_leg(H, cols, steps, torch, bytes_1):
+def multi_rhs_leg(H, cols, steps, torch, bytes_1, exact_rows=False):
     """H*X for X of c N(0,1) columns (seed 1): device time per call (CUDA
     events over `steps` calls after 3 warm-up calls), the factor bytes
     streamed per second, the equivalent single-column rate (c x the bytes
     of one column's matvec per second), and the agreement with the
-    single-column kernel on the first and last columns."""
+    single-column kernel on the first and last columns.  FP32/BF16 factors
+    run on the tensor cores; exact_rows adds the error of the first column
+    against exact FP64 kernel rows (the dense FullMat oracle, 1024 rows)."""
     import ctypes as C
     from hmatrix import _lib
     L = _lib.lib()
@@ -356,7 +361,14 @@ def multi_rhs_leg(H, cols, steps, torch, bytes_1):
         flops = 2.0 * c * (info.rk_entries + info.dense_entries)
         out[str(c)] = {"ms": ms, "factor_GB/s": bytes_1 / (ms * 1e-3) / 1e9,
                        "equiv_single_column_GB/s": c * bytes_1 / (ms * 1e-3) / 1e9,
-                       "fp64_GFLOP/s": flops / (ms * 1e-3) / 1e9, "rel_diff_vs_single_column": err}
+                       "GFLOP/s": flops / (ms * 1e-3) / 1e9, "rel_diff_vs_single_column": err}
+        if exact_rows:
+            from hmatrix import _lib as _l
+            rows = np.sort(np.random.default_rng(2).choice(H.n, 1024, replace=False))
+            ex = H.exact_rows(rows, X[0].cpu().numpy())
+            out[str(c)]["rel_err_vs_exact_fp64_rows"] = float(np.linalg.norm(Y[0].cpu().numpy()[rows] - ex)
+                                                               / np.linalg.norm(ex))
+            _l.check(L.hm_status(H._h, sp))
         del X, Y
         torch.cuda.empty_cache()
     return out
@@ -532,6 +544,90 @@ def batch_leg(count, torch, nthreads=0, budget_gb=90.0, rank=0, world=1, dist=No
     return out
 
 
+def kmeans_leg(a, torch, peak):
+    """The large 1-D matvec on the reference's own cluster tree: KMeans
+    bisection (src/cluster.jl:196-256, the same sklearn call, subtrees on a
+    pool of host processes), FP64 factors.  The tree build and the H-matrix
+    construction are timed apart from the matvec."""
+    import hmatrix as hm
+    from hmatrix.cluster import construct_cluster
+    n = a.n
+    t0 = time.perf_counter()
+    c = construct_cluster(np.linspace(0, 10, n), 64, "kmeans")
+    t_tree = time.perf_counter() - t0
+    prm = hm.Params(Geom=np.linspace(0, 10, n), Kernel=hm.Cauchy(1.0), MaxBlock=512, MinBlock=64, MaxRank=16,
+                    ConsMethod="aca2", εComp=1e-8, Device=torch.cuda.current_device())
+    t0 = time.perf_counter()
+    H = hm.new_on_cluster(prm, c)
+    t_build = time.perf_counter() - t0
+    info = H.info()
+    ms, ph, ck, e2e_ms, rel = measure(H, a, torch, None, 1)
+    bytes_mv = 8 * info.rk_entries + 8 * info.dense_entries + 16 * n
+    sz = c.e - c.s
+    leaf = c.left < 0
+    gbs = bytes_mv / (ms * 1e-3) / 1e9
+    out = {"tree": "kmeans (src/cluster.jl:196-256)", "tree_s": t_tree, "build_s": t_build,
+           "leaf_clusters": int(leaf.sum()), "leaf_sizes": [int(sz[leaf].min()), int(sz[leaf].max())],
+           "n_rk": info.n_rk, "n_dense": info.n_dense, "rk_entries": info.rk_entries,
+           "dense_entries": info.dense_entries, "max_rank": info.max_rank, "algorithmic_bytes": bytes_mv,
+           "ms_per_matvec": ms, "GB/s": gbs, "frac_of_peak": gbs / peak, "phase_ms": [float(v) for v in ph],
+           "e2e_GB/s": bytes_mv / (e2e_ms * 1e-3) / 1e9, "rel_err_vs_exact_fp64_rows": rel, "clocks": ck}
+    del H
+    torch.cuda.empty_cache()
+    return out
+
+
+def gradient_leg(n, torch):
+    """The differentiation configuration: n points on [0,10], Gaussian kernel
+    exp(-(x-y)^2/(2 l^2)) + sigma2 I with l = 0.7, sigma2 = 1e-2, MaxRank 24,
+    ACA tolerance 1e-10, b ~ N(0,1), loss L = b'(H\b) + |H b|^2.  Gradients
+    in b, l and sigma2 from the adjoint kernels (transposed matvec, transposed
+    solve on the stored LU, H-matrix of dK/dl), checked against central finite
+    differences of the H-path loss (step 1e-6 for l and sigma2; the H-matrices
+    at l +- h reuse the pivots of H, so their factors move smoothly with l)."""
+    import hmatrix as hm
+    from hmatrix.autodiff import KernelOperator
+
+    def prm(ell=0.7, s2=1e-2, keep=False):
+        return hm.Params(Geom=np.linspace(0, 10, n), Kernel=hm.Gauss(ell), MaxBlock=512, MinBlock=64, MaxRank=24,
+                         ConsMethod="aca2", εComp=1e-10, Tree="bisect", Shift=s2, KeepPivots=keep,
+                         Device=torch.cuda.current_device())
+
+    def loss(op, bb):
+        with torch.no_grad():
+            t = torch.tensor(bb, device="cuda")
+            return float(torch.dot(t, op.solve(t)) + torch.sum(op.matvec(t) ** 2))
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    op = KernelOperator(prm(keep=True), refine_tol=1e-13)
+    t_build = time.perf_counter() - t0
+    b0 = np.random.default_rng(4).standard_normal(n)
+    b = torch.tensor(b0, device="cuda", requires_grad=True)
+    t0 = time.perf_counter()
+    L = torch.dot(b, op.solve(b)) + torch.sum(op.matvec(b) ** 2)
+    L.backward()
+    torch.cuda.synchronize()
+    t_grad = time.perf_counter() - t0
+    gb, gl, gs = b.grad.cpu().numpy(), float(op.p.grad), float(op.sigma2.grad)
+    d = np.random.default_rng(5).standard_normal(n)
+    hb = 1e-3
+    fd_b = (loss(op, b0 + hb * d) - loss(op, b0 - hb * d)) / (2 * hb)
+    h = 1e-6
+    fd_s = (loss(KernelOperator(prm(s2=1e-2 + h), cluster=op.c, refine_tol=1e-13), b0)
+            - loss(KernelOperator(prm(s2=1e-2 - h), cluster=op.c, refine_tol=1e-13), b0)) / (2 * h)
+    fd_l = (loss(KernelOperator(prm(ell=0.7 + h), like=op, refine_tol=1e-13), b0)
+            - loss(KernelOperator(prm(ell=0.7 - h), like=op, refine_tol=1e-13), b0)) / (2 * h)
+    return {"config": {"n": n, "kernel": "exp(-(x-y)^2/(2 l^2)) + sigma2 I", "l": 0.7, "sigma2": 1e-2,
+                       "MaxRank": 24, "aca_tol": 1e-10, "loss": "b'(H\\b) + |H b|^2", "fd_step": h,
+                       "tree": "median bisection"},
+            "loss": float(L.detach()), "build_s": t_build, "forward_backward_s": t_grad,
+            "grad_l": gl, "fd_l": fd_l, "rel_err_l": abs(fd_l - gl) / abs(gl),
+            "grad_sigma2": gs, "fd_sigma2": fd_s, "rel_err_sigma2": abs(fd_s - gs) / abs(gs),
+            "rel_err_b_directional": abs(fd_b - gb @ d) / abs(gb @ d),
+            "target": 1e-6}
+
+
 def run_ours(a):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -579,22 +675,35 @@ def run_ours(a):
     if cols and world == 1:
         multi = multi_rhs_leg(H, cols, max(3, min(a.steps, 10)), torch, bytes_mv)
     extra = {}
-    if a.extra_precisions and world == 1:
+    if not a.no_precisions and world == 1:
+        # FP32 / BF16 factors: single-RHS matvec (FP32 partial sums) and the
+        # tensor-core multi-RHS product, each against exact FP64 rows
         for s in ("f32", "bf16"):
             if s == a.storage:
                 continue
             del H
+            H = None
             torch.cuda.empty_cache()
             _, H2, tb2 = build(a.n, s)
             i2 = H2.info()
             ms2, ph2, _, _, rel2 = measure(H2, a, torch, None, 1)
             eb2 = {"f32": 4, "bf16": 2}[s]
             b2 = eb2 * i2.rk_entries + 4 * i2.dense_entries + 16 * a.n
-            extra[s] = {"GB/s": b2 / (ms2 * 1e-3) / 1e9, "ms_per_step": ms2, "rel_err_4096_rows": rel2,
-                        "phase_ms": [float(v) for v in ph2], "build_s": tb2}
+            extra[s] = {"GB/s": b2 / (ms2 * 1e-3) / 1e9, "ms_per_step": ms2, "frac_of_peak": b2 / (ms2 * 1e-3) / 1e9 / peak,
+                        "rel_err_4096_rows": rel2, "phase_ms": [float(v) for v in ph2], "build_s": tb2}
+            if cols:
+                mr = multi_rhs_leg(H2, cols, max(3, min(a.steps, 10)), torch, b2, exact_rows=True)
+                for v in mr.values():
+                    # the factors stream once per call: the HBM floor is their bytes
+                    v["frac_of_hbm_floor"] = v["factor_GB/s"] / peak
+                extra[s]["multi_rhs_tensor_cores"] = mr
             del H2
-            H = None
             torch.cuda.empty_cache()
+    kmeans = None
+    if not a.no_kmeans and world == 1:
+        H = None
+        torch.cuda.empty_cache()
+        kmeans = kmeans_leg(a, torch, peak)
     lu = None
     if not a.no_lu and world == 1:
         H = None
@@ -610,6 +719,11 @@ def run_ours(a):
         H = None
         torch.cuda.empty_cache()
         batch = batch_leg(a.batch, torch, a.batch_nthreads, rank=rank, world=world, dist=dist)
+    c4 = None
+    if not a.no_c4 and world == 1:
+        H = None
+        torch.cuda.empty_cache()
+        c4 = gradient_leg(a.c4_n, torch)
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -644,7 +758,9 @@ def run_ours(a):
                           "dense_entries": info.dense_entries, "max_rank": info.max_rank,
                           "algorithmic_bytes": bytes_mv, "build_s": t_build},
             "multi_rhs": multi,
-            "extra_precisions": extra or None,
+            "reduced_precision": extra or None,
+            "kmeans_tree": kmeans,
+            "gradients": c4,
             "lu_solve": lu,
             "batched_lu_solve": batch}
     print(json.dumps(line))

@@ -215,6 +215,42 @@ int hm_new(const hm_params* p, int64_t n, const double* geom, int64_t ncluster, 
   return HM_OK;
 }
 
+int hm_new_like(const hm_handle* ref, const hm_params* p, hm_handle** out) {
+  if (!out || !ref) return fail(HM_ERR_ARG, "NULL argument");
+  *out = nullptr;
+  HM_TRY(check_params(p));
+  if (ref->factorized) return fail(HM_ERR_STATE, "the reference H-matrix is factorised");
+  const hm_params& r = ref->prm;
+  if (p->dim != r.dim || p->cons_method != HM_CONS_ACA2 || r.cons_method != HM_CONS_ACA2 ||
+      p->max_rank != r.max_rank || p->min_block != r.min_block ||
+      (p->max_block != r.max_block && !(p->max_block == -1)) || p->storage != r.storage ||
+      p->row_lo != r.row_lo || p->row_hi != r.row_hi)
+    return fail(HM_ERR_ARG, "hm_new_like: only the kernel, its parameter and the shift may differ from the reference");
+  DeviceGuard g(ref->device);
+  hm_handle* h = new (std::nothrow) hm_handle();
+  if (!h) return fail(HM_ERR_OOM, "host allocation");
+  h->prm = *p;
+  h->prm.max_block = r.max_block;
+  h->prm.device = ref->device;
+  h->n = ref->n;
+  h->dim = ref->dim;
+  h->device = ref->device;
+  h->storage = ref->storage;
+  h->kd = KernelDesc{p->kernel, p->dim, p->kparam, p->shift};
+  cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete h; return fail(HM_ERR_CUDA, cudaGetErrorString(e)); }
+  int s = build_like(h, ref);
+  if (s != HM_OK) {
+    std::string msg = g_last_error;
+    free_handle_data(h);
+    cudaStreamDestroy(h->stream);
+    delete h;
+    return fail(s, msg);
+  }
+  *out = h;
+  return HM_OK;
+}
+
 int hm_destroy(hm_handle* h) {
   if (!h) return HM_OK;
   DeviceGuard g(h->device);

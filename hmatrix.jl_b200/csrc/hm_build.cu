@@ -287,9 +287,22 @@ int build_handle(hm_handle* h, const double* geom, int64_t ncl, const int64_t* c
 
   // ---- matvec layout: pools ordered by row group -----------------------------
   HM_TRY(build_matvec_plans(h));
+  if (p.cons_method == HM_CONS_ACA2 && (p.build_flags & HM_BUILD_KEEP_PIVOTS)) {
+    h->piv_count = (int64_t)rk_leaf.size() * 2 * std::max(1, p.max_rank);
+    if (h->piv_count) {
+      cudaError_t e = cudaMalloc(&h->d_piv, sizeof(int32_t) * h->piv_count);
+      if (e != cudaSuccess) return fail(HM_ERR_OOM, std::string("aca2 pivots: ") + cudaGetErrorString(e));
+    }
+  }
+  return fill_pools(h, rk_leaf, false, &svd_store);
+}
 
-  // ---- fill the pools ---------------------------------------------------------
-  const int eb = elem_bytes(h->storage), deb = dense_elem_bytes(h->storage);
+// Dense leaves and low-rank factors into the laid-out pools.  replay: the
+// aca2 factors from the pivots in h->d_piv (hm_new_like).
+int fill_pools(hm_handle* h, const std::vector<int64_t>& rk_leaf, bool replay, const SvdCandidateStore* svd_store) {
+  const hm_params& p = h->prm;
+  const int64_t n = h->n;
+  const int deb = dense_elem_bytes(h->storage);
   {
     std::vector<DenseJob> jobs;
     for (auto& L : h->leaves)
@@ -313,15 +326,36 @@ int build_handle(hm_handle* h, const double* geom, int64_t ncl, const int64_t* c
     }
   }
   if (p.cons_method == HM_CONS_ACA2) {
-    HM_TRY(aca2_write(h, rk_leaf));
+    HM_TRY(aca2_write(h, rk_leaf, replay));
   } else if (p.cons_method == HM_CONS_BBFMM) {
     HM_TRY(bbfmm_write(h, rk_leaf));
   } else {
-    HM_TRY(svd_store.write_pool(h, rk_leaf));
+    if (!svd_store) return fail(HM_ERR_UNSUPPORTED, "svd-route factors are not kept");
+    HM_TRY(svd_store->write_pool(h, rk_leaf));
   }
-  (void)eb;
   HM_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return HM_OK;
+}
+
+// A new H-matrix of the kernel and shift in h->prm on the structure of ref:
+// same cluster tree, block partition, ranks and aca2 pivots (hm_new_like).
+int build_like(hm_handle* h, const hm_handle* ref) {
+  if (!ref->d_piv) return fail(HM_ERR_STATE, "the reference H-matrix kept no aca2 pivots (HM_BUILD_KEEP_PIVOTS)");
+  h->cl_s = ref->cl_s; h->cl_e = ref->cl_e; h->cl_left = ref->cl_left; h->cl_right = ref->cl_right;
+  h->cl_depth = ref->cl_depth; h->nodes = ref->nodes; h->leaves = ref->leaves; h->depth = ref->depth;
+  HM_CUDA_TRY(cudaMalloc((void**)&h->d_geom, sizeof(double) * h->n * h->dim));
+  HM_CUDA_TRY(cudaMemcpyAsync(h->d_geom, ref->d_geom, sizeof(double) * h->n * h->dim, cudaMemcpyDeviceToDevice,
+                              h->stream));
+  h->piv_count = ref->piv_count;
+  cudaError_t e = cudaMalloc(&h->d_piv, sizeof(int32_t) * h->piv_count);
+  if (e != cudaSuccess) return fail(HM_ERR_OOM, std::string("aca2 pivots: ") + cudaGetErrorString(e));
+  HM_CUDA_TRY(cudaMemcpyAsync(h->d_piv, ref->d_piv, sizeof(int32_t) * h->piv_count, cudaMemcpyDeviceToDevice,
+                              h->stream));
+  std::vector<int64_t> rk_leaf;
+  for (int64_t i = 0; i < (int64_t)h->leaves.size(); ++i)
+    if (h->leaves[i].type == T_RK) rk_leaf.push_back(i);
+  HM_TRY(build_matvec_plans(h));
+  return fill_pools(h, rk_leaf, true, nullptr);
 }
 
 // The leaves of the block partition alone, on the host (no device is used):
@@ -466,6 +500,9 @@ void free_handle_data(hm_handle* h) {
   fr(h->d_xm);
   fr(h->d_tc);
   fr(h->d_tc_err);
+  fr(h->d_piv);
+  h->d_piv = nullptr;
+  h->piv_count = 0;
   free_tc_plan(h->tc_fwd);
   free_tc_plan(h->tc_bwd);
   h->d_tc = nullptr;

@@ -215,6 +215,8 @@ struct hm_handle {
   void* d_tc = nullptr;            // their X and Z tiles
   size_t tc_bytes = 0;
   int* d_tc_err = nullptr;         // error word of their bounded waits
+  int32_t* d_piv = nullptr;        // aca2 pivots (row, column) of every step, when kept
+  int64_t piv_count = 0;
 
   hm::LuState* lu = nullptr;       // set once factorised
   bool factorized = false;
@@ -246,6 +248,7 @@ int build_handle(hm_handle* h, const double* geom, int64_t ncluster,
                  const int64_t* cl_s, const int64_t* cl_e, const int64_t* cl_left,
                  const int64_t* cl_right, int64_t n_nb, const int64_t* nb_pairs);
 int build_matvec_plans(hm_handle* h);
+int build_like(hm_handle* h, const hm_handle* ref);
 int partition_only(hm_handle* h, int64_t ncl, const int64_t* cl_s, const int64_t* cl_e, const int64_t* cl_left,
                    const int64_t* cl_right, int64_t n_nb, const int64_t* nb_pairs);
 int build_mv_descriptors(hm_handle* h, const std::vector<int64_t>& order, int trans);

@@ -22,11 +22,16 @@ struct AcaJob {
   int64_t off;      // element offset of the leaf in the low-rank pool
 };
 
+// Pivots: piv (2 R entries a job: row tau_r, column sigma_r of step r) is
+// written when pmode == 1 and read when pmode == 2.  A replay (write pass
+// only) takes the recorded rows and columns and runs exactly ranks[job]
+// steps with no stopping test, so that the factors of a nearby kernel come
+// from the same cross approximation and vary smoothly with its parameter.
 template <typename T>
 __global__ void __launch_bounds__(128) aca2_kernel(
     KernelDesc kd, const double* __restrict__ geom, int64_t ng, const AcaJob* __restrict__ jobs,
     int64_t njobs, int R, double eps_comp, double* __restrict__ scratch, int mcap, int ncap,
-    int32_t* __restrict__ ranks, T* __restrict__ pool, int write) {
+    int32_t* __restrict__ ranks, T* __restrict__ pool, int write, int32_t* __restrict__ piv, int pmode) {
   const int lane = threadIdx.x & 31;
   const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -40,7 +45,11 @@ __global__ void __launch_bounds__(128) aca2_kernel(
     uint64_t used = 0;          // bit q of lane l: row l + 32q is used
     double na0 = 1.0, nb0 = 1.0;
     int rank = R;
-    for (int r = 0; r < R; ++r) {
+    int32_t* jp = piv ? piv + job * 2 * (int64_t)R : nullptr;
+    const int rmax = pmode == 2 ? min(ranks[job], R) : R;
+    if (pmode == 2) rank = rmax;
+    for (int r = 0; r < rmax; ++r) {
+      if (pmode == 2) tau = jp[2 * r];
       // residual row tau (src/hlu.jl:73-77)
       double best = -1.0, bval = 0.0, nB = 0.0;
       int64_t bidx = INT64_MAX;
@@ -58,9 +67,11 @@ __global__ void __launch_bounds__(128) aca2_kernel(
       }
       warp_argmax(best, bidx, bval);
       nB = warp_sum(nB);
-      const int sigma = (int)bidx;
-      const double delta = bval;
+      __syncwarp();
+      const int sigma = pmode == 2 ? jp[2 * r + 1] : (int)bidx;
+      const double delta = pmode == 2 ? SB[(int64_t)r * ncap + sigma] : bval;
       if (!(delta != 0.0)) { rank = r; break; }      // delta == 0 (src/hlu.jl:87-89)
+      if (pmode == 1 && lane == 0) { jp[2 * r] = tau; jp[2 * r + 1] = sigma; }
       if ((tau & 31) == lane) used |= 1ull << (tau >> 5);
       __syncwarp();
       // residual column sigma, new a_r (src/hlu.jl:93-98)
@@ -86,6 +97,7 @@ __global__ void __launch_bounds__(128) aca2_kernel(
       __syncwarp();
       const double na = sqrt(nA), nb = sqrt(nB);
       if (r == 0) { na0 = na; nb0 = nb; }
+      if (pmode == 2) continue;                          // replay: the recorded steps, no stopping test
       if (idx2 == INT64_MAX) { rank = r + 1; break; }   // no unused row left
       tau = (int)idx2;
       const double eps = na * nb / na0 / nb0;           // src/hlu.jl:104
@@ -109,7 +121,7 @@ __global__ void __launch_bounds__(128) aca2_kernel(
 }
 
 static int aca2_launch(hm_handle* h, const std::vector<int64_t>& rk_leaf, int write,
-                       std::vector<int32_t>* ranks_out) {
+                       std::vector<int32_t>* ranks_out, int pmode) {
   const int64_t nj = (int64_t)rk_leaf.size();
   if (nj == 0) { if (ranks_out) ranks_out->clear(); return HM_OK; }
   std::vector<AcaJob> jobs(nj);
@@ -145,16 +157,16 @@ static int aca2_launch(hm_handle* h, const std::vector<int64_t>& rk_leaf, int wr
   switch (write ? h->storage : HM_F64) {
     case HM_F64:
       aca2_kernel<double><<<grid, 128, 0, h->stream>>>(h->kd, h->d_geom, h->n, dj, nj, R, h->prm.eps_comp,
-                                                      scratch, mcap, ncap, dr, (double*)h->d_rk, write);
+                                                      scratch, mcap, ncap, dr, (double*)h->d_rk, write, h->d_piv, pmode);
       break;
     case HM_F32:
       aca2_kernel<float><<<grid, 128, 0, h->stream>>>(h->kd, h->d_geom, h->n, dj, nj, R, h->prm.eps_comp,
-                                                     scratch, mcap, ncap, dr, (float*)h->d_rk, write);
+                                                     scratch, mcap, ncap, dr, (float*)h->d_rk, write, h->d_piv, pmode);
       break;
     default:
       aca2_kernel<__nv_bfloat16><<<grid, 128, 0, h->stream>>>(h->kd, h->d_geom, h->n, dj, nj, R,
                                                              h->prm.eps_comp, scratch, mcap, ncap, dr,
-                                                             (__nv_bfloat16*)h->d_rk, write);
+                                                             (__nv_bfloat16*)h->d_rk, write, h->d_piv, pmode);
   }
   HM_CUDA_TRY(cudaGetLastError());
   std::vector<int32_t> ranks(nj);
@@ -175,10 +187,12 @@ static int aca2_launch(hm_handle* h, const std::vector<int64_t>& rk_leaf, int wr
 }
 
 int aca2_ranks(hm_handle* h, const std::vector<int64_t>& rk_leaf, std::vector<int32_t>& ranks) {
-  return aca2_launch(h, rk_leaf, 0, &ranks);
+  return aca2_launch(h, rk_leaf, 0, &ranks, 0);
 }
-int aca2_write(hm_handle* h, const std::vector<int64_t>& rk_leaf) {
-  return aca2_launch(h, rk_leaf, 1, nullptr);
+// the write pass records the pivots when the handle keeps them (d_piv set
+// before, replay = false) or replays them (replay = true)
+int aca2_write(hm_handle* h, const std::vector<int64_t>& rk_leaf, bool replay) {
+  return aca2_launch(h, rk_leaf, 1, nullptr, h->d_piv ? (replay ? 2 : 1) : 0);
 }
 
 // ===========================================================================

@@ -68,7 +68,8 @@ int svd_compress_candidates(hm_handle* h, const std::vector<int64_t>& r0,
                             const std::vector<int32_t>& n, std::vector<int32_t>& ranks,
                             SvdCandidateStore& store, const std::vector<int32_t>& nodes);
 int aca2_ranks(hm_handle* h, const std::vector<int64_t>& rk_leaf, std::vector<int32_t>& ranks);
-int aca2_write(hm_handle* h, const std::vector<int64_t>& rk_leaf);
+int aca2_write(hm_handle* h, const std::vector<int64_t>& rk_leaf, bool replay = false);
+int fill_pools(hm_handle* h, const std::vector<int64_t>& rk_leaf, bool replay, const SvdCandidateStore* svd_store);
 // Chebyshev-interpolation ("bbfmm") leaves: the rank of an m x n leaf, and
 // the factors of every low-rank leaf written into the pool
 int bbfmm_rank(int64_t m, int64_t n, int dim, int max_rank);

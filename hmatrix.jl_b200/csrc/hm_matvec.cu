@@ -747,6 +747,8 @@ int copy_handle(const hm_handle* h, hm_handle** out) {
   chk(dup(&c->d_rk, h->d_rk, h->rk_bytes));
   chk(dup(&c->d_dense, h->d_dense, h->dense_bytes));
   chk(dup((void**)&c->d_z, h->d_z, sizeof(double) * h->zlen));
+  chk(dup((void**)&c->d_piv, h->d_piv, sizeof(int32_t) * h->piv_count));
+  c->piv_count = h->d_piv ? h->piv_count : 0;
   for (int t = 0; t < 2 && s == HM_OK; ++t) {
     const MvPlan& a = t ? h->bwd : h->fwd;
     MvPlan& b = t ? c->bwd : c->fwd;

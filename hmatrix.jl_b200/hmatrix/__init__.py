@@ -32,7 +32,7 @@ __all__ = [
     "Hparams", "Params", "NewHmat", "FullMat", "Hmat", "lu", "lu_", "getl", "getu", "info",
     "Cauchy", "InvQuad", "Gauss", "Kernel", "Cluster", "construct_cluster", "HmError",
     "aca_wrapper", "F64", "F32", "BF16", "new_on_cluster", "load", "coarsening", "CauchyDP", "InvQuadDP", "GaussDP",
-    "lu_batch", "lu_batch_", "solve_batch", "solve_refined_batch", "matvec_batch", "gmres", "bicgstab",
+    "lu_batch", "lu_batch_", "solve_batch", "solve_refined_batch", "matvec_batch", "gmres", "bicgstab", "new_like",
 ]
 
 F64, F32, BF16 = _lib.HM_F64, _lib.HM_F32, _lib.HM_BF16
@@ -61,6 +61,7 @@ class Params:
     LuMode: str = "auto"                  # "auto" | "recursive" (lu! as written) | "tiles"
     εTruncLU: float = 0.0                 # truncation inside H-LU (0: εTrunc, as in the reference)
     RowRange: tuple = (0, 0)              # build only rows [lo, hi) (a multi-GPU shard); (0, 0): all
+    KeepPivots: bool = False              # aca2: keep the pivots, for new_like
 
 
 Hparams = Params()
@@ -106,6 +107,7 @@ def _params_struct(prm: Params, dim: int):
     p.lu_mode = {"auto": 0, "recursive": 1, "tiles": 2}[prm.LuMode]
     p.eps_trunc_lu = prm.εTruncLU
     p.row_lo, p.row_hi = int(prm.RowRange[0]), int(prm.RowRange[1])
+    p.build_flags = _lib.HM_BUILD_KEEP_PIVOTS if prm.KeepPivots else 0
     return p
 
 
@@ -369,6 +371,23 @@ def new_on_cluster(prm: Params, c: Cluster):
                        _ptr(c.right), 0 if nb is None else len(nb),
                        None if nb is None else _ptr(np.ascontiguousarray(nb)), C.byref(out)))
     return Hmat(out.value, n, c)
+
+
+def new_like(H: "Hmat", prm: Params):
+    """The H-matrix of ``prm`` (a different kernel parameter, kernel or shift)
+    on the structure of ``H``: same tree, partition and ranks, every low-rank
+    block's cross approximation taken at ``H``'s pivots (``H`` built with
+    ``KeepPivots=True``), so that its factors vary smoothly with the kernel
+    parameter."""
+    X = np.asarray(H.c.X, dtype=np.float64)
+    d = 1 if X.ndim == 1 else X.shape[1]
+    if prm.MaxBlock == -1:
+        prm.MaxBlock = H.n // 4
+    p = _params_struct(prm, d)
+    p.build_flags = _lib.HM_BUILD_KEEP_PIVOTS
+    out = C.c_void_p()
+    check(lib().hm_new_like(H._h, C.byref(p), C.byref(out)))
+    return Hmat(out.value, H.n, H.c)
 
 
 def load(path, device=0):

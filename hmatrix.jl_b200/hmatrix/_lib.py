@@ -22,6 +22,7 @@ HM_F64, HM_F32, HM_BF16 = 0, 1, 2
 HM_FLAG_DEVICE_PTRS = 1
 HM_FLAG_TRANS = 2
 HM_FLAG_MV_SIMT = 4
+HM_BUILD_KEEP_PIVOTS = 1
 
 STATUS_NAMES = {
     1: "HM_ERR_ARG", 2: "HM_ERR_CUDA", 3: "HM_ERR_OOM", 4: "HM_ERR_STATE", 5: "HM_ERR_SINGULAR",
@@ -31,7 +32,7 @@ STATUS_NAMES = {
 
 # every symbol include/hmatrix_b200.h declares
 EXPORTED = [
-    "hm_version", "hm_last_error", "hm_default_params", "hm_new", "hm_partition", "hm_destroy", "hm_info",
+    "hm_version", "hm_last_error", "hm_default_params", "hm_new", "hm_new_like", "hm_partition", "hm_destroy", "hm_info",
     "hm_leaves", "hm_leaf_factors", "hm_to_dense", "hm_matvec", "hm_status", "hm_tc_selftest", "hm_matvec_profile", "hm_exact_rows",
     "hm_add_identity", "hm_scale", "hm_copy", "hm_coarsen", "hm_add", "hm_save", "hm_load", "hm_load_user", "hm_lu", "hm_lu_perm", "hm_solve", "hm_solve_refined",
     "hm_batch_lu", "hm_batch_solve", "hm_batch_solve_refined", "hm_batch_matvec",
@@ -46,7 +47,7 @@ class hm_params(C.Structure):
         ("eps_comp", C.c_double), ("eps_trunc", C.c_double), ("max_rank", C.c_int32),
         ("max_block", C.c_int32), ("min_block", C.c_int32), ("cons_method", C.c_int32),
         ("aca_force", C.c_int32), ("storage", C.c_int32), ("device", C.c_int32),
-        ("rank_cap", C.c_int32), ("lu_mode", C.c_int32), ("reserved0", C.c_int32),
+        ("rank_cap", C.c_int32), ("lu_mode", C.c_int32), ("build_flags", C.c_int32),
         ("eps_trunc_lu", C.c_double), ("row_lo", C.c_int32), ("row_hi", C.c_int32),
     ]
 
@@ -86,6 +87,7 @@ def lib():
     L.hm_default_params.argtypes = [C.POINTER(hm_params)]
     L.hm_new.argtypes = [C.POINTER(hm_params), C.c_int64, vp, C.c_int64, vp, vp, vp, vp, C.c_int64, vp,
                          C.POINTER(vp)]
+    L.hm_new_like.argtypes = [vp, C.POINTER(hm_params), C.POINTER(vp)]
     L.hm_partition.argtypes = [C.POINTER(hm_params), C.c_int64, C.c_int64, vp, vp, vp, vp, C.c_int64, vp,
                                C.c_int64, vp, p64]
     L.hm_destroy.argtypes = [vp]

@@ -20,16 +20,21 @@ import dataclasses
 
 import torch
 
-from . import Params, NewHmat, new_on_cluster, lu
+from . import Params, NewHmat, new_like, new_on_cluster, lu
 
 
 class KernelOperator:
     """H = K_p + sigma2 I (``prm.Kernel`` = K_p, ``prm.Shift`` = sigma2) with its
     LU and the H-matrix of dK/dp, both built on first use."""
 
-    def __init__(self, prm: Params, cluster=None, refine_tol: float = 0.0):
+    def __init__(self, prm: Params, cluster=None, refine_tol: float = 0.0, like=None):
+        """like: another KernelOperator built with ``prm.KeepPivots``; H is then
+        built on its structure and pivots (``new_like``), so that losses at
+        nearby kernel parameters differ smoothly (finite-difference checks)."""
         self.prm = prm
-        if cluster is None:
+        if like is not None:
+            self.c, self.H = like.c, new_like(like.H, prm)
+        elif cluster is None:
             self.c, self.H = NewHmat(prm)
         else:
             self.c, self.H = cluster, new_on_cluster(prm, cluster)

@@ -61,6 +61,9 @@ extern "C" {
 #define HM_F32             1
 #define HM_BF16            2   /* BF16 low-rank factors, FP32 dense leaves    */
 
+/* ---- hm_params.build_flags ---------------------------------------------- */
+#define HM_BUILD_KEEP_PIVOTS 1   /* aca2: keep every block's pivots for hm_new_like */
+
 /* ---- flags ------------------------------------------------------------- */
 #define HM_FLAG_DEVICE_PTRS 1u
 #define HM_FLAG_TRANS       2u   /* hm_solve / hm_solve_refined: solve with H' */
@@ -88,7 +91,7 @@ typedef struct hm_params {
     int32_t lu_mode;      /* H-LU schedule: 0 auto, 1 the recursion of lu!,
                              2 tile by tile (needs a level where every block
                              outside the diagonal tiles is one low-rank block) */
-    int32_t reserved0;
+    int32_t build_flags;  /* HM_BUILD_* */
     double  eps_trunc_lu; /* truncation tolerance of the recompressions inside
                              H-LU (0: eps_trunc, as in the reference); a looser
                              value gives a cheaper factorisation that
@@ -158,6 +161,16 @@ int hm_new(const hm_params* p, int64_t n, const double* geom,
 int hm_partition(const hm_params* p, int64_t n, int64_t ncluster, const int64_t* cl_s, const int64_t* cl_e,
                  const int64_t* cl_left, const int64_t* cl_right, int64_t n_nb, const int64_t* nb_pairs,
                  int64_t cap, int64_t* out, int64_t* count);
+
+/* A new H-matrix on the structure of `ref` (built with HM_BUILD_KEEP_PIVOTS
+ * by the aca2 route): same cluster tree, block partition and ranks, and every
+ * low-rank block's cross approximation taken at ref's pivot rows and columns,
+ * for the kernel parameter, kernel id and shift of p (the other fields of p
+ * must equal ref's).  The factors then depend smoothly on the kernel
+ * parameter, so finite differences of anything computed from the H-matrix
+ * match its derivative (the adjoint checks of the hyper-parameter
+ * gradients).  No counterpart in the reference. */
+int hm_new_like(const hm_handle* ref, const hm_params* p, hm_handle** out);
 
 /* free a handle */
 int hm_destroy(hm_handle* h);

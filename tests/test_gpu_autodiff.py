@@ -6,21 +6,23 @@ on [0,10], MaxRank 24, ACA tolerance 1e-10, loss L = b'(H\\b) + |H b|^2.
 * the derivative kernels: H-matrices of dK/dp against the dense derivative;
 * gradients against the dense FP64 gradient (tolerance 1e-5: the H-matrix is
   within 1e-10 of K, amplified by cond(H) ~ 1e4 in the solves);
-* gradients in b and sigma2 against central finite differences of the H-path
-  loss itself (b enters quadratically and sigma2 only shifts the diagonal
-  leaves, so the differences are exact up to rounding): 1e-6.
+* gradients in b, l and sigma2 against central finite differences (step
+  1e-6 for l and sigma2) of the H-path loss itself: b enters quadratically,
+  sigma2 only shifts the diagonal leaves, and the H-matrices at l +- h are
+  built on the structure and aca2 pivots of H (new_like), so their factors
+  move smoothly with l: 1e-6.
 """
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
-N = 2048
+N = 4096
 
 
-def prm(hm, ell=0.7, sigma2=1e-2, kernel=None):
+def prm(hm, ell=0.7, sigma2=1e-2, kernel=None, keep=False):
     return hm.Params(Geom=np.linspace(0, 10, N), Kernel=kernel or hm.Gauss(ell), MaxBlock=512, MinBlock=64,
-                     MaxRank=24, ConsMethod="aca2", εComp=1e-10, Tree="bisect", Shift=sigma2)
+                     MaxRank=24, ConsMethod="aca2", εComp=1e-10, Tree="bisect", Shift=sigma2, KeepPivots=keep)
 
 
 @pytest.mark.parametrize("kind", ["Gauss", "Cauchy", "InvQuad"])
@@ -53,7 +55,7 @@ def test_gradients_vs_dense_and_fd():
     import torch
     import hmatrix as hm
     from hmatrix.autodiff import KernelOperator
-    P = prm(hm)
+    P = prm(hm, keep=True)
     op = KernelOperator(P, refine_tol=1e-13)
     b0 = np.random.default_rng(4).standard_normal(N)
     b = torch.tensor(b0, device="cuda", requires_grad=True)
@@ -83,6 +85,31 @@ def test_gradients_vs_dense_and_fd():
     opm = KernelOperator(prm(hm, sigma2=1e-2 - hs), cluster=op.c, refine_tol=1e-13)
     fd_s = (loss(opp, b0) - loss(opm, b0)) / (2 * hs)
     assert abs(fd_s - gs) <= 1e-6 * abs(gs)
+    # l: H at l +- h on H's structure and pivots
+    hl = 1e-6
+    olp = KernelOperator(prm(hm, ell=0.7 + hl), like=op, refine_tol=1e-13)
+    olm = KernelOperator(prm(hm, ell=0.7 - hl), like=op, refine_tol=1e-13)
+    fd_l = (loss(olp, b0) - loss(olm, b0)) / (2 * hl)
+    assert abs(fd_l - gl) <= 1e-6 * abs(gl), (fd_l, gl)
+
+
+def test_new_like_replays_the_structure():
+    # the same kernel on the same pivots reproduces H bit for bit; another
+    # parameter keeps the partition and ranks and stays an accurate H-matrix
+    import hmatrix as hm
+    c, H = hm.NewHmat(prm(hm, keep=True))
+    H2 = hm.new_like(H, prm(hm))
+    assert np.array_equal(H.leaves(), H2.leaves())
+    x = np.random.default_rng(8).standard_normal(N)
+    assert np.array_equal(H * x, H2 * x)
+    H3 = hm.new_like(H, prm(hm, ell=0.71, sigma2=0.02))
+    assert np.array_equal(H.leaves()[:, :5], H3.leaves()[:, :5])
+    K3 = hm.FullMat(hm.Gauss(0.71), c.X, c.X) + 0.02 * np.eye(N)
+    assert np.linalg.norm(H3 * x - K3 @ x) <= 1e-8 * np.linalg.norm(K3 @ x)
+    bad = prm(hm)
+    bad.MaxRank = 12                      # only the kernel and the shift may change
+    with pytest.raises(hm.HmError):
+        hm.new_like(H3, bad)
 
 
 def test_matvec_and_solve_adjoints_multi_column():
