@@ -377,6 +377,29 @@ int hm_matvec(hm_handle* h, const double* X, double* Y, int64_t ncols, int32_t t
   return tc_status(h, st);
 }
 
+int hm_residual(hm_handle* h, const double* X, const double* B, double* R, int64_t ncols, int32_t trans,
+                uint32_t flags, void* stream) {
+  if (!h || !X || !B || !R || ncols < 0) return fail(HM_ERR_ARG, "invalid argument");
+  if (h->factorized && !h->lu) return fail(HM_ERR_STATE, "H is factorised");
+  DeviceGuard g(h->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  const int64_t n = h->n;
+  if (ncols == 0) return HM_OK;
+  auto run = [&](const double* dx, const double* db, double* dr) -> int {
+    for (int64_t q = 0; q < ncols; ++q) HM_TRY(residual_device(h, dx + q * n, db + q * n, dr + q * n, trans ? 1 : 0, st));
+    return HM_OK;
+  };
+  if (flags & HM_FLAG_DEVICE_PTRS) return run(X, B, R);
+  IoBuf io{h};
+  HM_TRY(io.get(sizeof(double) * 3 * n * ncols));
+  HM_CUDA_TRY(cudaMemcpyAsync(io.ptr, X, sizeof(double) * n * ncols, cudaMemcpyHostToDevice, st));
+  HM_CUDA_TRY(cudaMemcpyAsync(io.ptr + n * ncols, B, sizeof(double) * n * ncols, cudaMemcpyHostToDevice, st));
+  HM_TRY(run(io.ptr, io.ptr + n * ncols, io.ptr + 2 * n * ncols));
+  HM_CUDA_TRY(cudaMemcpyAsync(R, io.ptr + 2 * n * ncols, sizeof(double) * n * ncols, cudaMemcpyDeviceToHost, st));
+  HM_CUDA_TRY(cudaStreamSynchronize(st));
+  return HM_OK;
+}
+
 int hm_tc_selftest(int32_t kind, int32_t a_mn, int32_t nc, const float* A, const float* B, float* D) {
   if (!A || !B || !D) return fail(HM_ERR_ARG, "invalid argument");
   int ndev = 0;

@@ -501,6 +501,9 @@ void free_handle_data(hm_handle* h) {
   fr(h->d_tc);
   fr(h->d_tc_err);
   fr(h->d_piv);
+  fr(h->d_dd);
+  h->d_dd = nullptr;
+  h->dd_bytes = 0;
   h->d_piv = nullptr;
   h->piv_count = 0;
   free_tc_plan(h->tc_fwd);

@@ -215,6 +215,8 @@ struct hm_handle {
   void* d_tc = nullptr;            // their X and Z tiles
   size_t tc_bytes = 0;
   int* d_tc_err = nullptr;         // error word of their bounded waits
+  void* d_dd = nullptr;            // compensated residual: z as hi + lo
+  size_t dd_bytes = 0;
   int32_t* d_piv = nullptr;        // aca2 pivots (row, column) of every step, when kept
   int64_t piv_count = 0;
 
@@ -281,6 +283,8 @@ int matvec_multi_tc(hm_handle* h, const double* d_x, double* d_y, int64_t ncols,
 int tc_status(hm_handle* h, cudaStream_t st);
 int tc_selftest(int kind, int a_mn, int nc, const float* A, const float* B, float* D);
 void free_tc_plan(TcPlan*& p);
+// r = b - H x (trans: b - H' x) with compensated sums (hm_matvec.cu)
+int residual_device(hm_handle* h, const double* d_x, const double* d_b, double* d_r, int trans, cudaStream_t st);
 int exact_rows_device(hm_handle* h, const int64_t* d_rows, int64_t nrows,
                       const double* d_x, double* d_y, cudaStream_t st);
 

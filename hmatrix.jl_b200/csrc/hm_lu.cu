@@ -2582,15 +2582,10 @@ int lu_solve_refined(hm_handle* h, const double* d_b, double* d_x, int64_t ncols
   status = norms(Bv, nrm, hb);
   if (status == HM_OK) status = lu_solve_device(h, d_b, d_x, ncols, trans, st);
   for (; status == HM_OK; ++it) {
+    // r = b - H x, summed in twice the FP64 precision
     for (int64_t q = 0; q < ncols && status == HM_OK; ++q)
-      status = matvec_device(h, d_x + q * n, r + q * n, trans, st);
+      status = residual_device(h, d_x + q * n, d_b + q * n, r + q * n, trans, st);
     if (status != HM_OK) break;
-    try {
-      axpby(c, Rv, Bv, 1.0, -1.0);                    // r = b - H x
-    } catch (const LuError& e) {
-      status = fail(e.code, e.what());
-      break;
-    }
     status = norms(Rv, nrm + ncols, hr);
     if (status != HM_OK) break;
     worst = 0.0;

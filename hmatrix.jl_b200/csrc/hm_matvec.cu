@@ -545,6 +545,128 @@ int matvec_device(hm_handle* h, const double* d_x, double* d_y, int trans, cudaS
 }
 
 // ---------------------------------------------------------------------------
+// residual r = b - H x with compensated (double-double) sums, for iterative
+// refinement: every product is split exactly (TwoProduct by FMA) and every
+// sum carries its rounding error (TwoSum), the dot product and sum algorithms
+// of Ogita, Rump & Oishi (2005), "Accurate sum and dot product".  The result
+// is as accurate as if H x were summed in twice the FP64 precision, so the
+// refinement is not stopped by the rounding of H x near b.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  s = a + b;
+  const double bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+__device__ __forceinline__ void dd_add_prod(double& p, double& c, double a, double b) {
+  const double h = a * b;
+  const double r = fma(a, b, -h);          // a b = h + r exactly
+  double q;
+  two_sum(p, h, p, q);
+  c += q + r;
+}
+
+// z = F1' x per low-rank leaf and rank, as hi + lo; one warp per leaf
+template <typename T>
+__global__ void __launch_bounds__(256) mvdd_phase1_kernel(const P1Desc* __restrict__ d, int64_t nd,
+                                                          const T* __restrict__ pool, const double* __restrict__ x,
+                                                          double* __restrict__ zh, double* __restrict__ zl) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t b = gw; b < nd; b += nw) {
+    const P1Desc D = d[b];
+    for (int r = 0; r < D.k; ++r) {
+      const T* f = pool + D.off + (int64_t)r * D.stride;
+      double p = 0.0, c = 0.0;
+      for (uint32_t j = lane; j < D.len; j += 32) dd_add_prod(p, c, from_store<T>(f[j]), x[D.seg0 + j]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double p2 = __shfl_xor_sync(0xffffffffu, p, o), c2 = __shfl_xor_sync(0xffffffffu, c, o);
+        double q;
+        two_sum(p, p2, p, q);
+        c += c2 + q;
+      }
+      if (lane == 0) {
+        const double hi = p + c;
+        zh[D.zoff + r] = hi;
+        zl[D.zoff + r] = c - (hi - p);
+      }
+    }
+  }
+}
+
+// r = b - (sum over the window's leaves) per output row, one thread a row
+template <typename T, typename TD>
+__global__ void __launch_bounds__(512) mvdd_phase2_kernel(const MvWin* __restrict__ win,
+                                                          const P2Desc* __restrict__ d, const T* __restrict__ rk,
+                                                          const TD* __restrict__ dn, const double* __restrict__ zh,
+                                                          const double* __restrict__ zl,
+                                                          const double* __restrict__ x,
+                                                          const double* __restrict__ bvec, double* __restrict__ rvec) {
+  const MvWin W = win[blockIdx.x];
+  for (uint32_t row = threadIdx.x; row < W.nrows; row += blockDim.x) {
+    double p = 0.0, c = 0.0;
+    for (uint32_t e = W.begin; e < W.end; ++e) {
+      const P2Desc D = d[e];
+      const int lr = (int)row - D.row_off;
+      if (lr < 0 || lr >= (int)D.m) continue;
+      if (D.type == P2_RK) {
+        for (uint32_t q = 0; q < D.cnt; ++q) {
+          const double v = from_store<T>(rk[D.off + (uint64_t)q * D.ld + lr]);
+          dd_add_prod(p, c, v, zh[D.aux + q]);
+          c = fma(v, zl[D.aux + q], c);
+        }
+      } else if (D.type == P2_DENSE) {
+        for (uint32_t q = 0; q < D.cnt; ++q)
+          dd_add_prod(p, c, (double)dn[D.off + (uint64_t)q * D.ld + lr], x[D.aux + q]);
+      } else {
+        for (uint32_t q = 0; q < D.cnt; ++q)
+          dd_add_prod(p, c, (double)dn[D.off + (uint64_t)q + (uint64_t)lr * D.ld], x[D.aux + q]);
+      }
+    }
+    const uint32_t i = W.row0 + row;
+    double t, q;
+    two_sum(bvec[i], -p, t, q);
+    rvec[i] = t + (q - c);
+  }
+}
+
+template <typename T>
+static int residual_t(hm_handle* h, const double* d_x, const double* d_b, double* d_r, int trans, cudaStream_t st) {
+  using TD = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
+  const MvPlan& P = trans ? h->bwd : h->fwd;
+  const size_t need = sizeof(double) * 2 * (size_t)std::max<int64_t>(h->zlen, 1);
+  if (h->dd_bytes < need) {
+    if (h->d_dd) cudaFree(h->d_dd);
+    h->d_dd = nullptr;
+    h->dd_bytes = 0;
+    cudaError_t e = cudaMalloc(&h->d_dd, need);
+    if (e != cudaSuccess) return fail(HM_ERR_OOM, std::string("residual buffers: ") + cudaGetErrorString(e));
+    h->dd_bytes = need;
+  }
+  double* zh = (double*)h->d_dd;
+  double* zl = zh + std::max<int64_t>(h->zlen, 1);
+  if (P.np1 > 0) {
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+    const int64_t blocks = std::min<int64_t>((P.np1 + 7) / 8, (int64_t)nsm * 8);
+    mvdd_phase1_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(P.d_p1, P.np1, (const T*)h->d_rk, d_x, zh, zl);
+  }
+  mvdd_phase2_kernel<T, TD><<<(unsigned)P.nwin, 512, 0, st>>>(P.d_win, P.d_p2, (const T*)h->d_rk,
+                                                              (const TD*)h->d_dense, zh, zl, d_x, d_b, d_r);
+  HM_CUDA_TRY(cudaGetLastError());
+  return HM_OK;
+}
+
+int residual_device(hm_handle* h, const double* d_x, const double* d_b, double* d_r, int trans, cudaStream_t st) {
+  switch (h->storage) {
+    case HM_F64: return residual_t<double>(h, d_x, d_b, d_r, trans, st);
+    case HM_F32: return residual_t<float>(h, d_x, d_b, d_r, trans, st);
+    default: return residual_t<__nv_bfloat16>(h, d_x, d_b, d_r, trans, st);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // exact FP64 rows (K14): y_i = sum_j K(x_rows[i], x_j) x_j + shift * x_rows[i]
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(512) exact_rows_kernel(KernelDesc kd, const double* __restrict__ geom, int64_t n,

@@ -32,7 +32,7 @@ __all__ = [
     "Hparams", "Params", "NewHmat", "FullMat", "Hmat", "lu", "lu_", "getl", "getu", "info",
     "Cauchy", "InvQuad", "Gauss", "Kernel", "Cluster", "construct_cluster", "HmError",
     "aca_wrapper", "F64", "F32", "BF16", "new_on_cluster", "load", "coarsening", "CauchyDP", "InvQuadDP", "GaussDP",
-    "lu_batch", "lu_batch_", "solve_batch", "solve_refined_batch", "matvec_batch", "gmres", "bicgstab", "new_like",
+    "lu_batch", "lu_batch_", "solve_batch", "solve_refined_batch", "matvec_batch", "gmres", "bicgstab", "gmres_ir", "new_like",
 ]
 
 F64, F32, BF16 = _lib.HM_F64, _lib.HM_F32, _lib.HM_BF16
@@ -210,6 +210,29 @@ class Hmat:
         # v*H  (src/harithm.jl:331-337): rows of v times H = (H' v')'
         v = np.atleast_2d(np.asarray(x, dtype=np.float64))
         return self.matvec(v.T, trans=True).T
+
+    def residual(self, x, b, trans=False):
+        """b - H x (b - H' x) summed in twice the FP64 precision (hm_residual):
+        the residual of iterative refinement.  numpy arrays or CUDA float64
+        tensors (n or n x k)."""
+        try:
+            import torch
+            if isinstance(x, torch.Tensor):
+                X = x.reshape(self.n, -1).t().contiguous()
+                B = b.reshape(self.n, -1).t().contiguous()
+                R = torch.empty_like(X)
+                check(lib().hm_residual(self._h, C.c_void_p(X.data_ptr()), C.c_void_p(B.data_ptr()),
+                                        C.c_void_p(R.data_ptr()), X.shape[0], int(bool(trans)),
+                                        _lib.HM_FLAG_DEVICE_PTRS, _torch_stream()))
+                return R.t().reshape(x.shape)
+        except ImportError:
+            pass
+        x = np.asarray(x, dtype=np.float64)
+        X = np.asfortranarray(x.reshape(self.n, -1))
+        B = np.asfortranarray(np.asarray(b, dtype=np.float64).reshape(self.n, -1))
+        R = np.zeros_like(X, order="F")
+        check(lib().hm_residual(self._h, _ptr(X), _ptr(B), _ptr(R), X.shape[1], int(bool(trans)), 0, None))
+        return R.reshape(x.shape)
 
     def exact_rows(self, rows, x):
         """Exact FP64 rows of (K + shift I) x: the dense FullMat oracle for sampled rows."""
@@ -542,4 +565,4 @@ def aca_wrapper(A, eps, rank):
     return Uf[:, :M].copy(), Vf[:, :M].copy(), R
 
 
-from .krylov import bicgstab, gmres  # noqa: E402  (src/tools.jl:7-65)
+from .krylov import bicgstab, gmres, gmres_ir  # noqa: E402  (src/tools.jl:7-65)

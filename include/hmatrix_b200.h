@@ -219,6 +219,16 @@ int hm_status(hm_handle* h, void* stream);
  * nc = 16 or 64.  No counterpart in the reference. */
 int hm_tc_selftest(int32_t kind, int32_t a_mn, int32_t nc, const float* A, const float* B, float* D);
 
+/* R = B - H*X (trans=0) or B - H'*X (trans=1) for n x ncols column-major
+ * blocks, every product and sum carried in twice the FP64 precision (error-free
+ * TwoProduct/TwoSum, Ogita-Rump-Oishi 2005): the residual of iterative
+ * refinement, exact to the last bits of R even where H*X nearly cancels B.
+ * hm_solve_refined uses it; so does the GMRES-based refinement of the host
+ * mirror.  The unfactorised H is read (a factorised handle keeps it).  No
+ * counterpart in the reference. */
+int hm_residual(hm_handle* h, const double* X, const double* B, double* R, int64_t ncols,
+                int32_t trans, uint32_t flags, void* stream);
+
 /* One single-RHS matvec on device pointers with CUDA events between its three
  * launches; ms[0..2] = x staging, phase 1 (z = B'x per low-rank leaf), phase 2
  * (y = sum A z + dense).  Profiling aid; no counterpart in the reference. */
@@ -284,7 +294,8 @@ int hm_solve(hm_handle* h, const double* B, double* X, int64_t ncols,
              uint32_t flags, void* stream);
 
 /* H\y with iterative refinement: x = (LU)^{-1} b, then r = b - H x with the
- * FP64 H-matvec of the unfactorised H (lu! keeps it), x += (LU)^{-1} r, until
+ * compensated H-matvec of hm_residual on the unfactorised H (lu! keeps it),
+ * x += (LU)^{-1} r, until
  * max over columns |r|/|b| <= tol or max_iter refinement steps.  *iters and
  * *relres (may be NULL) report the steps taken and the final residual.
  * No counterpart in the reference (its \ has no refinement). */

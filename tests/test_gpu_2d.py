@@ -38,3 +38,23 @@ def test_2d_mixed_lu_refined_and_adjoint_solve():
     assert np.linalg.norm(Hd.T @ Xt - B) <= 1e-9 * np.linalg.norm(B)
     Xd = np.linalg.solve(D, B)
     assert np.linalg.norm(X - Xd) <= 1e-3 * np.linalg.norm(Xd)
+
+
+def test_2d_gmres_ir_and_adjoint():
+    # GMRES-based refinement (compensated residual, GMRES preconditioned by the
+    # H-LU for the corrections) to 1e-11, forward and transposed
+    import hmatrix as hm
+    rng = np.random.default_rng(5)
+    G = rng.uniform(0, 1, (N, 2))
+    prm = hm.Params(Geom=G, Kernel=hm.Cauchy(1.0), MaxBlock=512, MinBlock=64, MaxRank=32, ConsMethod="aca2",
+                    εComp=1e-9, Tree="bisect", Shift=1e-3, εTruncLU=1e-6)
+    c, H = hm.NewHmat(prm)
+    L = hm.lu(H)
+    b = rng.standard_normal(N)
+    x, it, rr = hm.gmres_ir(H, L, b, tol=1e-11)
+    assert rr <= 1e-11
+    Hd = H.to_dense()
+    assert np.linalg.norm(Hd @ x - b) <= 1e-10 * np.linalg.norm(b)
+    xt, it2, rr2 = hm.gmres_ir(H, L, b, tol=1e-11, trans=True)
+    assert rr2 <= 1e-11
+    assert np.linalg.norm(Hd.T @ xt - b) <= 1e-10 * np.linalg.norm(b)
