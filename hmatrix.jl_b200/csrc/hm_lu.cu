@@ -15,7 +15,6 @@
 #include "hm_lowrank.cuh"
 #include "hm_core.cuh"
 
-#include <cublas_v2.h>
 
 #include <algorithm>
 #include <map>
@@ -106,6 +105,77 @@ __global__ void __launch_bounds__(256) lu_gemm_batch_kernel(const GemmJob* __res
   const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
   if (i0 >= J.C.rows || j0 >= J.C.cols) return;
   gemm_tile(J.A, J.B, J.C, J.alpha, J.beta, i0, j0);
+}
+
+// Large products (the tile schedule's B_ik' A_kj cores and Q_i = A_ik W): C
+// tiles of 128 x 128 per CTA, K in steps of 16 through shared memory, 8 x 8
+// outputs per thread (rows tx + 16 u, columns 8 ty + v, so that a warp's
+// stores of column-major C are 128-byte runs).  Tiles are read along whichever
+// stride of the view is 1, so transposed views stay coalesced.
+constexpr int GB_T = 128, GB_K = 16, GB_LD = GB_T + 4;
+__device__ __forceinline__ void gemm_big_tile(const View& A, const View& B, const View& C, double alpha,
+                                              double beta, int i0, int j0) {
+  __shared__ __align__(16) double As[GB_K][GB_LD];
+  __shared__ __align__(16) double Bs[GB_K][GB_LD];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int m = C.rows, n = C.cols, K = A.cols;
+  double acc[8][8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u)
+#pragma unroll
+    for (int v = 0; v < 8; ++v) acc[u][v] = 0.0;
+  for (int k0 = 0; k0 < K; k0 += GB_K) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + 256 * q;
+      int i, kk;
+      if (A.rs == 1) { i = e & 127; kk = e >> 7; } else { kk = e & 15; i = e >> 4; }
+      As[kk][i] = (i0 + i < m && k0 + kk < K) ? A.p[(int64_t)(i0 + i) * A.rs + (int64_t)(k0 + kk) * A.cs] : 0.0;
+      int j;
+      if (B.rs == 1) { kk = e & 15; j = e >> 4; } else { j = e & 127; kk = e >> 7; }
+      Bs[kk][j] = (k0 + kk < K && j0 + j < n) ? B.p[(int64_t)(k0 + kk) * B.rs + (int64_t)(j0 + j) * B.cs] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < GB_K; ++kk) {
+      double a[8], b[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) a[u] = As[kk][tx + 16 * u];
+#pragma unroll
+      for (int v = 0; v < 8; v += 2) {
+        const double2 t = *reinterpret_cast<const double2*>(&Bs[kk][8 * ty + v]);
+        b[v] = t.x;
+        b[v + 1] = t.y;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int v = 0; v < 8; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    const int j = j0 + 8 * ty + v;
+    if (j >= n) continue;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int i = i0 + tx + 16 * u;
+      if (i < m) {
+        double* c = C.p + (int64_t)i * C.rs + (int64_t)j * C.cs;
+        *c = (beta == 0.0) ? alpha * acc[u][v] : fma(alpha, acc[u][v], beta * *c);
+      }
+    }
+  }
+}
+__global__ void __launch_bounds__(256) lu_gemm_big_kernel(View A, View B, View C, double alpha, double beta) {
+  gemm_big_tile(A, B, C, alpha, beta, blockIdx.y * GB_T, blockIdx.x * GB_T);
+}
+__global__ void __launch_bounds__(256) lu_gemm_big_batch_kernel(const GemmJob* __restrict__ jobs) {
+  const GemmJob& J = jobs[blockIdx.z];
+  const int i0 = blockIdx.y * GB_T, j0 = blockIdx.x * GB_T;
+  if (i0 >= J.C.rows || j0 >= J.C.cols) return;
+  gemm_big_tile(J.A, J.B, J.C, J.alpha, J.beta, i0, j0);
 }
 
 // Y = alpha * X + beta * Y (beta == 0: Y is not read)
@@ -410,7 +480,6 @@ struct Ctx {
   int* flags;          // device error bits: 1 rank overflow, 2 non-finite, 4 singular
   double eps_trunc;
   const hm_handle* h;
-  cublasHandle_t blas = nullptr;   // large plain products go to cuBLAS DGEMM
   struct Arena* ar = nullptr;      // when set, temporaries come from this fixed buffer
 };
 
@@ -488,22 +557,13 @@ static BP new_rk(Ctx& c, int m, int n, int32_t s, int32_t t, bool alloc_a = true
 static bool is_leaf_cluster(const Ctx& c, int32_t cl) { return cl >= 0 && c.h->cl_left[cl] < 0; }
 
 // ---- primitive launches --------------------------------------------------
-// a view as a column-major cuBLAS operand (op, leading dimension)
-static bool blas_operand(const View& v, cublasOperation_t& op, int& ld) {
-  if (v.rs == 1 && v.cs >= std::max(v.rows, 1) && v.cs < INT32_MAX) { op = CUBLAS_OP_N; ld = (int)v.cs; return true; }
-  if (v.cs == 1 && v.rs >= std::max(v.cols, 1) && v.rs < INT32_MAX) { op = CUBLAS_OP_T; ld = (int)v.rs; return true; }
-  return false;
-}
 
 static void gemm(Ctx& c, View C, View A, View B, double alpha, double beta) {
   if (C.rows == 0 || C.cols == 0) return;
-  cublasOperation_t oa, ob;
-  int lda, ldb;
-  if (c.blas && A.cols > 0 && (double)C.rows * C.cols * A.cols >= 4.0e6 && C.rs == 1 && C.cs >= C.rows &&
-      blas_operand(A, oa, lda) && blas_operand(B, ob, ldb)) {
-    if (cublasDgemm(c.blas, oa, ob, C.rows, C.cols, A.cols, &alpha, A.p, lda, B.p, ldb, &beta, C.p,
-                    (int)C.cs) != CUBLAS_STATUS_SUCCESS)
-      throw LuError(HM_ERR_CUDA, "cublasDgemm");
+  if (A.cols > 0 && (double)C.rows * C.cols * A.cols >= 4.0e6) {
+    dim3 g((C.cols + GB_T - 1) / GB_T, (C.rows + GB_T - 1) / GB_T);
+    lu_gemm_big_kernel<<<g, 256, 0, c.st>>>(A, B, C, alpha, beta);
+    LU_LAUNCH_CHECK();
     return;
   }
   if (A.cols == 0) {
@@ -1122,12 +1182,14 @@ struct Loader {
 static BP build_tree(Ctx& c, const hm_handle* h, int32_t node, Loader& ld);
 static BP build_from_handle(Ctx& c, const hm_handle* h, int32_t node);
 
-static void gemm_batch(Ctx& c, const std::vector<GemmJob>& jobs) {
+// independent products in one launch; big = true: 128 x 128 tiles
+static void gemm_batch(Ctx& c, const std::vector<GemmJob>& jobs, bool big = false) {
   if (jobs.empty()) return;
+  const int t = big ? GB_T : 32;
   int gx = 1, gy = 1;
   for (auto& j : jobs) {
-    gx = std::max(gx, (j.C.cols + 31) / 32);
-    gy = std::max(gy, (j.C.rows + 31) / 32);
+    gx = std::max(gx, (j.C.cols + t - 1) / t);
+    gy = std::max(gy, (j.C.rows + t - 1) / t);
   }
   for (size_t b = 0; b < jobs.size(); b += 65535) {
     const size_t nb = std::min<size_t>(65535, jobs.size() - b);
@@ -1135,7 +1197,8 @@ static void gemm_batch(Ctx& c, const std::vector<GemmJob>& jobs) {
     tmp.st = c.st;
     std::vector<GemmJob> part(jobs.begin() + b, jobs.begin() + b + nb);
     GemmJob* d = upload_jobs(c, tmp, part);
-    lu_gemm_batch_kernel<<<dim3(gx, gy, (unsigned)nb), 256, 0, c.st>>>(d);
+    if (big) lu_gemm_big_batch_kernel<<<dim3(gx, gy, (unsigned)nb), 256, 0, c.st>>>(d);
+    else lu_gemm_batch_kernel<<<dim3(gx, gy, (unsigned)nb), 256, 0, c.st>>>(d);
     LU_LAUNCH_CHECK();
   }
 }
@@ -1575,7 +1638,7 @@ struct StepQ {
 };
 
 static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vector<int32_t>& gcl,
-                        const std::vector<int32_t>& dnode, cudaStream_t look, cublasHandle_t look_blas) {
+                        const std::vector<int32_t>& dnode, cudaStream_t look) {
   const int T = (int)gcl.size(), cap = c.cap;
   TL.T = T;
   TL.start.resize(T);
@@ -1670,44 +1733,21 @@ static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vecto
     out.qbase = (double*)dmalloc(x, hold, sizeof(double) * (size_t)qtot);
     int64_t qo = 0;
     for (int i = k + 1; i < T; ++i) { Q[i] = out.qbase + qo; qo += TL.size[i] * (int64_t)R; }
-    // tiles of equal height: one batched cuBLAS product per height
-    std::map<int, std::vector<int>> by_m;
-    for (int i = k + 1; i < T; ++i) by_m[(int)TL.size[i]].push_back(i);
+    // Q_i = A_ik W_i,: for every trailing tile row: one batched launch, with
+    // 128 x 128 tiles once the products are large
     std::vector<GemmJob> gq;
-    for (auto& kv : by_m) {
-      const int mi = kv.first;
-      const std::vector<int>& rows = kv.second;
-      if (x.blas && (double)mi * R * cap * rows.size() >= 4.0e6) {
-        std::vector<const double*> pa, pb;
-        std::vector<double*> pc;
-        for (int i : rows) {
-          pa.push_back(TL.Ai(i, k, cap));
-          pb.push_back(W + (int64_t)(i - k - 1) * cap);
-          pc.push_back(Q[i]);
-        }
-        const double** da = (const double**)dmalloc(x, hold, sizeof(void*) * rows.size());
-        const double** db = (const double**)dmalloc(x, hold, sizeof(void*) * rows.size());
-        double** dc = (double**)dmalloc(x, hold, sizeof(void*) * rows.size());
-        if (cudaMemcpyAsync(da, pa.data(), sizeof(void*) * rows.size(), cudaMemcpyHostToDevice, x.st) ||
-            cudaMemcpyAsync(db, pb.data(), sizeof(void*) * rows.size(), cudaMemcpyHostToDevice, x.st) ||
-            cudaMemcpyAsync(dc, pc.data(), sizeof(void*) * rows.size(), cudaMemcpyHostToDevice, x.st))
-          throw LuError(HM_ERR_CUDA, "pointer upload");
-        const double one = 1.0, zero = 0.0;
-        if (cublasDgemmBatched(x.blas, CUBLAS_OP_N, CUBLAS_OP_N, mi, R, cap, &one, da, mi, db, R, &zero, dc, mi,
-                               (int)rows.size()) != CUBLAS_STATUS_SUCCESS)
-          throw LuError(HM_ERR_CUDA, "cublasDgemmBatched");
-      } else {
-        for (int i : rows) {
-          GemmJob g{};
-          g.A = View{TL.Ai(i, k, cap), 1, mi, mi, cap};
-          g.B = vsub(Wv, (i - k - 1) * cap, 0, cap, R);
-          g.C = View{Q[i], 1, mi, mi, R};
-          g.alpha = 1.0; g.beta = 0.0;
-          gq.push_back(g);
-        }
-      }
+    double macs = 0.0;
+    for (int i = k + 1; i < T; ++i) {
+      const int mi = (int)TL.size[i];
+      GemmJob g{};
+      g.A = View{TL.Ai(i, k, cap), 1, mi, mi, cap};
+      g.B = vsub(Wv, (i - k - 1) * cap, 0, cap, R);
+      g.C = View{Q[i], 1, mi, mi, R};
+      g.alpha = 1.0; g.beta = 0.0;
+      gq.push_back(g);
+      macs += (double)mi * R * cap;
     }
-    gemm_batch(x, gq);
+    gemm_batch(x, gq, macs >= 4.0e6);
   };
   // updates of the trailing diagonal tiles i in [i0, i1) (H-structured targets)
   auto diag_updates = [&](int k, const StepQ& sq, int i0, int i1) {
@@ -1723,7 +1763,6 @@ static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vecto
   };
   Ctx cl = c;
   cl.st = look;
-  cl.blas = look_blas;
   cudaEvent_t ev_up = nullptr, ev_dn = nullptr;
   if (look && (cudaEventCreateWithFlags(&ev_up, cudaEventDisableTiming) != cudaSuccess ||
                cudaEventCreateWithFlags(&ev_dn, cudaEventDisableTiming) != cudaSuccess))
@@ -2213,13 +2252,9 @@ struct LuState {
   int* flags = nullptr;
   int cap = 0;
   cudaStream_t st = nullptr;
-  cublasHandle_t blas = nullptr;
-  void* blas_ws = nullptr;
-  // look-ahead stream of the tile schedule and its cuBLAS handle (blocks made
-  // there keep it as their stream, so it lives as long as the factors)
+  // look-ahead stream of the tile schedule (blocks made there keep it as
+  // their stream, so it lives as long as the factors)
   cudaStream_t look = nullptr;
-  cublasHandle_t look_blas = nullptr;
-  void* look_ws = nullptr;
   std::vector<std::unique_ptr<SolvePlan>> plans;
   ~LuState() {
     if (!plans.empty()) cudaDeviceSynchronize();
@@ -2234,13 +2269,9 @@ struct LuState {
       cudaStreamSynchronize(look);
       cudaStreamDestroy(look);
     }
-    if (blas) cublasDestroy(blas);
-    if (blas_ws) cudaFree(blas_ws);
-    if (look_blas) cublasDestroy(look_blas);
-    if (look_ws) cudaFree(look_ws);
   }
-  // a second stream with its own cuBLAS handle and workspace (nullptr if
-  // either cannot be made: the schedule then runs on one stream)
+  // a second stream (nullptr if it cannot be made: the schedule then runs on
+  // one stream)
   void make_look() {
     if (look) return;
     // high priority: its small kernels are scheduled between the blocks of the
@@ -2250,33 +2281,7 @@ struct LuState {
     if (cudaStreamCreateWithPriority(&look, cudaStreamNonBlocking, greatest) != cudaSuccess) {
       cudaGetLastError();
       look = nullptr;
-      return;
     }
-    if (cublasCreate(&look_blas) != CUBLAS_STATUS_SUCCESS) {
-      look_blas = nullptr;
-      return;
-    }
-    if (cudaMalloc(&look_ws, BLAS_WS) != cudaSuccess) {
-      cudaGetLastError();
-      look_ws = nullptr;
-    }
-    cublasSetStream(look_blas, look);
-    if (look_ws) cublasSetWorkspace(look_blas, look_ws, BLAS_WS);
-  }
-  // cuBLAS on stream s (created on first use).  The handle gets a fixed
-  // workspace so that a captured product allocates nothing; cublasSetStream
-  // resets the workspace, hence it is set again after every stream change.
-  static constexpr size_t BLAS_WS = (size_t)32 << 20;
-  cublasHandle_t blas_on(cudaStream_t s) {
-    if (!blas) {
-      if (cublasCreate(&blas) != CUBLAS_STATUS_SUCCESS) blas = nullptr;
-      if (blas && cudaMalloc(&blas_ws, BLAS_WS) != cudaSuccess) blas_ws = nullptr;
-    }
-    if (blas) {
-      cublasSetStream(blas, s);
-      if (blas_ws) cublasSetWorkspace(blas, blas_ws, BLAS_WS);
-    }
-    return blas;
   }
 };
 
@@ -2350,7 +2355,7 @@ int lu_factor(hm_handle* h) {
   HM_CUDA_TRY(cudaMallocAsync((void**)&S->flags, sizeof(int), h->stream));
   HM_CUDA_TRY(cudaMemsetAsync(S->flags, 0, sizeof(int), h->stream));
   const double eps_lu = h->prm.eps_trunc_lu > 0.0 ? h->prm.eps_trunc_lu : h->prm.eps_trunc;
-  Ctx c{h->stream, S->cap, S->P, S->flags, eps_lu, h, S->blas_on(h->stream)};
+  Ctx c{h->stream, S->cap, S->P, S->flags, eps_lu, h};
   const int mode = h->prm.lu_mode;     // 0 auto, 1 recursion, 2 tiles
   try {
     if (h->kmax > S->cap) throw LuError(HM_ERR_RANK, "a leaf rank exceeds the H-LU rank capacity");
@@ -2360,7 +2365,7 @@ int lu_factor(hm_handle* h) {
     if (tiled) {
       S->tile.reset(new TileLU());
       S->make_look();
-      tile_factor(c, h, *S->tile, gcl, dnode, S->look_blas ? S->look : nullptr, S->look_blas);
+      tile_factor(c, h, *S->tile, gcl, dnode, S->look);
     } else {
       S->root = build_from_handle(c, h, 0);
       lu_rec(c, *S->root);
@@ -2464,7 +2469,7 @@ static void capture_plan(LuState* S, hm_handle* h, SolvePlan* pl, cudaStream_t c
   }
   pl->arena.size = pl->tape.temp_bytes;
   pl->arena.used = 0;
-  Ctx c{cs, S->cap, S->P, S->flags, h->prm.eps_trunc, h, S->blas_on(cs), &pl->arena};
+  Ctx c{cs, S->cap, S->P, S->flags, h->prm.eps_trunc, h, &pl->arena};
   pl->tape.record = false;
   pl->tape.replay = true;
   pl->tape.pos = 0;
@@ -2490,7 +2495,6 @@ static void capture_plan(LuState* S, hm_handle* h, SolvePlan* pl, cudaStream_t c
   pl->tape.replay = false;
   pl->no_graph = !ok;
   cudaStreamDestroy(cs);
-  S->blas_on(caller);
   // the plan's buffers were allocated in the caller's stream order; later
   // calls may come on other streams
   cudaStreamSynchronize(caller);
@@ -2500,7 +2504,7 @@ int lu_solve_device(hm_handle* h, const double* d_b, double* d_x, int64_t ncols,
   LuState* S = h->lu;
   if (!S) return fail(HM_ERR_STATE, "a has not been factorized");
   if (ncols <= 0) return HM_OK;
-  Ctx c{st, S->cap, S->P, S->flags, h->prm.eps_trunc, h, S->blas_on(st)};
+  Ctx c{st, S->cap, S->P, S->flags, h->prm.eps_trunc, h};
   try {
     if (S->tile) ensure_sweep(c, *S->tile);
     if (ncols > SOLVE_GRAPH_MAX_COLS) {
