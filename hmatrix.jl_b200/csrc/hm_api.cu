@@ -137,6 +137,27 @@ int run_batch(hm_handle* const* hs, int64_t count, int32_t nthreads, int32_t* st
   return first;
 }
 
+// Times `calls` launches of fn on the handle's stream (after two untimed
+// ones) and returns the mean milliseconds, or a negative value on error.
+template <typename F>
+float time_calls(hm_handle* h, int calls, F fn) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return -1.f;
+  float ms = -1.f;
+  bool ok = fn() == HM_OK && fn() == HM_OK;
+  if (ok && cudaEventRecord(a, h->stream) == cudaSuccess) {
+    for (int i = 0; i < calls && ok; ++i) ok = fn() == HM_OK;
+    if (ok && cudaEventRecord(b, h->stream) == cudaSuccess && cudaEventSynchronize(b) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, a, b) == cudaSuccess)
+      ms /= calls;
+    else
+      ms = -1.f;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return ms;
+}
+
 }  // namespace
 }  // namespace hm
 
@@ -285,6 +306,10 @@ int hm_info(const hm_handle* h, hm_info_t* o) {
   o->matvec_bytes = (int64_t)eb * o->rk_entries + (int64_t)deb * o->dense_entries + 16 * h->n;
   o->n_row_groups = h->fwd.nwin;
   o->factorized = h->factorized ? 1 : 0;
+  o->tune_p2_split = h->tune.p2_split;
+  o->tune_p1_waves = h->tune.p1_waves;
+  for (int b = 0; b < 3; ++b) o->tune_tc_nc[b] = h->tune.tc_nc[b];
+  o->tuned = h->tune.tuned;
   if (h->lu) lu_describe(h, &o->lu_tiles, &o->lu_rank_cap);
   return HM_OK;
 }
@@ -405,6 +430,56 @@ int hm_tc_selftest(int32_t kind, int32_t a_mn, int32_t nc, const float* A, const
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(HM_ERR_CUDA, "no CUDA device");
   return tc_selftest(kind, a_mn, nc, A, B, D);
+}
+
+int hm_autotune(hm_handle* h, int64_t ncols, int32_t calls, double* times) {
+  if (!h || ncols < 1 || calls < 1) return fail(HM_ERR_ARG, "invalid argument");
+  if (h->factorized) return fail(HM_ERR_STATE, "H is factorised");
+  DeviceGuard g(h->device);
+  const int64_t n = h->n;
+  double* buf = nullptr;
+  cudaError_t e = cudaMalloc(&buf, sizeof(double) * 2 * (size_t)n * (size_t)ncols);
+  if (e != cudaSuccess) return fail(HM_ERR_OOM, std::string("autotune buffers: ") + cudaGetErrorString(e));
+  struct Free { double* p; ~Free() { cudaFree(p); } } fr{buf};
+  HM_CUDA_TRY(cudaMemsetAsync(buf, 0, sizeof(double) * (size_t)n * (size_t)ncols, h->stream));
+  double* x = buf;
+  double* y = buf + n * ncols;
+  // single right-hand side: phase-2 split x phase-1 waves
+  float best = -1.f;
+  hm_handle::Tune keep = h->tune;
+  const int splits[3] = {2, 4, 8}, waves[3] = {1, 2, 4};
+  if (times)
+    for (int i = 0; i < 12; ++i) times[i] = -1.0;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      h->tune.p2_split = splits[a];
+      h->tune.p1_waves = waves[b];
+      const float ms = time_calls(h, calls, [&] { return matvec_device(h, x, y, 0, h->stream); });
+      if (ms < 0) { h->tune = keep; return fail(HM_ERR_CUDA, "autotune: a timed matvec failed"); }
+      if (times) times[3 * a + b] = ms;
+      if (best < 0 || ms < best) { best = ms; keep.p2_split = splits[a]; keep.p1_waves = waves[b]; }
+    }
+  h->tune = keep;
+  // several columns on the tensor cores: the column block
+  if (ncols > 1 && (h->storage == HM_F32 || h->storage == HM_BF16)) {
+    const int bucket = ncols <= 16 ? 0 : (ncols <= 32 ? 1 : 2);
+    float bm = -1.f;
+    int bnc = 0;
+    const int ncs[3] = {16, 32, 64};
+    for (int q = 0; q < 3; ++q) {
+      const int nc = ncs[q];
+      if ((bucket == 0 && nc > 16) || (bucket == 1 && nc > 32)) continue;
+      h->tune.tc_nc[bucket] = nc;
+      const float ms = time_calls(h, calls, [&] { return matvec_multi_device(h, x, y, ncols, 0, h->stream); });
+      if (ms < 0) { h->tune.tc_nc[bucket] = 0; return fail(HM_ERR_CUDA, "autotune: a timed block product failed"); }
+      if (times) times[9 + q] = ms;
+      if (bm < 0 || ms < bm) { bm = ms; bnc = nc; }
+    }
+    h->tune.tc_nc[bucket] = bnc;
+    HM_TRY(tc_status(h, h->stream));
+  }
+  h->tune.tuned = 1;
+  return HM_OK;
 }
 
 int hm_status(hm_handle* h, void* stream) {

@@ -220,6 +220,12 @@ struct hm_handle {
   int32_t* d_piv = nullptr;        // aca2 pivots (row, column) of every step, when kept
   int64_t piv_count = 0;
 
+  struct Tune {                    // launch shapes chosen by hm_autotune (hm_api.cu)
+    int p2_split = 4;              // phase-2 CTAs per 1024-row window (2, 4, 8)
+    int p1_waves = 1;              // phase-1 grid in resident waves (1, 2, 4)
+    int tc_nc[3] = {0, 0, 0};      // tensor-core column block for c <= 16, <= 32, > 32 (0: by c)
+    int tuned = 0;
+  } tune;
   hm::LuState* lu = nullptr;       // set once factorised
   bool factorized = false;
 };

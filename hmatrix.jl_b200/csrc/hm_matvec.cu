@@ -169,13 +169,13 @@ __global__ void __launch_bounds__(256, HM_P1_MINB) mv_phase1_kernel(const P1Desc
 // multiple of 4 elements and 16 bytes, padding rows hold zeros).
 // ---------------------------------------------------------------------------
 constexpr int P2_NB = 32;      // descriptors staged per round
-#ifndef HM_P2_SPLIT
-#define HM_P2_SPLIT 4
-#endif
-constexpr int P2_SPLIT = HM_P2_SPLIT;              // CTAs per window
-constexpr int P2_CROWS = MV_WROWS / P2_SPLIT;      // rows of one CTA
-constexpr int P2_WARPS = P2_CROWS / 128;           // 32 lanes x 4 rows a warp
-constexpr int P2_EMAX = 1024 / P2_SPLIT;           // expanded (leaf, column) entries per sub-round
+// SPLIT (2, 4 or 8 CTAs per 1024-row window) is chosen per handle by the
+// autotuner (hm_autotune); 4 until then
+template <int SPLIT> struct P2Shape {
+  static constexpr int CROWS = MV_WROWS / SPLIT;   // rows of one CTA
+  static constexpr int WARPS = CROWS / 128;        // 32 lanes x 4 rows a warp
+  static constexpr int EMAX = 1024 / SPLIT;        // expanded (leaf, column) entries per sub-round
+};
 constexpr uint64_t P2_DENSE_FLAG = 1ull << 63;
 
 // 4 consecutive rows of one column are loaded as raw words and converted to
@@ -247,14 +247,15 @@ template <> struct Row4<__nv_bfloat16> {        // dense leaves: float (raw floa
   }
 };
 
-template <typename T, typename TD>
-__global__ void __launch_bounds__(P2_WARPS * 32) mv_phase2_kernel(const MvWin* __restrict__ win,
+template <typename T, typename TD, int SPLIT>
+__global__ void __launch_bounds__(P2Shape<SPLIT>::WARPS * 32) mv_phase2_kernel(const MvWin* __restrict__ win,
                                                                   const P2Desc* __restrict__ d,
                                                                   const T* __restrict__ rk, const TD* __restrict__ dn,
                                                                   const double* __restrict__ z,
                                                                   const double* __restrict__ x,
                                                                   double* __restrict__ y) {
   constexpr int U = Row4<T>::U;
+  constexpr int P2_SPLIT = SPLIT, P2_CROWS = P2Shape<SPLIT>::CROWS, P2_EMAX = P2Shape<SPLIT>::EMAX;
   __shared__ P2Desc sd[P2_NB];
   __shared__ int spre[P2_NB + 1];
   __shared__ uint64_t e_off[P2_EMAX];
@@ -523,14 +524,22 @@ static int matvec_t(hm_handle* h, const double* d_x, double* d_y, int trans, cud
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mv_phase1_kernel<T>, 256, 0) != cudaSuccess ||
         per_sm < 1)
       per_sm = 1;
-    int64_t blocks = std::min<int64_t>((P.np1 + 7) / 8, (int64_t)nsm * per_sm);
+    int64_t blocks = std::min<int64_t>((P.np1 + 7) / 8, (int64_t)nsm * per_sm * std::max(1, h->tune.p1_waves));
     mv_phase1_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(P.d_p1, P.np1, (const T*)h->d_rk, xs, stride, h->d_z);
   }
   if (ev) HM_CUDA_TRY(cudaEventRecord(ev[2], st));
   // dense leaves are FP64 with FP64 factors and FP32 otherwise
   using TD = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
-  mv_phase2_kernel<T, TD><<<(unsigned)(P.nwin * P2_SPLIT), P2_WARPS * 32, 0, st>>>(P.d_win, P.d_p2, (const T*)h->d_rk,
-                                                            (const TD*)h->d_dense, h->d_z, d_x, d_y);
+  auto p2 = [&](auto split) {
+    constexpr int S = decltype(split)::value;
+    mv_phase2_kernel<T, TD, S><<<(unsigned)(P.nwin * S), P2Shape<S>::WARPS * 32, 0, st>>>(
+        P.d_win, P.d_p2, (const T*)h->d_rk, (const TD*)h->d_dense, h->d_z, d_x, d_y);
+  };
+  switch (h->tune.p2_split) {
+    case 2: p2(std::integral_constant<int, 2>{}); break;
+    case 8: p2(std::integral_constant<int, 8>{}); break;
+    default: p2(std::integral_constant<int, 4>{});
+  }
   if (ev) HM_CUDA_TRY(cudaEventRecord(ev[3], st));
   HM_CUDA_TRY(cudaGetLastError());
   return HM_OK;

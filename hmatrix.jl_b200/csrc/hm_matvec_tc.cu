@@ -902,10 +902,15 @@ static int launch_tc(hm_handle* h, TcPlan& P, const double* d_x, double* d_y, in
   return HM_OK;
 }
 
+// column block NC: the autotuner's choice for this many columns, else the
+// smallest block of 16, 32, 64 that holds them
 template <typename T>
 static int tc_dispatch(hm_handle* h, TcPlan& P, const double* d_x, double* d_y, int64_t ncols, cudaStream_t st) {
-  if (ncols <= 16) return launch_tc<T, 16>(h, P, d_x, d_y, ncols, st);
-  if (ncols <= 32) return launch_tc<T, 32>(h, P, d_x, d_y, ncols, st);
+  const int bucket = ncols <= 16 ? 0 : (ncols <= 32 ? 1 : 2);
+  int nc = h->tune.tc_nc[bucket];
+  if (nc == 0) nc = bucket == 0 ? 16 : (bucket == 1 ? 32 : 64);
+  if (nc == 16) return launch_tc<T, 16>(h, P, d_x, d_y, ncols, st);
+  if (nc == 32) return launch_tc<T, 32>(h, P, d_x, d_y, ncols, st);
   return launch_tc<T, 64>(h, P, d_x, d_y, ncols, st);
 }
 

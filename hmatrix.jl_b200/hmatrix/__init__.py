@@ -211,6 +211,23 @@ class Hmat:
         v = np.atleast_2d(np.asarray(x, dtype=np.float64))
         return self.matvec(v.T, trans=True).T
 
+    def autotune(self, ncols=1, calls=5):
+        """Choose the matvec launch shapes on this H-matrix's own data
+        (hm_autotune); returns the timing table {name: ms} and the choice."""
+        t = np.zeros(12)
+        check(lib().hm_autotune(self._h, int(ncols), int(calls), _ptr(t)))
+        table = {}
+        for a, sp in enumerate((2, 4, 8)):
+            for b, wv in enumerate((1, 2, 4)):
+                table["split%d_waves%d" % (sp, wv)] = float(t[3 * a + b])
+        for q, nc in enumerate((16, 32, 64)):
+            if t[9 + q] >= 0:
+                table["tc_nc%d_cols%d" % (nc, ncols)] = float(t[9 + q])
+        o = self.info()
+        choice = {"p2_split": o.tune_p2_split, "p1_waves": o.tune_p1_waves,
+                  "tc_nc": [int(v) for v in o.tune_tc_nc]}
+        return table, choice
+
     def residual(self, x, b, trans=False):
         """b - H x (b - H' x) summed in twice the FP64 precision (hm_residual):
         the residual of iterative refinement.  numpy arrays or CUDA float64

@@ -121,7 +121,12 @@ typedef struct hm_info_t {
     int64_t factorized;       /* 1 after lu!                                   */
     int64_t lu_tiles;         /* after lu!: tiles of the tile schedule (0: the recursion ran) */
     int64_t lu_rank_cap;      /* after lu!: column capacity of the low-rank factors */
-    int64_t reserved[2];
+    int64_t tune_p2_split;    /* launch shapes of the matvec (hm_autotune): CTAs per
+                                 1024-row window of phase 2 (2, 4, 8)             */
+    int64_t tune_p1_waves;    /* phase-1 grid in resident waves (1, 2, 4)       */
+    int64_t tune_tc_nc[3];    /* tensor-core column block for <= 16, <= 32 and
+                                 more columns (0: not tuned, the default rule)    */
+    int64_t tuned;            /* 1 after hm_autotune                              */
 } hm_info_t;
 
 typedef struct hm_handle hm_handle;
@@ -204,6 +209,17 @@ int hm_to_dense(const hm_handle* h, double* out, uint32_t flags);
  * device-pointer calls. */
 int hm_matvec(hm_handle* h, const double* X, double* Y, int64_t ncols,
               int32_t trans, uint32_t flags, void* stream);
+
+/* Autotuner of the matvec launch shapes on this handle's own data: times
+ * `calls` matvecs (CUDA events, after two untimed ones) for every phase-2
+ * split (2, 4, 8 CTAs per window) and phase-1 grid (1, 2, 4 resident waves)
+ * and keeps the fastest; with ncols > 1 and FP32/BF16 factors, also the
+ * tensor-core column block (16, 32, 64) for that many columns.  The choice
+ * stays with the handle (hm_info reports it).  times (may be NULL) receives 12
+ * mean milliseconds: [3 a + b] for split (2, 4, 8)[a] and waves (1, 2, 4)[b],
+ * [9 + q] for column block (16, 32, 64)[q] (-1: not tried).  No counterpart in
+ * the reference. */
+int hm_autotune(hm_handle* h, int64_t ncols, int32_t calls, double* times);
 
 /* Waits for `stream` (NULL: the handle's stream) and reports, once, whether a
  * bounded wait inside the tensor-core kernels gave up since the last check

@@ -27,7 +27,7 @@ def test_library_exports_header():
 def test_struct_layouts():
     from hmatrix import _lib
     assert C.sizeof(_lib.hm_params) == 4 * 2 + 8 * 4 + 4 * 8 + 4 * 6
-    assert C.sizeof(_lib.hm_info_t) == 8 * 16
+    assert C.sizeof(_lib.hm_info_t) == 8 * 20
 
 
 def test_defaults_and_errors_without_gpu():
