@@ -561,6 +561,7 @@ def kmeans_leg(a, torch, peak):
     H = hm.new_on_cluster(prm, c)
     t_build = time.perf_counter() - t0
     info = H.info()
+    _, tune_choice = H.autotune(1, calls=3)
     ms, ph, ck, e2e_ms, rel = measure(H, a, torch, None, 1)
     bytes_mv = 8 * info.rk_entries + 8 * info.dense_entries + 16 * n
     sz = c.e - c.s
@@ -571,7 +572,8 @@ def kmeans_leg(a, torch, peak):
            "n_rk": info.n_rk, "n_dense": info.n_dense, "rk_entries": info.rk_entries,
            "dense_entries": info.dense_entries, "max_rank": info.max_rank, "algorithmic_bytes": bytes_mv,
            "ms_per_matvec": ms, "GB/s": gbs, "frac_of_peak": gbs / peak, "phase_ms": [float(v) for v in ph],
-           "e2e_GB/s": bytes_mv / (e2e_ms * 1e-3) / 1e9, "rel_err_vs_exact_fp64_rows": rel, "clocks": ck}
+           "e2e_GB/s": bytes_mv / (e2e_ms * 1e-3) / 1e9, "rel_err_vs_exact_fp64_rows": rel, "clocks": ck,
+           "autotune": tune_choice}
     del H
     torch.cuda.empty_cache()
     return out
@@ -643,6 +645,8 @@ def run_ours(a):
     shard = world > 1 and not a.replicas
     c, H, t_build = build(a.n, a.storage, (rank, world) if shard else None)
     info = H.info()
+    # launch shapes from the autotuner, on this matrix (untimed)
+    tune_table, tune_choice = H.autotune(1, calls=5)
     ms, ph, ck, e2e_ms, rel = measure(H, a, torch, dist, world, shard)
     eb = {"f64": 8, "f32": 4, "bf16": 2}[a.storage]
     deb = 8 if a.storage == "f64" else 4
@@ -692,6 +696,11 @@ def run_ours(a):
             extra[s] = {"GB/s": b2 / (ms2 * 1e-3) / 1e9, "ms_per_step": ms2, "frac_of_peak": b2 / (ms2 * 1e-3) / 1e9 / peak,
                         "rel_err_4096_rows": rel2, "phase_ms": [float(v) for v in ph2], "build_s": tb2}
             if cols:
+                tuned = {}
+                for cc in cols:                 # the tensor-core column block for each width
+                    tt, ch = H2.autotune(cc, calls=3)
+                    tuned[str(cc)] = {"choice": ch["tc_nc"], "ms": {k: v for k, v in tt.items() if k.startswith("tc_")}}
+                extra[s]["autotune"] = tuned
                 mr = multi_rhs_leg(H2, cols, max(3, min(a.steps, 10)), torch, b2, exact_rows=True)
                 for v in mr.values():
                     # the factors stream once per call: the HBM floor is their bytes
@@ -744,6 +753,7 @@ def run_ours(a):
             "config": dict(workload(a.n), storage=a.storage, parallelism=("%d row shards, NCCL all-gather of y" % world) if shard
                         else ("replicas" if world > 1 else "1 GPU")),
             "clocks": ck,
+            "autotune": {"choice": tune_choice, "single_column_ms": tune_table},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * a.n, "d2h_bytes_per_step": 8 * a.n,
                     "ms_per_step": e2e_ms},
             "gpu_launches": 3 * a.steps,

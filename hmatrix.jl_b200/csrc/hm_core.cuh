@@ -77,10 +77,12 @@ static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, i
     if (threadIdx.x == 0) *J.rank = (pre == 3) ? 1 : 0;
     return;
   }
+  // zero_fill writes zeros up to zlim only: beyond it the columns are zero
+  const int zlim = J.known_zero ? min(max(J.zero_from, 0), J.kcap) : J.kcap;
   if (r == 0) {
     if (J.zero_fill) {
-      zero_cols(J.outA, J.m, J.ldoa, 0, J.kcap);
-      zero_cols(J.outB, J.n, J.ldob, 0, J.kcap);
+      zero_cols(J.outA, J.m, J.ldoa, 0, zlim);
+      zero_cols(J.outB, J.n, J.ldob, 0, zlim);
     }
     if (threadIdx.x == 0) *J.rank = 0;
     return;
@@ -124,7 +126,7 @@ static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, i
   bool nonfinite = !isfinite(sabs);
   if (J.zero_test && sabs < 1e-5) {
     // compress(): an (absolutely) tiny core becomes rank-1 zeros (src/hlu.jl:163-167)
-    const int kz = J.zero_fill ? J.kcap : 1;
+    const int kz = J.zero_fill ? max(zlim, 1) : 1;
     zero_cols(J.outA, J.m, J.ldoa, 0, kz);
     zero_cols(J.outB, J.n, J.ldob, 0, kz);
     if (threadIdx.x == 0) *J.rank = 1;
@@ -133,8 +135,11 @@ static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, i
   // V = I
   for (int e = threadIdx.x; e < r * r; e += blockDim.x) b0[e] = (e % r == e / r) ? 1.0 : 0.0;
   __syncthreads();
-  // one-sided Jacobi on the columns of W, round-robin pairing
+  // one-sided Jacobi on the columns of W, round-robin pairing.  A pair is
+  // rotated while its cosine exceeds thr; the truncation only needs the
+  // singular values far below eps_trunc, so thr follows it (at least 1e-15)
   const int rr = (r + 1) & ~1;
+  const double thr = fmax(1e-15, 1e-3 * eps_trunc);
   for (int sweep = 0; sweep < 60; ++sweep) {
     if (threadIdx.x == 0) s_rot = 0;
     __syncthreads();
@@ -154,7 +159,7 @@ static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, i
           ga = fma(wp[t], wq[t], ga);
         }
         al = warp_sum(al); be = warp_sum(be); ga = warp_sum(ga);
-        if (ga != 0.0 && fabs(ga) > 1e-15 * sqrt(al * be)) {
+        if (ga != 0.0 && fabs(ga) > thr * sqrt(al * be)) {
           const double zeta = (be - al) / (2.0 * ga);
           const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
           const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
@@ -234,9 +239,9 @@ static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, i
     for (int j = 0; j < r; ++j) s = fma(J.B[i + (int64_t)j * J.ldb], b2[j + c * r], s);
     J.outB[i + (int64_t)c * J.ldob] = s;
   }
-  if (J.zero_fill && k < J.kcap) {
-    zero_cols(J.outA, J.m, J.ldoa, k, J.kcap);
-    zero_cols(J.outB, J.n, J.ldob, k, J.kcap);
+  if (J.zero_fill && k < zlim) {
+    zero_cols(J.outA, J.m, J.ldoa, k, zlim);
+    zero_cols(J.outB, J.n, J.ldob, k, zlim);
   }
   if (threadIdx.x == 0) *J.rank = k;
 }

@@ -89,6 +89,8 @@ struct CoreJob {
   const int32_t* r_dev;    // if set: the core size r is read on the device
   const int32_t* pre_status;  // if set: status of the fully pivoted ACA that made A, B
   int32_t zero_fill;       // zero the output columns [k, kcap)
+  int32_t known_zero;      // the output's columns [zero_from, kcap) are zero already:
+  int32_t zero_from;       // zero_fill stops there (writes only what changes)
   int32_t ortho_k;         // the first ortho_k columns of A are orthonormal and those of B
                            // mutually orthogonal (a previous core's output): no QR for them
 };

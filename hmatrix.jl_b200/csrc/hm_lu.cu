@@ -1529,6 +1529,9 @@ __global__ void __launch_bounds__(128) lu_tile_core_kernel(TileJobArgs a, int rl
   J.m = mi; J.n = nj; J.r = r; J.lda = max(mi, 1); J.ldb = max(nj, 1);
   J.ldoa = mi; J.ldob = nj; J.kcap = a.cap;
   J.zero_test = 1; J.rank = kij; J.zero_fill = 1;
+  // the tile's columns at and beyond its previous rank k1 are zero: only the
+  // columns [k, k1) a smaller new rank frees need zeros
+  J.known_zero = 1; J.zero_from = k1;
   // from step 1 on, every trailing tile (and tile (k, j)) is a previous step's
   // core output: A_ij orthonormal, B_ij and B_kj with orthogonal columns
   J.ortho_k = a.k >= 1 ? k1 : 0;
