@@ -14,35 +14,36 @@ namespace hm {
 // ===========================================================================
 // Columns [0, j0) are already orthonormal and their block of Rm is set by the
 // caller (cgs2_qr zeroes the rest of Rm first).
-static __device__ void cgs2_qr(double* X, int len, int ld, int r, double* Rm /* r x r, col-major */,
-                        double* proj /* r */, double* red, int j0 = 0) {
+template <typename TS>
+static __device__ void cgs2_qr(TS* X, int len, int ld, int r, TS* Rm /* r x r, col-major */,
+                        TS* proj /* r */, double* red, int j0 = 0) {
   for (int e = threadIdx.x; e < r * r; e += blockDim.x)
     if (!(e % r < j0 && e / r < j0)) Rm[e] = 0.0;
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int j = j0; j < r; ++j) {
-    double* xj = X + (int64_t)j * ld;
+    TS* xj = X + (int64_t)j * ld;
     for (int pass = 0; pass < 2; ++pass) {
       for (int i = w; i < j; i += nw) {
-        const double* qi = X + (int64_t)i * ld;
-        double s = 0.0;
+        const TS* qi = X + (int64_t)i * ld;
+        TS s = 0;
         for (int t = lane; t < len; t += 32) s = fma(qi[t], xj[t], s);
         s = warp_sum(s);
         if (lane == 0) proj[i] = s;
       }
       __syncthreads();
       for (int t = threadIdx.x; t < len; t += blockDim.x) {
-        double s = 0.0;
+        TS s = 0;
         for (int i = 0; i < j; ++i) s = fma(X[t + (int64_t)i * ld], proj[i], s);
         xj[t] -= s;
       }
       if (threadIdx.x < j) Rm[threadIdx.x + j * r] += proj[threadIdx.x];
       __syncthreads();
     }
-    double ss = 0.0;
+    TS ss = 0;
     for (int t = threadIdx.x; t < len; t += blockDim.x) ss = fma(xj[t], xj[t], ss);
-    const double nrm = sqrt(block_sum(ss, red));
-    const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+    const TS nrm = sqrt((TS)block_sum((double)ss, red));
+    const TS inv = nrm > (TS)0 ? (TS)1 / nrm : (TS)0;
     for (int t = threadIdx.x; t < len; t += blockDim.x) xj[t] *= inv;
     if (threadIdx.x == 0) Rm[j + j * r] = nrm;
     __syncthreads();
@@ -54,18 +55,25 @@ static __device__ void zero_cols(double* X, int len, int64_t ld, int c0, int c1)
     X[(e % len) + (int64_t)(c0 + e / len) * ld] = 0.0;
 }
 
-static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, int* __restrict__ flags) {
-  extern __shared__ double sm[];
+// TS: the working precision (double; float for a loose truncation, where
+// FP32 Gram-Schmidt and Jacobi keep far more accuracy than the truncation
+// discards).  A, B: the tall factors (in TS), J's other fields as for
+// core_body; the new factors are written in FP64.
+template <typename TS>
+static __device__ void core_body_t(const CoreJob& J, TS* __restrict__ JA, TS* __restrict__ JB, int rmax,
+                                   double eps_trunc, int* __restrict__ flags) {
+  extern __shared__ double sm_raw[];
+  TS* sm = reinterpret_cast<TS*>(sm_raw);
   __shared__ double red[32];
-  __shared__ double proj[RCORE_MAX];
-  __shared__ double sig[RCORE_MAX];
+  __shared__ TS proj[RCORE_MAX];
+  __shared__ TS sig[RCORE_MAX];
   __shared__ int ord[RCORE_MAX];
   __shared__ int s_rot;
   __shared__ int s_k;
   int r = J.r_dev ? *J.r_dev : J.r;
-  double* b0 = sm;                       // R_A, later V (Jacobi right vectors)
-  double* b1 = sm + rmax * rmax;         // R_B, later U-coefficients
-  double* b2 = sm + 2 * rmax * rmax;     // W, later V-coefficients
+  TS* b0 = sm;                           // R_A, later V (Jacobi right vectors)
+  TS* b1 = sm + rmax * rmax;             // R_B, later U-coefficients
+  TS* b2 = sm + 2 * rmax * rmax;         // W, later V-coefficients
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int pre = J.pre_status ? *J.pre_status : 0;
   if (pre != 0 || r > rmax) {
@@ -97,30 +105,30 @@ static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, i
       b1[i + j * r] = 0.0;
     }
     for (int j = w; j < ok; j += nw) {
-      double s = 0.0;
-      for (int t = lane; t < J.n; t += 32) s = fma(J.B[t + (int64_t)j * J.ldb], J.B[t + (int64_t)j * J.ldb], s);
+      TS s = 0;
+      for (int t = lane; t < J.n; t += 32) s = fma(JB[t + (int64_t)j * J.ldb], JB[t + (int64_t)j * J.ldb], s);
       s = warp_sum(s);
       if (lane == 0) proj[j] = sqrt(s);
     }
     __syncthreads();
     for (int e = threadIdx.x; e < J.n * ok; e += blockDim.x) {
       const int t = e % J.n, j = e / J.n;
-      const double nj = proj[j];
-      J.B[t + (int64_t)j * J.ldb] = nj > 0.0 ? J.B[t + (int64_t)j * J.ldb] / nj : 0.0;
+      const TS nj = proj[j];
+      JB[t + (int64_t)j * J.ldb] = nj > (TS)0 ? JB[t + (int64_t)j * J.ldb] / nj : (TS)0;
     }
     if (threadIdx.x < ok) b1[threadIdx.x + threadIdx.x * r] = proj[threadIdx.x];
     __syncthreads();
   }
-  cgs2_qr(J.A, J.m, J.lda, r, b0, proj, red, ok);
-  cgs2_qr(J.B, J.n, J.ldb, r, b1, proj, red, ok);
+  cgs2_qr(JA, J.m, J.lda, r, b0, proj, red, ok);
+  cgs2_qr(JB, J.n, J.ldb, r, b1, proj, red, ok);
   // W = R_A R_B^T  (r x r, column-major, ld r)
   double sabs = 0.0;
   for (int e = threadIdx.x; e < r * r; e += blockDim.x) {
     const int i = e % r, j = e / r;
-    double s = 0.0;
+    TS s = 0;
     for (int q = max(i, j); q < r; ++q) s = fma(b0[i + q * r], b1[j + q * r], s);
     b2[e] = s;
-    sabs += fabs(s);
+    sabs += fabs((double)s);
   }
   sabs = block_sum(sabs, red);
   bool nonfinite = !isfinite(sabs);
@@ -133,13 +141,13 @@ static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, i
     return;
   }
   // V = I
-  for (int e = threadIdx.x; e < r * r; e += blockDim.x) b0[e] = (e % r == e / r) ? 1.0 : 0.0;
+  for (int e = threadIdx.x; e < r * r; e += blockDim.x) b0[e] = (e % r == e / r) ? (TS)1 : (TS)0;
   __syncthreads();
   // one-sided Jacobi on the columns of W, round-robin pairing.  A pair is
   // rotated while its cosine exceeds thr; the truncation only needs the
   // singular values far below eps_trunc, so thr follows it (at least 1e-15)
   const int rr = (r + 1) & ~1;
-  const double thr = fmax(1e-15, 1e-3 * eps_trunc);
+  const TS thr = (TS)fmax(sizeof(TS) == 8 ? 1e-15 : 1e-7, 1e-3 * eps_trunc);
   for (int sweep = 0; sweep < 60; ++sweep) {
     if (threadIdx.x == 0) s_rot = 0;
     __syncthreads();
@@ -150,26 +158,26 @@ static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, i
         int p = posv(pidx), q = posv(rr - 1 - pidx);
         if (p > q) { int t = p; p = q; q = t; }
         if (q >= r) continue;
-        double* wp = b2 + p * r;
-        double* wq = b2 + q * r;
-        double al = 0.0, be = 0.0, ga = 0.0;
+        TS* wp = b2 + p * r;
+        TS* wq = b2 + q * r;
+        TS al = 0, be = 0, ga = 0;
         for (int t = lane; t < r; t += 32) {
           al = fma(wp[t], wp[t], al);
           be = fma(wq[t], wq[t], be);
           ga = fma(wp[t], wq[t], ga);
         }
         al = warp_sum(al); be = warp_sum(be); ga = warp_sum(ga);
-        if (ga != 0.0 && fabs(ga) > thr * sqrt(al * be)) {
-          const double zeta = (be - al) / (2.0 * ga);
-          const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-          const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
-          double* vp = b0 + p * r;
-          double* vq = b0 + q * r;
+        if (ga != (TS)0 && fabs(ga) > thr * sqrt(al * be)) {
+          const TS zeta = (be - al) / ((TS)2 * ga);
+          const TS t = (zeta >= (TS)0 ? (TS)1 : (TS)-1) / (fabs(zeta) + sqrt((TS)1 + zeta * zeta));
+          const TS c = (TS)1 / sqrt((TS)1 + t * t), s = c * t;
+          TS* vp = b0 + p * r;
+          TS* vq = b0 + q * r;
           for (int t2 = lane; t2 < r; t2 += 32) {
-            const double x = wp[t2], y = wq[t2];
+            const TS x = wp[t2], y = wq[t2];
             wp[t2] = c * x - s * y;
             wq[t2] = s * x + c * y;
-            const double u = vp[t2], v = vq[t2];
+            const TS u = vp[t2], v = vq[t2];
             vp[t2] = c * u - s * v;
             vq[t2] = s * u + c * v;
           }
@@ -183,7 +191,7 @@ static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, i
   }
   // singular values = column norms of W; sort descending
   for (int j = w; j < r; j += nw) {
-    double s = 0.0;
+    TS s = 0;
     for (int t = lane; t < r; t += 32) s = fma(b2[t + j * r], b2[t + j * r], s);
     s = warp_sum(s);
     if (lane == 0) sig[j] = sqrt(s);
@@ -202,7 +210,7 @@ static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, i
     const double s1 = sig[ord[0]];
     int k = 0;
     for (int j = 0; j < r; ++j)
-      if (sig[ord[j]] / s1 > eps_trunc) k = j + 1;   // findlast(S/S[1] .> εTrunc)
+      if ((double)sig[ord[j]] / s1 > eps_trunc) k = j + 1;   // findlast(S/S[1] .> εTrunc)
     if (!(s1 > 0.0)) k = 0;
     s_k = k;
   }
@@ -217,8 +225,8 @@ static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, i
   for (int e = threadIdx.x; e < r * k; e += blockDim.x) {
     const int j = e % r, c = e / r;
     const int o = ord[c];
-    const double s = sig[o];
-    b1[e] = s > 0.0 ? b2[j + o * r] / s : 0.0;
+    const TS s = sig[o];
+    b1[e] = s > (TS)0 ? b2[j + o * r] / s : (TS)0;
   }
   __syncthreads();
   for (int e = threadIdx.x; e < r * k; e += blockDim.x) {
@@ -229,21 +237,25 @@ static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, i
   __syncthreads();
   for (int64_t e = threadIdx.x; e < (int64_t)J.m * k; e += blockDim.x) {
     const int i = (int)(e % J.m), c = (int)(e / J.m);
-    double s = 0.0;
-    for (int j = 0; j < r; ++j) s = fma(J.A[i + (int64_t)j * J.lda], b1[j + c * r], s);
-    J.outA[i + (int64_t)c * J.ldoa] = s;
+    TS s = 0;
+    for (int j = 0; j < r; ++j) s = fma(JA[i + (int64_t)j * J.lda], b1[j + c * r], s);
+    J.outA[i + (int64_t)c * J.ldoa] = (double)s;
   }
   for (int64_t e = threadIdx.x; e < (int64_t)J.n * k; e += blockDim.x) {
     const int i = (int)(e % J.n), c = (int)(e / J.n);
-    double s = 0.0;
-    for (int j = 0; j < r; ++j) s = fma(J.B[i + (int64_t)j * J.ldb], b2[j + c * r], s);
-    J.outB[i + (int64_t)c * J.ldob] = s;
+    TS s = 0;
+    for (int j = 0; j < r; ++j) s = fma(JB[i + (int64_t)j * J.ldb], b2[j + c * r], s);
+    J.outB[i + (int64_t)c * J.ldob] = (double)s;
   }
   if (J.zero_fill && k < zlim) {
     zero_cols(J.outA, J.m, J.ldoa, k, zlim);
     zero_cols(J.outB, J.n, J.ldob, k, zlim);
   }
   if (threadIdx.x == 0) *J.rank = k;
+}
+
+static __device__ void core_body(const CoreJob& J, int rmax, double eps_trunc, int* __restrict__ flags) {
+  core_body_t<double>(J, J.A, J.B, rmax, eps_trunc, flags);
 }
 
 

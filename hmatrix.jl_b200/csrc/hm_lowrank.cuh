@@ -24,6 +24,11 @@ __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
 
 // arg-max of |v| with the smallest index on ties; returns the winner in all lanes
 __device__ __forceinline__ void warp_argmax(double& a, int64_t& idx, double& val) {

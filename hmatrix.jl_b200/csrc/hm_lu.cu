@@ -1302,6 +1302,9 @@ static int64_t tile_pair_count(int T, int k, int mode) {
   return Tr >= 2 ? (Tr - 1) * (Tr - 2) : 0;
 }
 
+// truncation tolerance from which the tile recompressions run in FP32
+constexpr double MIXED_CORE_EPS = 1e-6;
+
 struct TileJobArgs {
   const double* const* Ap;
   const double* const* Bp;
@@ -1496,8 +1499,12 @@ static bool tile_structure(const hm_handle* h, std::vector<int32_t>& gcl, std::v
 // The same update with the gather fused into the recompression: the CTA
 // loads [A_ij | -Q_ij] and [B_ij | B_kj] into shared memory (rl columns at
 // most, smax rows) and runs the QR + SVD core there.
+// TS: the precision of the staged factors and of the QR + SVD core (FP32 when
+// the truncation tolerance is loose: the mixed-precision factorisation)
+template <typename TS>
 __global__ void __launch_bounds__(128) lu_tile_core_kernel(TileJobArgs a, int rl, int smax, double eps_trunc) {
-  extern __shared__ double sm[];
+  extern __shared__ double sm_raw[];
+  TS* sm = reinterpret_cast<TS*>(sm_raw);
   const int64_t gq = a.q0 + blockIdx.x;
   int i, j;
   tile_pair(a.T, a.k, a.mode, gq, i, j);
@@ -1513,19 +1520,19 @@ __global__ void __launch_bounds__(128) lu_tile_core_kernel(TileJobArgs a, int rl
     if (threadIdx.x == 0) atomicOr(a.flags, 1);
     r = rl;
   }
-  double* XA = sm + 3 * rl * rl;
-  double* XB = XA + (int64_t)smax * rl;
+  TS* XA = sm + 3 * rl * rl;
+  TS* XB = XA + (int64_t)smax * rl;
   for (int e = threadIdx.x; e < mi * r; e += blockDim.x) {
     const int t = e % mi, q = e / mi;
-    XA[e] = q < k1 ? Aij[t + (int64_t)q * mi] : -Qij[t + (int64_t)(q - k1) * mi];
+    XA[e] = (TS)(q < k1 ? Aij[t + (int64_t)q * mi] : -Qij[t + (int64_t)(q - k1) * mi]);
   }
   for (int e = threadIdx.x; e < nj * r; e += blockDim.x) {
     const int t = e % nj, q = e / nj;
-    XB[e] = q < k1 ? Bij[t + (int64_t)q * nj] : Bkj[t + (int64_t)(q - k1) * nj];
+    XB[e] = (TS)(q < k1 ? Bij[t + (int64_t)q * nj] : Bkj[t + (int64_t)(q - k1) * nj]);
   }
   __syncthreads();
   CoreJob J{};
-  J.A = XA; J.B = XB; J.outA = Aij; J.outB = Bij;
+  J.outA = Aij; J.outB = Bij;
   J.m = mi; J.n = nj; J.r = r; J.lda = max(mi, 1); J.ldb = max(nj, 1);
   J.ldoa = mi; J.ldob = nj; J.kcap = a.cap;
   J.zero_test = 1; J.rank = kij; J.zero_fill = 1;
@@ -1535,7 +1542,7 @@ __global__ void __launch_bounds__(128) lu_tile_core_kernel(TileJobArgs a, int rl
   // from step 1 on, every trailing tile (and tile (k, j)) is a previous step's
   // core output: A_ij orthonormal, B_ij and B_kj with orthogonal columns
   J.ortho_k = a.k >= 1 ? k1 : 0;
-  core_body(J, rl, eps_trunc, a.flags);
+  core_body_t<TS>(J, XA, XB, rl, eps_trunc, a.flags);
 }
 
 // an upper bound of rank(A_ij) + rank(B_kj) over the trailing pairs of step k
@@ -1591,16 +1598,19 @@ static void recompress_tile_pairs(Ctx& c, const TileLU& TL, int k, int64_t R, co
   Blk tmp;
   tmp.st = c.st;
   {
-    // fused path: the pairs' factors staged in shared memory
-    const size_t smem = sizeof(double) * ((size_t)3 * rl * rl + (size_t)2 * smax * rl);
+    // fused path: the pairs' factors staged in shared memory, in FP32 when the
+    // truncation tolerance is loose (>= 1e-6, the mixed-precision scheme)
+    const bool f32 = c.eps_trunc >= MIXED_CORE_EPS;
+    const size_t smem = (f32 ? sizeof(float) : sizeof(double)) * ((size_t)3 * rl * rl + (size_t)2 * smax * rl);
     if (smem <= 200 * 1024) {
-      if (smem_attr((const void*)lu_tile_core_kernel, 200 * 1024) != cudaSuccess)
-        throw LuError(HM_ERR_CUDA, "tile core smem");
+      const void* kfn = f32 ? (const void*)lu_tile_core_kernel<float> : (const void*)lu_tile_core_kernel<double>;
+      if (smem_attr(kfn, 200 * 1024) != cudaSuccess) throw LuError(HM_ERR_CUDA, "tile core smem");
       for (int64_t q0 = 0; q0 < njobs; q0 += INT32_MAX) {
         const int64_t nb = std::min<int64_t>(INT32_MAX, njobs - q0);
         TileJobArgs a{TL.d_Ap, TL.d_Bp, TL.d_start, TL.d_size, TL.kmat, T, c.cap, k, rmax, R, qbase, nullptr, 0,
                       nullptr, c.flags, nullptr, q0, mode};
-        lu_tile_core_kernel<<<(unsigned)nb, 128, smem, c.st>>>(a, rl, (int)smax, c.eps_trunc);
+        if (f32) lu_tile_core_kernel<float><<<(unsigned)nb, 128, smem, c.st>>>(a, rl, (int)smax, c.eps_trunc);
+        else lu_tile_core_kernel<double><<<(unsigned)nb, 128, smem, c.st>>>(a, rl, (int)smax, c.eps_trunc);
         LU_LAUNCH_CHECK();
       }
       return;
