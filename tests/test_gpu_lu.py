@@ -219,3 +219,26 @@ def test_captured_solve_replays(mode):
             assert np.array_equal(L.solve(ys[0], trans=trans), xs[0])   # replay == first run
     Xr, it, rr = L.solve_refined(rng.standard_normal((n, 2)), tol=1e-13, max_iter=5)
     assert rr <= 1e-13
+
+
+@pytest.mark.parametrize("eps_lu", [1e-6, 1e-3])
+def test_mixed_fp32_core_refined(eps_lu):
+    # the tile schedule's recompressions run in FP32 from a truncation of 1e-6
+    # on; refined with the compensated FP64 residual the solve reaches the
+    # FP64 path's accuracy, forward and transposed
+    import hmatrix as hm
+    n = 8192
+    base = dict(Geom=np.linspace(0, 10, n), Kernel=hm.Cauchy(1.0), MaxBlock=256, MinBlock=32, MaxRank=12,
+                ConsMethod="aca2", εComp=1e-10, Tree="bisect", Shift=1.0)
+    _, H = hm.NewHmat(hm.Params(**base))
+    L64 = hm.lu(H)
+    _, Hm = hm.NewHmat(hm.Params(εTruncLU=eps_lu, **base))
+    Lm = hm.lu(Hm)
+    assert Lm.info().lu_tiles > 0
+    y = np.random.default_rng(51).standard_normal(n)
+    x64, _, r64 = L64.solve_refined(y, tol=1e-12, max_iter=10)
+    for trans in (False, True):
+        x, it, rr = Lm.solve_refined(y, tol=1e-12, max_iter=40, trans=trans)
+        assert rr <= 1e-12, (trans, it, rr)
+        if not trans:
+            assert np.linalg.norm(x - x64) <= 1e-10 * np.linalg.norm(x64)
