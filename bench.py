@@ -54,6 +54,10 @@ def parse():
     ap.add_argument("--no-kmeans", action="store_true", help="skip the matvec on the reference's KMeans tree")
     ap.add_argument("--no-c4", action="store_true", help="skip the gradient (adjoint) leg")
     ap.add_argument("--c4-n", type=int, default=1 << 17, help="size of the gradient leg")
+    ap.add_argument("--c5", action="store_true",
+                    help="also run the 2-D point-cloud leg (mixed H-LU, GMRES-based refinement, adjoint solve)")
+    ap.add_argument("--c5-n", type=int, default=1 << 18, help="size of the 2-D leg")
+    ap.add_argument("--c5-eps-lu", type=float, default=1e-6, help="LU truncation of the 2-D leg")
     ap.add_argument("--cpu-rows", type=int, default=4096, help="rows of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-lu", action="store_true", help="skip the H-LU + solve leg")
@@ -630,6 +634,53 @@ def gradient_leg(n, torch):
             "target": 1e-6}
 
 
+def c5_leg(n, eps_lu, torch):
+    """The 2-D point cloud: n points i.i.d. uniform in [0,1]^2 (seed 5), coordinate
+    bisection, 1/(1+|x-y|^2) + 1e-3 I, MaxBlock 512, MinBlock 64, MaxRank 32, ACA
+    tolerance 1e-9, 8 N(0,1) right-hand sides.  Mixed-precision H-LU (truncation
+    eps_lu: FP32 recompression cores from 1e-6 on), then GMRES-based refinement
+    (compensated FP64 residual, GMRES preconditioned by the H-LU) to a relative
+    residual <= 1e-10, then the adjoint (transposed) solve the same way.  The
+    errors against the dense FP64 oracle are measured on 1024 sampled rows of
+    K + 1e-3 I (exact kernel rows)."""
+    import hmatrix as hm
+    rng = np.random.default_rng(5)
+    G = rng.uniform(0, 1, (n, 2))
+    prm = hm.Params(Geom=G, Kernel=hm.Cauchy(1.0), MaxBlock=512, MinBlock=64, MaxRank=32, ConsMethod="aca2",
+                    εComp=1e-9, Tree="bisect", Shift=1e-3, εTruncLU=eps_lu, Device=torch.cuda.current_device())
+    t0 = time.perf_counter()
+    c, H = hm.NewHmat(prm)
+    t_build = time.perf_counter() - t0
+    info = H.info()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L = hm.lu(H)
+    t_lu = time.perf_counter() - t0
+    B = rng.standard_normal((n, 8))
+    rows = np.sort(np.random.default_rng(7).choice(n, 1024, replace=False))
+    out = {"config": {"n": n, "kernel": "1/(1+|x-y|^2) + 1e-3 I", "MaxBlock": 512, "MinBlock": 64, "MaxRank": 32,
+                      "aca_tol": 1e-9, "eps_trunc_lu": eps_lu, "rhs": 8, "tree": "coordinate bisection",
+                      "refinement": "GMRES-IR (compensated residual, GMRES(30) preconditioned by the H-LU)"},
+           "build_s": t_build, "lu_s": t_lu, "n_rk": info.n_rk, "max_rank": info.max_rank,
+           "lu_tiles": L.info().lu_tiles, "fp32_core": eps_lu >= 1e-6}
+    for name, trans in (("solve", False), ("adjoint_solve", True)):
+        t0 = time.perf_counter()
+        worst, steps, dense_err = 0.0, 0, 0.0
+        for j in range(B.shape[1]):
+            x, it, rr = hm.gmres_ir(H, L, B[:, j], tol=1e-10, trans=trans)
+            worst = max(worst, rr)
+            steps = max(steps, it)
+            if not trans:
+                ex = H.exact_rows(rows, x)            # rows of (K + 1e-3 I) x, FP64 dense oracle
+                dense_err = max(dense_err, float(np.linalg.norm(ex - B[rows, j]) / np.linalg.norm(B[rows, j])))
+        out[name] = {"s": time.perf_counter() - t0, "max_relres": worst, "max_outer_steps": steps}
+        if not trans:
+            out[name]["rel_residual_vs_dense_rows"] = dense_err
+    del L, H
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(a):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -728,6 +779,11 @@ def run_ours(a):
         H = None
         torch.cuda.empty_cache()
         batch = batch_leg(a.batch, torch, a.batch_nthreads, rank=rank, world=world, dist=dist)
+    c5 = None
+    if a.c5 and world == 1:
+        H = None
+        torch.cuda.empty_cache()
+        c5 = c5_leg(a.c5_n, a.c5_eps_lu, torch)
     c4 = None
     if not a.no_c4 and world == 1:
         H = None
@@ -771,6 +827,7 @@ def run_ours(a):
             "reduced_precision": extra or None,
             "kmeans_tree": kmeans,
             "gradients": c4,
+            "point_cloud_2d": c5,
             "lu_solve": lu,
             "batched_lu_solve": batch}
     print(json.dumps(line))
