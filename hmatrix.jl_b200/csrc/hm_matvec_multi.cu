@@ -1,9 +1,10 @@
-// Multi-RHS H-matvec (K5): Y = H X and Y = H' X for an n x c block of
-// right-hand sides, the device form of *(Hmat, Matrix) (src/harithm.jl:
-// 323-329), which the reference evaluates one column at a time.  Here every
-// factor is streamed from HBM once per block of CB columns instead of once per
-// column; the arithmetic is FP64 on the CUDA cores (the leaf ranks are too
-// small -- k of 2 to 16 -- for a tensor-core tile to fill).
+// Multi-RHS H-matvec (K5) on the CUDA cores: Y = H X and Y = H' X for an
+// n x c block of right-hand sides, the device form of *(Hmat, Matrix)
+// (src/harithm.jl:323-329), which the reference evaluates one column at a
+// time.  Every factor is streamed from HBM once per block of CB columns
+// instead of once per column, in FP64 arithmetic.  This is the path of FP64
+// factors (tcgen05 has no FP64 kind) and of the dense leaves of FP32/BF16
+// handles, whose low-rank part runs on the tensor cores (hm_matvec_tc.cu).
 //
 // Layout: the input is first transposed into XR, n+2 rows of LD = c rounded up
 // to CB doubles (row i holds x[i, 0..c), zero padded), so that a leaf row's CB
