@@ -389,6 +389,37 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase1_kernel(P1Args<T, NC> 
 // ---------------------------------------------------------------------------
 // phase 2
 // ---------------------------------------------------------------------------
+// Phase-2 A tiles are M-major (a factor column's rows are contiguous).  The
+// 16-byte chunk ci of a 128-row tile holds rows KE g .. KE g + KE - 1 of its K
+// column k; a2_chunk gives (g, k) and the chunk's byte offset in the tile.
+//  BF16 (KE 8): no swizzle, core matrices of 8 K x 16 bytes: (k / 8) 2048 +
+//    g 128 + (k % 8) 16; descriptor LBO = 2048 (along K), SBO = 128 (along M).
+//  TF32 (KE 4): M-major TF32 operands take the 128-byte swizzle with 32-byte
+//    atoms (descriptor layout 1): atoms of 32 rows (128 bytes) x 4 K rows
+//    whose 32-byte pieces are permuted by XOR with k % 4; the 4 row atoms
+//    512 bytes apart (LBO), groups of 4 K 2048 bytes apart (SBO).  Eight
+//    consecutive chunks fill one 128-byte atom row (no bank conflicts) and
+//    read 128 contiguous bytes of one factor column.
+template <int KE>
+__device__ __forceinline__ uint32_t a2_chunk(int ci, int& g, int& k) {
+  if constexpr (KE == 8) {
+    k = 8 * (ci / 128) + (ci % 8);
+    g = (ci / 8) % 16;
+    return (uint32_t)ci * 16u;
+  } else {
+    const int g8 = ci % 8;
+    k = (ci / 8) % 16;
+    g = (ci / 128) * 8 + g8;
+    return (uint32_t)((g / 8) * 512 + (k / 4) * 2048 + (k % 4) * 128 + ((((g % 8) >> 1) ^ (k % 4)) << 5) +
+                      (g & 1) * 16);
+  }
+}
+// descriptor of K step ks (32 bytes of K) of the phase-2 A tile at `tile`
+template <int KE>
+__device__ __forceinline__ uint64_t a2_desc(uint32_t tile, int ks) {
+  if constexpr (KE == 8) return tc::smem_desc(tile + ks * 2 * 2048, 2048, 128, 0);
+  else return tc::smem_desc(tile + ks * 2 * 2048, 512, 2048, 1);
+}
 template <typename T, int NC>
 struct P2Args {
   const TcItem2* items;
@@ -408,9 +439,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
   using S = TcSmem<T, NC>;
   constexpr int KE = Tr::KE;
   constexpr int KC = TC_KB * KE;                    // K values (Z slots) per stage
-  constexpr int MG = 128 / KE;                      // 16-byte row groups of a tile
-  constexpr uint32_t LBO_A = MG * 128;              // M-major A: K groups of 8
-  constexpr uint32_t SBO_A = 128;
   extern __shared__ __align__(1024) uint8_t smem[];
   TcBars* bars = reinterpret_cast<TcBars*>(smem + S::BAR_OFF);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -454,19 +482,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
           tc::mbar_arrive_expect_tx(&bars->full[s], S::B_STAGE);
           tc::bulk_g2s(abase + S::A_STAGE + S::A_LO, a.zt + (zc / KE) * (2 * NC * KE), S::B_STAGE, &bars->full[s]);
         }
-        // chunk ci = tid + 128 j: tile j / 4; k = 8 kg + ci % 8, row group
-        // g = (ci / 8) % MG, kg = (ci % 512) / (8 MG)
+        // chunk ci = tid + 128 (j % 4) of tile j / 4: rows KE g.. of K column k
         int64_t zcur = -1;
         TcZ2 Z{};
 #pragma unroll
         for (int j = 0; j < TC_T * 4; ++j) {
           const int t = j / 4;
           const int ci = tid + TC_PROD * (j % 4);
-          const int k = 8 * (ci / (8 * MG)) + (ci % 8);
-          const int g = (ci / 8) % MG;
+          int g, k;
+          const uint32_t coff = a2_chunk<KE>(ci, g, k);
           const int64_t zp = zc + k;
-          uint8_t* dsm = smem + s * S::STAGE + t * S::A_TILE + ci * 16;
-          const uint32_t dst = abase + (uint32_t)(t * S::A_TILE + ci * 16);
+          uint8_t* dsm = smem + s * S::STAGE + t * S::A_TILE + coff;
+          const uint32_t dst = abase + (uint32_t)(t * S::A_TILE) + coff;
           if (zp < (int64_t)I.zb || zp >= (int64_t)I.ze) {
             *reinterpret_cast<uint4*>(dsm) = make_uint4(0u, 0u, 0u, 0u);
             continue;
@@ -504,7 +531,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
   } else if (warp == 8) {
     if (lane == 0) {
       constexpr uint32_t LBO_B = 2 * NC * 16, SBO_B = 128;
-      constexpr uint32_t KSTEP_A = (KE == 4) ? LBO_A : 2 * LBO_A;   // 32 bytes of K per MMA
       const uint32_t id_full = tc::idesc(Tr::FMT, 2 * NC, 1, 0);
       const uint32_t id_half = tc::idesc(Tr::FMT, NC, 1, 0);
       uint32_t it = 0, item = 0;
@@ -527,10 +553,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
 #pragma unroll
             for (int ks = 0; ks < TC_KB / 2; ++ks) {
               const uint64_t bd = tc::smem_desc(bbase + ks * 2 * LBO_B, LBO_B, SBO_B);
-              const uint64_t ad = tc::smem_desc(abase + t * S::A_TILE + ks * KSTEP_A, LBO_A, SBO_A);
+              const uint64_t ad = a2_desc<KE>(abase + t * S::A_TILE, ks);
               tc::mma<Tr::KIND>(tmem + t * 2 * NC, ad, bd, id_full, (kc > 0 || ks > 0) ? 1u : 0u);
               if constexpr (Tr::SPLIT) {
-                const uint64_t al = tc::smem_desc(abase + S::A_STAGE + t * S::A_TILE + ks * KSTEP_A, LBO_A, SBO_A);
+                const uint64_t al = a2_desc<KE>(abase + S::A_STAGE + t * S::A_TILE, ks);
                 tc::mma<Tr::KIND>(tmem + t * 2 * NC, al, bd, id_half, 1u);
               }
             }
@@ -592,7 +618,6 @@ __global__ void __launch_bounds__(128, 1) tc_selftest_kernel(const float* __rest
   using Tr = TcT<T>;
   constexpr int KE = Tr::KE;
   constexpr int KC = TC_KB * KE;
-  constexpr int MG = 128 / KE;
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t bar;
   __shared__ uint32_t tslot;
@@ -607,8 +632,12 @@ __global__ void __launch_bounds__(128, 1) tc_selftest_kernel(const float* __rest
       // phase 1: row i, K block b: (i / 8) * KB * 128 + b * 128 + (i % 8) * 16 bytes
       off = ((i / 8) * TC_KB * 128 + (k / KE) * 128 + (i % 8) * 16) / (int)sizeof(T) + k % KE;
     } else {
-      // phase 2: chunk (row group g = i / KE, k): (k / 8) * MG * 128 + g * 128 + (k % 8) * 16 bytes
-      off = ((k / 8) * MG * 128 + (i / KE) * 128 + (k % 8) * 16) / (int)sizeof(T) + i % KE;
+      // phase 2: the chunk of rows KE g .. of column k, laid out by a2_chunk
+      int ci = 0;
+      if (KE == 8) ci = (k / 8) * 128 + ((i / KE) % 16) * 8 + (k % 8);
+      else ci = ((i / KE) / 8) * 128 + (k % 16) * 8 + (i / KE) % 8;
+      int gg, kk;
+      off = (int)(a2_chunk<KE>(ci, gg, kk) / sizeof(T)) + i % KE;
     }
     sa[off] = Tr::bits(A[e]);
   }
@@ -636,7 +665,7 @@ __global__ void __launch_bounds__(128, 1) tc_selftest_kernel(const float* __rest
       const uint64_t bd = tc::smem_desc(bbase + ks * 2 * LBO_B, LBO_B, SBO_B);
       uint64_t ad;
       if (!A_MN) ad = tc::smem_desc(abase + ks * 2 * 128, 128, TC_KB * 128);
-      else ad = tc::smem_desc(abase + ks * ((KE == 4) ? MG * 128 : 2 * MG * 128), MG * 128, 128);
+      else ad = a2_desc<KE>(abase, ks);
       tc::mma<Tr::KIND>(tmem, ad, bd, id, ks > 0 ? 1u : 0u);
     }
     tc::mma_commit(&bar);

@@ -86,17 +86,21 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
 }
 
 // ---------------------------------------------------------------------------
-// shared-memory matrix descriptor (tcgen05 form, version 1), no swizzle:
-// 8 x 16-byte core matrices; LBO = byte distance between core matrices
-// adjacent in K, SBO = between core matrices adjacent in M/N.
+// shared-memory matrix descriptor (tcgen05 form, version 1).
+// layout 0, no swizzle: 8 x 16-byte core matrices; LBO = byte distance
+//   between core matrices adjacent in K, SBO = between those adjacent in M/N.
+// layout 1, 128-byte swizzle with 32-byte atoms (the form M-major TF32
+//   operands need): atoms of 128 bytes along M/N x 4 K rows; LBO = distance
+//   between atoms adjacent in M/N, SBO = between groups of 4 K.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo, uint32_t layout = 0) {
   uint64_t d = 0;
   d |= (uint64_t)((addr >> 4) & 0x3FFFu);
   d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
   d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
   d |= (uint64_t)1 << 46;   // version 1 (sm_100)
-  // base offset 0, leading-offset mode 0, layout type 0 (no swizzle)
+  d |= (uint64_t)(layout & 7u) << 61;
+  // base offset 0 (atoms start on their pattern's alignment), leading-offset mode 0
   return d;
 }
 
