@@ -2606,9 +2606,13 @@ int lu_solve_refined(hm_handle* h, const double* d_b, double* d_x, int64_t ncols
     status = norms(Rv, nrm + ncols, hr);
     if (status != HM_OK) break;
     worst = 0.0;
-    for (int64_t q = 0; q < ncols; ++q)
-      worst = std::max(worst, hb[q] > 0 ? std::sqrt(hr[q] / hb[q]) : std::sqrt(hr[q]));
-    if (!(worst == worst)) { status = fail(HM_ERR_NONFINITE, "refinement: non-finite residual"); break; }
+    bool finite = true;
+    for (int64_t q = 0; q < ncols; ++q) {
+      const double v = hb[q] > 0 ? std::sqrt(hr[q] / hb[q]) : std::sqrt(hr[q]);
+      if (!std::isfinite(v) || !std::isfinite(hb[q])) finite = false;   // std::max would drop a NaN
+      worst = std::max(worst, v);
+    }
+    if (!finite) { status = fail(HM_ERR_NONFINITE, "refinement: non-finite residual"); break; }
     if (worst <= tol || it >= max_iter) break;
     status = lu_solve_device(h, r, d, ncols, trans, st);
     if (status != HM_OK) break;
