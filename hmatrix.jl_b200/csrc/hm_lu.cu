@@ -124,18 +124,38 @@ __device__ __forceinline__ void gemm_big_tile(const View& A, const View& B, cons
   for (int u = 0; u < 8; ++u)
 #pragma unroll
     for (int v = 0; v < 8; ++v) acc[u][v] = 0.0;
-  for (int k0 = 0; k0 < K; k0 += GB_K) {
+  // the next K step's tiles are loaded into registers while this one is
+  // multiplied, so the global loads overlap the FMAs
+  double ra[8], rb[8];
+  auto load = [&](int k0) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const int e = tid + 256 * q;
       int i, kk;
       if (A.rs == 1) { i = e & 127; kk = e >> 7; } else { kk = e & 15; i = e >> 4; }
-      As[kk][i] = (i0 + i < m && k0 + kk < K) ? A.p[(int64_t)(i0 + i) * A.rs + (int64_t)(k0 + kk) * A.cs] : 0.0;
+      ra[q] = (i0 + i < m && k0 + kk < K) ? A.p[(int64_t)(i0 + i) * A.rs + (int64_t)(k0 + kk) * A.cs] : 0.0;
       int j;
       if (B.rs == 1) { kk = e & 15; j = e >> 4; } else { j = e & 127; kk = e >> 7; }
-      Bs[kk][j] = (k0 + kk < K && j0 + j < n) ? B.p[(int64_t)(k0 + kk) * B.rs + (int64_t)(j0 + j) * B.cs] : 0.0;
+      rb[q] = (k0 + kk < K && j0 + j < n) ? B.p[(int64_t)(k0 + kk) * B.rs + (int64_t)(j0 + j) * B.cs] : 0.0;
     }
+  };
+  auto stash = [&]() {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + 256 * q;
+      int i, kk;
+      if (A.rs == 1) { i = e & 127; kk = e >> 7; } else { kk = e & 15; i = e >> 4; }
+      As[kk][i] = ra[q];
+      int j;
+      if (B.rs == 1) { kk = e & 15; j = e >> 4; } else { j = e & 127; kk = e >> 7; }
+      Bs[kk][j] = rb[q];
+    }
+  };
+  load(0);
+  for (int k0 = 0; k0 < K; k0 += GB_K) {
+    stash();
     __syncthreads();
+    if (k0 + GB_K < K) load(k0 + GB_K);
 #pragma unroll 4
     for (int kk = 0; kk < GB_K; ++kk) {
       double a[8], b[8];
@@ -560,7 +580,10 @@ static bool is_leaf_cluster(const Ctx& c, int32_t cl) { return cl >= 0 && c.h->c
 
 static void gemm(Ctx& c, View C, View A, View B, double alpha, double beta) {
   if (C.rows == 0 || C.cols == 0) return;
-  if (A.cols > 0 && (double)C.rows * C.cols * A.cols >= 4.0e6) {
+  // 128 x 128 tiles once they fill the GPU; medium products keep the 32 x 32
+  // tiles (more CTAs)
+  const int64_t big_tiles = (int64_t)((C.rows + GB_T - 1) / GB_T) * ((C.cols + GB_T - 1) / GB_T);
+  if (A.cols > 0 && (double)C.rows * C.cols * A.cols >= 4.0e6 && big_tiles >= 148) {
     dim3 g((C.cols + GB_T - 1) / GB_T, (C.rows + GB_T - 1) / GB_T);
     lu_gemm_big_kernel<<<g, 256, 0, c.st>>>(A, B, C, alpha, beta);
     LU_LAUNCH_CHECK();
@@ -1760,7 +1783,10 @@ static void tile_factor(Ctx& c, const hm_handle* h, TileLU& TL, const std::vecto
       gq.push_back(g);
       macs += (double)mi * R * cap;
     }
-    gemm_batch(x, gq, macs >= 4.0e6);
+    // 128 x 128 tiles when the batch fills the GPU with them
+    int64_t big_tiles = 0;
+    for (auto& g : gq) big_tiles += (int64_t)((g.C.rows + GB_T - 1) / GB_T) * ((g.C.cols + GB_T - 1) / GB_T);
+    gemm_batch(x, gq, macs >= 4.0e6 && big_tiles >= 148);
   };
   // updates of the trailing diagonal tiles i in [i0, i1) (H-structured targets)
   auto diag_updates = [&](int k, const StepQ& sq, int i0, int i1) {

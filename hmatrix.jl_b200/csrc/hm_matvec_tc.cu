@@ -451,9 +451,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
     auto finish = [&](uint32_t f) {
       const int s = (int)(f % TC_STAGES);
       if constexpr (Tr::SPLIT) {
+        // exactly the chunks this thread filled (cp.async.wait_group covers
+        // only this thread's own copies)
 #pragma unroll
-        for (int j = 0; j < TC_T * 128 * TC_KB / TC_PROD; ++j) {
-          const uint32_t off = (uint32_t)(tid + TC_PROD * j) * 16;
+        for (int j = 0; j < TC_T * 4; ++j) {
+          int g, k;
+          const uint32_t off = (uint32_t)((j / 4) * S::A_TILE) + a2_chunk<KE>(tid + TC_PROD * (j % 4), g, k);
           float4 v = *reinterpret_cast<const float4*>(smem + s * S::STAGE + off);
           float4 h, l;
           h.x = tc::tf32_rn(v.x); l.x = tc::tf32_rn(v.x - h.x);

@@ -96,7 +96,7 @@ def test_allocation_failure_is_oom_and_library_recovers():
     # MinBlock >= n: the root cluster is one leaf and H one dense block of n^2
     # entries, far beyond the device's memory; the pool allocation fails
     with pytest.raises(hm.HmError) as ei:
-        hm.NewHmat(_prm(hm, np.linspace(0, 10, n), MaxBlock=n, MinBlock=n))
+        hm.NewHmat(_prm(hm, np.linspace(0, 10, n), MaxBlock=512, MinBlock=n))
     assert ei.value.code == _lib.HM_ERR_OOM
     assert "pool" in str(ei.value)
     # a normal construction, matvec and factorisation on the same device next

@@ -97,7 +97,10 @@ def test_aca2_vs_oracle(n, tree):
     assert np.abs(A - H.to_dense()).max() < 1e-7
 
 
-@pytest.mark.parametrize("storage,tol", [("F32", 2e-6), ("BF16", 2e-2)])
+# FP32 factors are multiplied and summed in FP32 over a few terms before the
+# FP64 sum: with random x the row sums cancel (|H x| is about 20 times below
+# |H| |x| here), so the relative error is about 20 x 2^-24 per partial sum
+@pytest.mark.parametrize("storage,tol", [("F32", 1e-5), ("BF16", 2e-2)])
 def test_reduced_storage_matvec(storage, tol):
     import hmatrix as hm
     n = 8192

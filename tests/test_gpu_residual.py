@@ -12,17 +12,25 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _longdouble_residual(H, x, b):
+def _longdouble_residual(H, x, b, trans=False):
+    """b - H x (b - H' x) from the stored leaves, summed in long double."""
     D = H.to_dense()                     # dense leaves are copied as stored
     lv = H.leaves()
     xl = x.astype(np.longdouble)
     y = np.zeros(H.n, np.longdouble)
     for i, (t, r0, c0, m, n, k) in enumerate(lv):
         if t == 0:
-            y[r0:r0 + m] += D[r0:r0 + m, c0:c0 + n].astype(np.longdouble) @ xl[c0:c0 + n]
+            C = D[r0:r0 + m, c0:c0 + n].astype(np.longdouble)
+            if trans:
+                y[c0:c0 + n] += C.T @ xl[r0:r0 + m]
+            else:
+                y[r0:r0 + m] += C @ xl[c0:c0 + n]
         elif k > 0:
-            A, B = H.leaf_factors(i)
-            y[r0:r0 + m] += A.astype(np.longdouble) @ (B.astype(np.longdouble).T @ xl[c0:c0 + n])
+            A, B = (f.astype(np.longdouble) for f in H.leaf_factors(i))
+            if trans:
+                y[c0:c0 + n] += B @ (A.T @ xl[r0:r0 + m])
+            else:
+                y[r0:r0 + m] += A @ (B.T @ xl[c0:c0 + n])
     return b.astype(np.longdouble) - y
 
 
@@ -43,10 +51,10 @@ def test_compensated_residual_vs_long_double():
     err64 = float(np.linalg.norm((r64 - ref).astype(np.float64)))
     assert err <= 1e-17 * scale, err / scale
     assert err64 > 10 * err                               # the plain FP64 residual is coarser
-    # transposed: b - H' x
+    # transposed: b - H' x against the same long-double sum over the leaves
     rt = H.residual(x, b, trans=True)
-    Dt = H.to_dense().T.astype(np.longdouble)
-    assert np.linalg.norm((rt - (b - Dt @ x.astype(np.longdouble))).astype(np.float64)) <= 1e-6 * np.linalg.norm(rt)
+    reft = _longdouble_residual(H, x, b, trans=True)
+    assert float(np.linalg.norm((rt - reft).astype(np.float64))) <= 1e-17 * scale
 
 
 def test_residual_device_pointers_two_columns():
