@@ -28,4 +28,4 @@ def test_autotune_single_and_block():
     table, choice = H32.autotune(ncols=40, calls=2)
     assert set(k for k in table if k.startswith("tc_")) == {"tc_nc16_cols40", "tc_nc32_cols40", "tc_nc64_cols40"}
     assert choice["tc_nc"][2] in (16, 32, 64)
-    assert np.linalg.norm(H32 * X - Y0) <= 2e-6 * np.linalg.norm(Y0)
+    assert np.linalg.norm(H32 * X - Y0) <= 1e-5 * np.linalg.norm(Y0)

@@ -8,10 +8,12 @@ the stacked factor products run as tensor-core GEMMs.  Checked:
   M-major of phase 2);
 * H*X and H'*X on the tensor cores against the CUDA-core block kernels on the
   same stored factors (HM_FLAG_MV_SIMT) and against the FP64-factor product:
-  FP32 factors use three TF32 products per term, so the two paths agree to
-  2e-6 relative; BF16 factors multiply a two-part BF16 split of X, so they
-  agree to 2e-5, far inside the BF16 storage error itself (about 3e-3 against
-  FP64 factors);
+  FP32 factors use three TF32 products per term and FP32 accumulation; the
+  rows of H X cancel (|H X| is about 20 times below |H| |X| for random X), so
+  both FP32-accumulated paths sit a few 1e-6 from the FP64 result: 1e-5.  BF16
+  factors multiply a two-part BF16 split of X: 2e-5 against the CUDA-core
+  path, far inside the BF16 storage error itself (about 3e-3 against FP64
+  factors);
 * both the median-bisection tree (every leaf on a 16-byte row boundary) and
   the reference's KMeans tree (leaves at arbitrary rows: the unaligned gather
   path).
@@ -23,7 +25,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"F32": 2e-6, "BF16": 2e-5}
+TOL = {"F32": 1e-5, "BF16": 2e-5}
 
 
 def _bf16(x):
@@ -95,7 +97,7 @@ def test_tc_against_fp64_factors():
     _, H64 = _build("F64", "bisect", n)
     X = np.random.default_rng(22).standard_normal((n, 16))
     R = H64 * X
-    assert np.linalg.norm(H32 * X - R) <= 2e-6 * np.linalg.norm(R)
+    assert np.linalg.norm(H32 * X - R) <= 1e-5 * np.linalg.norm(R)
     assert H32.info().factorized == 0
 
 
