@@ -425,11 +425,11 @@ int hm_residual(hm_handle* h, const double* X, const double* B, double* R, int64
   return HM_OK;
 }
 
-int hm_tc_selftest(int32_t kind, int32_t a_mn, int32_t nc, const float* A, const float* B, float* D) {
+int hm_tc_selftest(int32_t kind, int32_t a_src, int32_t nc, const float* A, const float* B, float* D) {
   if (!A || !B || !D) return fail(HM_ERR_ARG, "invalid argument");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(HM_ERR_CUDA, "no CUDA device");
-  return tc_selftest(kind, a_mn, nc, A, B, D);
+  return tc_selftest(kind, a_src, nc, A, B, D);
 }
 
 int hm_autotune(hm_handle* h, int64_t ncols, int32_t calls, double* times) {

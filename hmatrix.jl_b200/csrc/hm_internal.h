@@ -165,6 +165,8 @@ struct MvPlan {
   int64_t np2 = 0;
   MvWin* d_win = nullptr;
   int32_t nwin = 0;
+  P2Desc* d_p2d = nullptr;         // the dense descriptors alone, window by window (built on first use)
+  MvWin* d_wind = nullptr;         // windows over d_p2d (nwin of them)
 };
 
 struct LuState;            // H-LU data (hm_lu.cu)
@@ -287,7 +289,7 @@ int matvec_multi_device(hm_handle* h, const double* d_x, double* d_y, int64_t nc
 // the low-rank part of Y = H X on the tensor cores, added into Y (hm_matvec_tc.cu)
 int matvec_multi_tc(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st);
 int tc_status(hm_handle* h, cudaStream_t st);
-int tc_selftest(int kind, int a_mn, int nc, const float* A, const float* B, float* D);
+int tc_selftest(int kind, int a_src, int nc, const float* A, const float* B, float* D);
 void free_tc_plan(TcPlan*& p);
 // r = b - H x (trans: b - H' x) with compensated sums (hm_matvec.cu)
 int residual_device(hm_handle* h, const double* d_x, const double* d_b, double* d_r, int trans, cudaStream_t st);

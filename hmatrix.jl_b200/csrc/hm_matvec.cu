@@ -396,6 +396,8 @@ void free_mv_plan(MvPlan& p) {
   if (p.d_t1s) cudaFree(p.d_t1s);
   if (p.d_p2) cudaFree(p.d_p2);
   if (p.d_win) cudaFree(p.d_win);
+  if (p.d_p2d) cudaFree(p.d_p2d);
+  if (p.d_wind) cudaFree(p.d_wind);
   p = MvPlan{};
 }
 

@@ -266,9 +266,7 @@ template <int CB> struct M2Cfg {
   static constexpr int EMAX = CB >= 16 ? 256 : 512;   // entries per sub-round (z rows in shared memory)
 };
 
-// DENSE_ONLY: the dense leaves alone (the low-rank part is added afterwards
-// by the tensor-core kernels)
-template <typename T, typename TD, int CB, bool DENSE_ONLY = false>
+template <typename T, typename TD, int CB>
 __global__ void __launch_bounds__(M2_THREADS) mvm_phase2_kernel(const MvWin* __restrict__ win,
                                                                 const P2Desc* __restrict__ d,
                                                                 const T* __restrict__ rk, const TD* __restrict__ dn,
@@ -305,7 +303,6 @@ __global__ void __launch_bounds__(M2_THREADS) mvm_phase2_kernel(const MvWin* __r
         const int r0 = sd[lane].row_off, r1 = r0 + (int)sd[lane].m;
         const int h0 = (int)(wh & 1) * (2 * M2_THREADS);
         cnt = (r1 > h0 && r0 < h0 + 2 * M2_THREADS) ? (int)sd[lane].cnt : 0;
-        if (DENSE_ONLY && sd[lane].type == P2_RK) cnt = 0;
       }
       int incl = cnt;
 #pragma unroll
@@ -353,6 +350,7 @@ __global__ void __launch_bounds__(M2_THREADS) mvm_phase2_kernel(const MvWin* __r
       __syncthreads();
       for (int e = 0; e < ne; e += U) {
         double2 f[U];
+        bool cov = false;                     // some entry of this group covers a row of this thread
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           f[u] = make_double2(0.0, 0.0);
@@ -363,6 +361,7 @@ __global__ void __launch_bounds__(M2_THREADS) mvm_phase2_kernel(const MvWin* __r
             const uint64_t o = e_off[ee];
             const uint32_t rs = e_rs[ee];
             const int lr = base - ro;
+            cov = cov || (lr + 1 >= 0 && lr < mm);
             const bool dense = (o & M2_DENSE_FLAG) != 0;
             const uint64_t oo = o & ~M2_DENSE_FLAG;
             if (((ro & 1) == 0) && rs == 1) {
@@ -375,6 +374,9 @@ __global__ void __launch_bounds__(M2_THREADS) mvm_phase2_kernel(const MvWin* __r
             }
           }
         }
+        // a warp covers 64 consecutive rows: leaves shorter than the half
+        // window (dense near-field blocks) leave most warps idle here
+        if (!__any_sync(0xffffffffu, cov)) continue;
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           if (e + u < ne) {
@@ -401,6 +403,105 @@ __global__ void __launch_bounds__(M2_THREADS) mvm_phase2_kernel(const MvWin* __r
         const int col = cb * CB + j;
         if (col < ncols) Y[(int64_t)(W.row0 + r) + (int64_t)col * ldy] = acc[q][j];
       }
+    }
+  }
+}
+
+// The dense leaves' part of Y = H X alone (the tensor-core kernels add the
+// low-rank part afterwards).  One CTA per 128 output rows and column block,
+// a warp per 32 rows.  Warp 0 collects the window's dense leaves that cover
+// the tile; for each, the CTA stages the X rows of its input segment in shared
+// memory (DX_ROWS at a time, coalesced) and every warp whose rows it covers
+// streams the leaf column by column (32 consecutive rows a load, eight
+// columns in flight) against those rows.  Each warp writes its rows of Y once.
+constexpr int DX_ROWS = 64;
+
+template <typename TD, int CB>
+__global__ void __launch_bounds__(128) mvm_dense_kernel(const MvWin* __restrict__ win, const P2Desc* __restrict__ d,
+                                                        const TD* __restrict__ dn, const double* __restrict__ xr,
+                                                        int ld, int ncb, int64_t ntile, double* __restrict__ Y,
+                                                        int64_t ldy, int ncols) {
+  __shared__ P2Desc sd[32];
+  __shared__ int s_cnt;
+  __shared__ __align__(16) double xs[DX_ROWS * CB];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cb = (int)(blockIdx.x % ncb);
+  const int64_t grow = (int64_t)(blockIdx.x / ncb) * 128;      // first output row of the tile
+  const MvWin W = win[grow / MV_WROWS];
+  const int t0 = (int)(grow - W.row0);                         // tile rows [t0, t0 + 128) of the window
+  const int w0 = t0 + 32 * warp;                               // this warp's rows [w0, w0 + 32)
+  const int r = w0 + lane;
+  double acc[CB];
+#pragma unroll
+  for (int j = 0; j < CB; ++j) acc[j] = 0.0;
+  for (uint32_t b0 = W.begin; b0 < W.end; b0 += 32) {
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t nb = min(32u, W.end - b0);
+      P2Desc D{};
+      bool cov = false;
+      if ((uint32_t)lane < nb) {
+        D = d[b0 + lane];
+        cov = D.row_off < t0 + 128 && D.row_off + (int)D.m > t0;
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, cov);
+      if (cov) sd[__popc(bal & ((1u << lane) - 1u))] = D;
+      if (lane == 0) s_cnt = __popc(bal);
+    }
+    __syncthreads();
+    const int cnt = s_cnt;
+    for (int li = 0; li < cnt; ++li) {
+      const P2Desc L = sd[li];
+      const bool wcov = L.row_off < w0 + 32 && L.row_off + (int)L.m > w0;   // uniform per warp
+      const int lr = r - L.row_off;
+      const bool mine = lr >= 0 && lr < (int)L.m;
+      const bool tr = L.type == P2_DENSE_T;
+      const TD* col = dn + L.off + (mine ? (tr ? (int64_t)lr * L.ld : (int64_t)lr) : 0);
+      const int64_t cs = tr ? 1 : (int64_t)L.ld;                // distance between the leaf's input columns
+      for (uint32_t c0 = 0; c0 < L.cnt; c0 += DX_ROWS) {
+        const int nr = (int)min((uint32_t)DX_ROWS, L.cnt - c0);
+        __syncthreads();                                         // the previous rows are consumed
+        for (int e = threadIdx.x; e < nr * (CB / 2); e += blockDim.x) {
+          const int rr = e / (CB / 2), jj = e % (CB / 2);
+          reinterpret_cast<double2*>(xs)[e] =
+              __ldg(reinterpret_cast<const double2*>(xr + (int64_t)(L.aux + c0 + rr) * ld + cb * CB) + jj);
+        }
+        __syncthreads();
+        if (!wcov) continue;
+        int c = 0;
+        for (; c + 8 <= nr; c += 8) {
+          double v[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) v[u] = mine ? (double)__ldcs(col + (int64_t)(c0 + c + u) * cs) : 0.0;
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const double* xx = xs + (c + u) * CB;
+#pragma unroll
+            for (int j = 0; j < CB; j += 2) {
+              const double2 x = *reinterpret_cast<const double2*>(xx + j);
+              acc[j] = fma(v[u], x.x, acc[j]);
+              acc[j + 1] = fma(v[u], x.y, acc[j + 1]);
+            }
+          }
+        }
+        for (; c < nr; ++c) {
+          const double v = mine ? (double)__ldcs(col + (int64_t)(c0 + c) * cs) : 0.0;
+          const double* xx = xs + c * CB;
+#pragma unroll
+          for (int j = 0; j < CB; j += 2) {
+            const double2 x = *reinterpret_cast<const double2*>(xx + j);
+            acc[j] = fma(v, x.x, acc[j]);
+            acc[j + 1] = fma(v, x.y, acc[j + 1]);
+          }
+        }
+      }
+    }
+  }
+  if (r < (int)W.nrows) {
+#pragma unroll
+    for (int j = 0; j < CB; ++j) {
+      const int cl = cb * CB + j;
+      if (cl < ncols) Y[(int64_t)(W.row0 + r) + (int64_t)cl * ldy] = acc[j];
     }
   }
 }
@@ -448,6 +549,30 @@ static int ensure_sorted_p1(MvPlan& P) {
   return HM_OK;
 }
 
+// The dense-leaf descriptors alone, window by window (the tensor-core path
+// adds the low-rank part itself, so its CUDA-core pass skips those entirely).
+static int ensure_dense_p2(MvPlan& P) {
+  if (P.d_wind || P.nwin == 0) return HM_OK;
+  std::vector<P2Desc> v((size_t)P.np2);
+  std::vector<MvWin> win((size_t)P.nwin);
+  if (P.np2 > 0) HM_CUDA_TRY(cudaMemcpy(v.data(), P.d_p2, sizeof(P2Desc) * v.size(), cudaMemcpyDeviceToHost));
+  HM_CUDA_TRY(cudaMemcpy(win.data(), P.d_win, sizeof(MvWin) * win.size(), cudaMemcpyDeviceToHost));
+  std::vector<P2Desc> d;
+  for (MvWin& W : win) {
+    const uint32_t b = (uint32_t)d.size();
+    for (uint32_t i = W.begin; i < W.end; ++i)
+      if (v[i].type != P2_RK) d.push_back(v[i]);
+    W.begin = b;
+    W.end = (uint32_t)d.size();
+  }
+  if (d.empty()) d.push_back(P2Desc{});          // keeps the pointer valid; no window refers to it
+  HM_CUDA_TRY(cudaMalloc(&P.d_p2d, sizeof(P2Desc) * d.size()));
+  HM_CUDA_TRY(cudaMemcpy(P.d_p2d, d.data(), sizeof(P2Desc) * d.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(cudaMalloc(&P.d_wind, sizeof(MvWin) * win.size()));
+  HM_CUDA_TRY(cudaMemcpy(P.d_wind, win.data(), sizeof(MvWin) * win.size(), cudaMemcpyHostToDevice));
+  return HM_OK;
+}
+
 template <typename T, int CB>
 int launch_multi(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st,
                  bool dense_only = false) {
@@ -478,8 +603,12 @@ int launch_multi(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, in
   const int64_t nblk = (int64_t)P.nwin * 2 * ncb;
   if (nblk > (int64_t)INT32_MAX) return fail(HM_ERR_UNSUPPORTED, "too many phase-2 blocks");
   if (dense_only) {
-    mvm_phase2_kernel<T, TD, CB, true><<<(unsigned)nblk, M2_THREADS, 0, st>>>(
-        P.d_win, P.d_p2, (const T*)h->d_rk, (const TD*)h->d_dense, zr, xr, ld, ncb, d_y, h->n, (int)ncols);
+    HM_TRY(ensure_dense_p2(P));
+    const int64_t ntile = (h->n + 127) / 128;
+    const int64_t blocks = ntile * ncb;
+    if (blocks > (int64_t)INT32_MAX) return fail(HM_ERR_UNSUPPORTED, "too many dense-pass blocks");
+    mvm_dense_kernel<TD, CB><<<(unsigned)blocks, 128, 0, st>>>(P.d_wind, P.d_p2d, (const TD*)h->d_dense, xr, ld, ncb,
+                                                             ntile, d_y, h->n, (int)ncols);
     HM_CUDA_TRY(cudaGetLastError());
     return HM_OK;
   }

@@ -3,17 +3,32 @@
 // stored factors, the device form of *(Hmat, Matrix) (src/harithm.jl:
 // 317-329), which the reference evaluates one column at a time.
 //
-// Phase 1 (Z = F1' X_seg): the factor columns of all low-rank leaves that
-//   share one input segment are stacked into 128-row M-tiles; one tcgen05 MMA
-//   chain per tile computes Z_tile = F1_stack' X_seg (K = segment points,
-//   N = columns) into a TMEM accumulator.  The factor rows are gathered into
-//   shared memory by cp.async (their pool offsets are irregular), the X tiles
-//   come pre-tiled from HBM by 1-D bulk copies (TMA engine).
-// Phase 2 (Y += F2 Z): output windows of 512 rows (4 M-tiles); K runs over
-//   the low-rank columns that touch the window (their Z rows are laid out
-//   contiguously per window by phase 1's epilogue), A = F2 columns in
-//   M-major form (rows contiguous in the pool).  Dense leaves are added by
-//   the CUDA-core block kernel first.
+// Phase 1 (Z = F1' X_seg): the factor columns of the low-rank leaves that
+//   share one input segment are cut into 128-column M-tiles; one tcgen05 MMA
+//   chain per tile computes Z_tile = F1_tile' X_seg (K = segment points,
+//   N = right-hand-side columns) into a TMEM accumulator.
+// Phase 2 (Y += F2 Z): an output window of 512 rows keeps its Z slots (the k
+//   values of every leaf that touches the window) contiguous; one MMA chain
+//   per 128-row tile of a window runs K over the window's slots.  The dense
+//   leaves are added by the CUDA-core block kernel first.
+//
+// Data movement.  Factor columns are contiguous in the pool, so a pipeline
+// stage takes one contiguous piece of each factor column it needs (phase 1:
+// KC values = 256 bytes of each of the tile's 128 columns; phase 2: the
+// tile's rows of each of KC columns) into a raw shared-memory stage, by
+// 16-byte cp.async gathers of four producer warps (16 lanes per 256-byte
+// piece, so every warp instruction reads whole 128-byte lines) whose
+// completion arrives on the stage's mbarrier without blocking the producers
+// (cp.async.mbarrier.arrive.noinc).  A 1-D bulk copy per factor column would
+// be simpler, but each lane's bulk copy issues separately (about 80 cycles a
+// copy measured), which capped a single producer warp near 1 TB/s.  The X / Z
+// tile of the stage, one contiguous block pre-tiled in the MMA's K-major
+// core-matrix layout, arrives by one bulk copy of the TMA engine.  Converter warps read the
+// raw stage row by row (one TMEM lane per thread), split FP32 values into TF32
+// hi and lo parts, and write the A operand straight into tensor memory
+// (tcgen05.st); the MMA reads A from TMEM and B from shared memory.  Shared
+// memory thus carries each factor byte twice (bulk-copy write, converter read)
+// instead of five times when hi/lo operand tiles are staged in shared memory.
 //
 // Accuracy.  FP32 factors use three TF32 products per term (F_hi X_hi +
 // F_hi X_lo + F_lo X_hi, the split of Ootomo & Yokota 2022), BF16 factors
@@ -22,11 +37,14 @@
 // Both splits round to nearest and leave exact values of the narrow format,
 // so the hardware's own input conversion does not matter.
 //
-// Pipeline per CTA (persistent, one per SM): warps 0-3 produce stages
-// (cp.async gathers, the split of FP32 factors into hi/lo, the bulk copy of
-// the X / Z tile), warp 8 issues the MMAs (one thread), warps 4-7 drain the
-// TMEM accumulators (tcgen05.ld).  mbarriers link the roles; every wait is
-// bounded and a timeout sets an error word and ends the kernel cleanly.
+// Roles per CTA (persistent, one per SM, 13 warps): warps 8-11 produce stages;
+// warps 0-7 convert them into two TMEM A buffers (warp w: TMEM lanes
+// 32 (w % 4) .., the K half w / 4 of each stage, two converter warps per SM
+// sub-partition) and drain the accumulator of the previous tile (tcgen05.ld)
+// once its MMAs are known to be done; warp 12 issues the MMAs (one thread).
+// The two TMEM accumulators alternate between tiles.  mbarriers link
+// the roles; every wait is bounded, and a timeout sets an error word and ends
+// the kernel cleanly once the copies and MMAs in flight have finished.
 #include "hm_internal.h"
 #include "hm_tc.cuh"
 
@@ -39,7 +57,7 @@ struct TcCol1 {            // phase-1 M row: one factor column of F1
   uint64_t off;            // pool element offset of the column's first entry
   uint32_t zp0, zp1;       // its Z slots: zpl[zp0 .. zp1)
 };
-struct TcItem1 {           // up to TC_T tiles of one input segment
+struct TcItem1 {           // one tile of up to 128 columns of one input segment
   uint32_t col0, ncol;     // columns [col0, col0 + ncol) of the column table
   uint32_t seg0, len;      // input index range of the segment
 };
@@ -47,9 +65,11 @@ struct TcZ2 {              // phase-2 K column (a Z slot) inside its window
   int64_t a_off;           // pool element offset of F2 at window row rlo
   int32_t rlo, rhi;        // rows [rlo, rhi) of the window it covers
 };
-struct TcItem2 {           // one output window
-  uint32_t row0, nrows;
-  uint32_t zb, ze;         // its Z slots [zb, ze)
+struct TcItem2 {           // one tile of up to 128 rows of an output window
+  uint32_t row0, nrows;    // first output row of the tile, its rows
+  uint32_t zb, ze;         // the window's Z slots [zb, ze)
+  uint32_t toff;           // row offset of the tile inside its window
+  uint32_t pad;
 };
 
 struct TcPlan {
@@ -63,38 +83,199 @@ struct TcPlan {
   int64_t nz2 = 0;
   TcItem2* d_item2 = nullptr;
   int64_t nitem2 = 0;
-  bool aligned = true;     // every phase-2 column starts on a 16-byte row group
 };
 
 namespace {
 
-constexpr int TC_T = 4;              // 128-row M-tiles per work item
-constexpr int TC_WR = 128 * TC_T;    // rows of a phase-2 output window
-constexpr int TC_KB = 4;             // 16-byte K blocks per pipeline stage
-constexpr int TC_STAGES = 3;
-constexpr int TC_THREADS = 288;      // warps 0-3 producers, 4-7 epilogue, 8 MMA
-constexpr int TC_PROD = 128;
+constexpr int TC_WR = 512;           // rows of a phase-2 window
+constexpr int TC_THREADS = 416;      // warps 0-7 convert + drain, 8-11 produce, 12 MMA
+constexpr int TC_PROD0 = 256;        // first producer thread
+constexpr int TC_NA = 2;             // TMEM A buffers
+constexpr int TC_TMEM_COLS = 512;    // one CTA per SM (shared memory), so all of TMEM
 constexpr uint32_t TC_WAIT = 1u << 22;   // polls of a bounded mbarrier wait
 
 template <typename T> struct TcT;
 template <> struct TcT<float> {
   static constexpr int KE = 4;                      // elements per 16 bytes
+  static constexpr int KC = 64;                     // K values per stage (256 bytes of a column)
+  static constexpr int KM = 8;                      // K values per MMA
+  static constexpr int ACOLS = 2 * KC;              // TMEM columns of an A buffer: hi | lo
   static constexpr int KIND = 0;                    // kind::tf32
   static constexpr int FMT = tc::FMT_TF32;
   static constexpr bool SPLIT = true;               // A = A_hi + A_lo
+  static constexpr int SIG = 11;                    // significant bits of the narrow format
+  static constexpr int SHIFT = 0;                   // its bits: the FP32 pattern >> SHIFT
   using Bits = uint32_t;
   __device__ static float hi(float x) { return tc::tf32_rn(x); }
   __device__ static Bits bits(float x) { return __float_as_uint(x); }
 };
 template <> struct TcT<__nv_bfloat16> {
   static constexpr int KE = 8;
+  static constexpr int KC = 128;
+  static constexpr int KM = 16;
+  static constexpr int ACOLS = KC / 2;              // two BF16 values per 32-bit column
   static constexpr int KIND = 1;                    // kind::f16, BF16 inputs
   static constexpr int FMT = tc::FMT_BF16;
   static constexpr bool SPLIT = false;              // BF16 factors are exact
+  static constexpr int SIG = 8;
+  static constexpr int SHIFT = 16;
   using Bits = uint16_t;
   __device__ static float hi(float x) { return tc::bf16_rn(x); }
   __device__ static Bits bits(float x) { return (uint16_t)(__float_as_uint(x) >> 16); }
 };
+
+// shared memory and TMEM of one CTA
+template <typename T, int NC>
+struct TcCfg {
+  using Tr = TcT<T>;
+  static constexpr int KE = Tr::KE, KC = Tr::KC, ES = (int)sizeof(T);
+  static constexpr int S = NC <= 16 ? 5 : (NC <= 32 ? 4 : 3);   // pipeline stages
+  static constexpr int B_BYTES = KC * 2 * NC * ES;           // the X / Z tile of a stage (hi | lo parts)
+  static constexpr int RS1 = KC * ES + 16;                   // phase-1 raw row: one column's KC values (+16: banks)
+  static constexpr int RAW1 = 128 * RS1;
+  static constexpr int RS2 = (128 + KE) * ES;                // phase-2 raw row: one slot's 128 rows (+KE: shift)
+  static constexpr int RAW2 = KC * RS2;
+  static constexpr int META = KC * 16;                       // phase-2 slot table: rows [lo, hi), word offset
+  static constexpr int RAW = RAW1 > RAW2 + META ? RAW1 : RAW2 + META;
+  static constexpr int STAGE = (B_BYTES + RAW + 1023) / 1024 * 1024;
+  static constexpr int BAR_OFF = S * STAGE;
+  static constexpr int BYTES = BAR_OFF + 512;
+  static constexpr int ACC0 = TC_NA * Tr::ACOLS;             // first accumulator column
+  static_assert(BYTES <= 227 * 1024, "stages exceed the shared memory of a CTA");
+  static_assert(ACC0 + 2 * 2 * NC <= TC_TMEM_COLS, "A buffers and accumulators exceed TMEM");
+  static_assert(RS1 % 16 == 0 && RS2 % 16 == 0 && B_BYTES % 16 == 0, "bulk copies move 16-byte units");
+  static_assert(KC % 4 == 0 && KC % Tr::KM == 0, "a stage is whole MMAs and whole producer warps");
+};
+
+struct TcBars {
+  uint64_t full[5];        // raw stage landed (the producers' cp.async arrivals)
+  uint64_t bfull[5];       // the stage's B tile landed (bulk-copy bytes + one arrival)
+  uint64_t empty[5];       // the MMAs that read the stage's B tile finished (tcgen05.commit)
+  uint64_t afull[TC_NA];   // A buffer written (256 converter threads)
+  uint64_t aempty[TC_NA];  // the MMAs that read the A buffer finished
+  uint64_t accfull[2];     // accumulator complete (commit after a tile's last MMA)
+  uint64_t accempty[2];    // accumulator drained (256 converter threads)
+  uint64_t done;           // the MMA issuer's last commit: every MMA finished
+  uint32_t tmem;
+  int abort;
+};
+static_assert(sizeof(TcBars) <= 512, "barrier block");
+static_assert((TcT<float>::KE & (TcT<float>::KE - 1)) == 0 && (TcT<__nv_bfloat16>::KE & (TcT<__nv_bfloat16>::KE - 1)) == 0,
+              "K blocks of a power-of-two size");
+static_assert(TcT<float>::KC * 4 == 256 && TcT<__nv_bfloat16>::KC * 2 == 256, "phase-1 pieces are 16 x 16 bytes");
+
+__device__ __forceinline__ void tc_fail(int* err, TcBars* b, int code) {
+  atomicOr(&b->abort, 1);
+  atomicOr(err, code);
+}
+__device__ __forceinline__ bool tc_aborted(const TcBars* b) { return *(volatile const int*)&b->abort != 0; }
+
+// Bounded wait that also gives up once another role has aborted; a timeout
+// records `code`.
+__device__ __forceinline__ bool tc_wait(TcBars* b, uint64_t* bar, uint32_t parity, int* err, int code) {
+  for (uint32_t i = 0; i < TC_WAIT; ++i) {
+    if (tc::mbar_try_wait(bar, parity)) return true;
+    if ((i & 63u) == 63u && tc_aborted(b)) return false;
+  }
+  tc_fail(err, b, code);
+  return false;
+}
+// the same for a whole warp: every lane waits, the outcome is uniform
+__device__ __forceinline__ bool tc_wait_warp(TcBars* b, uint64_t* bar, uint32_t parity, int* err, int code) {
+  const bool ok = tc_wait(b, bar, parity, err, code);
+  return __all_sync(0xffffffffu, ok) != 0;
+}
+
+// barriers, TMEM; called by all threads.  full_count: arrivals that complete
+// a raw stage.
+__device__ __forceinline__ uint32_t tc_setup(TcBars* b, int warp, int nstage, uint32_t full_count) {
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < nstage; ++s) {
+      tc::mbar_init(&b->full[s], full_count);
+      tc::mbar_init(&b->bfull[s], 1);
+      tc::mbar_init(&b->empty[s], 1);
+    }
+    for (int q = 0; q < TC_NA; ++q) {
+      tc::mbar_init(&b->afull[q], 256);
+      tc::mbar_init(&b->aempty[q], 1);
+    }
+    for (int q = 0; q < 2; ++q) {
+      tc::mbar_init(&b->accfull[q], 1);
+      tc::mbar_init(&b->accempty[q], 256);
+    }
+    tc::mbar_init(&b->done, 1);
+    b->abort = 0;
+    tc::fence_mbar_init();
+  }
+  if (warp == 4) tc::tmem_alloc(&b->tmem, TC_TMEM_COLS);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  return b->tmem;
+}
+
+// end of the kernel: copies and MMAs have finished; free TMEM
+__device__ __forceinline__ void tc_teardown(TcBars* b, int warp, uint32_t tmem) {
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 4) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tmem, TC_TMEM_COLS);
+  }
+}
+
+// The B-tile producer's last step: every bulk copy it issued has landed.  The
+// wait ignores an abort (shared memory must not be released under copies in
+// flight) but stays bounded.  `it` stages were issued, stage s last by the
+// largest iteration below `it` that is s mod nstage.
+__device__ __forceinline__ void tc_copies_drain(TcBars* b, uint32_t it, int nstage, int* err) {
+  for (int s = 0; s < nstage && (uint32_t)s < it; ++s) {
+    const uint32_t last = it - 1 - ((it - 1 - (uint32_t)s) % (uint32_t)nstage);
+    if (!tc::mbar_wait(&b->bfull[s], (last / (uint32_t)nstage) & 1u, TC_WAIT)) tc_fail(err, b, 32);
+  }
+}
+
+// MMA issuer (one thread): per tile, K stages of A (TMEM) x B (shared
+// memory) into accumulator q = tile parity; nk_of(w) gives tile w's stages.
+template <typename T, int NC, typename NkOf>
+__device__ __forceinline__ void tc_mma_role(TcBars* b, uint32_t sbase, uint32_t tmem, int64_t nitems, NkOf nk_of,
+                                            int* err) {
+  using Tr = TcT<T>;
+  using C = TcCfg<T, NC>;
+  constexpr uint32_t LBO_B = 2 * NC * 16, SBO_B = 128;        // K-major [hi | lo] B tiles
+  const uint32_t id_full = tc::idesc(Tr::FMT, 2 * NC, 0, 0);
+  const uint32_t id_half = tc::idesc(Tr::FMT, NC, 0, 0);
+  uint32_t it = 0, j = 0;
+  bool ok = true;
+  int nk = blockIdx.x < nitems ? nk_of(blockIdx.x) : 0;
+  for (int64_t w = blockIdx.x; w < nitems && ok; w += gridDim.x, ++j) {
+    const int nk_next = w + gridDim.x < nitems ? nk_of(w + gridDim.x) : 0;   // loaded ahead of its use
+    const uint32_t q = j & 1u;
+    if (!tc_wait(b, &b->accempty[q], ((j >> 1) & 1u) ^ 1u, err, 2)) break;
+    tc::tc_fence_after();
+    const uint32_t dacc = tmem + (uint32_t)C::ACC0 + q * 2 * NC;
+    for (int kc = 0; kc < nk; ++kc, ++it) {
+      const int s = (int)(it % C::S), a = (int)(it % TC_NA);
+      if (!tc_wait(b, &b->bfull[s], (it / C::S) & 1u, err, 4)) { ok = false; break; }
+      if (!tc_wait(b, &b->afull[a], (it / TC_NA) & 1u, err, 4)) { ok = false; break; }
+      tc::tc_fence_after();
+      const uint32_t bbase = sbase + (uint32_t)(s * C::STAGE);
+      const uint32_t abuf = tmem + (uint32_t)(a * Tr::ACOLS);
+#pragma unroll
+      for (int ks = 0; ks < Tr::KC / Tr::KM; ++ks) {
+        const uint64_t bd = tc::smem_desc(bbase + ks * 2 * LBO_B, LBO_B, SBO_B);
+        tc::mma_ts<Tr::KIND>(dacc, abuf + ks * 8, bd, id_full, (kc > 0 || ks > 0) ? 1u : 0u);
+        if constexpr (Tr::SPLIT) tc::mma_ts<Tr::KIND>(dacc, abuf + Tr::KC + ks * 8, bd, id_half, 1u);
+      }
+      tc::mma_commit(&b->empty[s]);
+      tc::mma_commit(&b->aempty[a]);
+    }
+    if (ok) tc::mma_commit(&b->accfull[q]);
+    nk = nk_next;
+  }
+  tc::mma_commit(&b->done);
+  if (!tc::mbar_wait(&b->done, 0u, TC_WAIT)) tc_fail(err, b, 16);
+}
 
 // ---------------------------------------------------------------------------
 // X tiles for the B operand: XT[q][kb][part][n][e] holds part (0: hi, 1: lo)
@@ -135,71 +316,89 @@ __global__ void tc_zero_kernel(typename TcT<T>::Bits* __restrict__ p, int64_t cn
     p[e] = 0;
 }
 
-// shared memory of one CTA
-template <typename T, int NC>
-struct TcSmem {
-  static constexpr int A_TILE = 128 * TC_KB * 16;                     // bytes of one 128-row A tile
-  static constexpr int A_STAGE = TC_T * A_TILE;
-  static constexpr int A_LO = TcT<T>::SPLIT ? A_STAGE : 0;
-  static constexpr int B_STAGE = TC_KB * 2 * NC * 16;
-  static constexpr int STAGE = A_STAGE + A_LO + B_STAGE;
-  static constexpr int BAR_OFF = TC_STAGES * STAGE;
-  static constexpr int BYTES = BAR_OFF + 256;
-  static constexpr int TMEM_COLS = TC_T * 2 * NC <= 32 ? 32 : (TC_T * 2 * NC <= 64 ? 64 : (TC_T * 2 * NC <= 128 ? 128 : (TC_T * 2 * NC <= 256 ? 256 : 512)));
-  static_assert(BYTES <= 227 * 1024, "stages exceed the shared memory of a CTA");
-  static_assert(TC_T * 2 * NC <= 512, "accumulators exceed TMEM");
-};
-
-struct TcBars {
-  uint64_t full[TC_STAGES];
-  uint64_t empty[TC_STAGES];
-  uint64_t acc_full;
-  uint64_t acc_empty;
-  uint64_t done;           // the MMA issuer's last commit: every MMA finished
-  uint32_t tmem;
-  int abort;
-};
-
-__device__ __forceinline__ void tc_fail(int* err, TcBars* b, int code) {
-  atomicOr(&b->abort, 1);
-  atomicOr(err, code);
-}
-__device__ __forceinline__ bool tc_aborted(const TcBars* b) { return *(volatile const int*)&b->abort != 0; }
-
-// barriers, TMEM; called by all threads
-__device__ __forceinline__ uint32_t tc_setup(TcBars* bars, int warp, uint32_t tmem_cols) {
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < TC_STAGES; ++s) {
-      tc::mbar_init(&bars->full[s], TC_PROD + 1);    // 128 producers + the bulk-copy arrival
-      tc::mbar_init(&bars->empty[s], 1);             // one tcgen05.commit
+// ---------------------------------------------------------------------------
+// converters: raw shared-memory rows -> TMEM A rows (this thread's lane)
+// ---------------------------------------------------------------------------
+// Each converter warp writes 32 TMEM columns of the stage's A buffer, half h
+// (FP32: K values [32 h, 32 h + 32) as hi and lo; BF16: columns
+// [32 h, 32 h + 32), i.e. K values [64 h, 64 h + 64)).
+// phase 1: `raw` is this row's KC values (a factor column's chunk), of which
+// the first kl are valid (the rest is padding or stale and becomes zero)
+__device__ __forceinline__ void conv1(const uint8_t* raw, int kl, uint32_t ta, int h, float*) {
+  constexpr int KC = TcT<float>::KC;
+#pragma unroll
+  for (int c0 = 32 * h; c0 < 32 * h + 32; c0 += 16) {
+    float x[16];
+    uint32_t hi[16], lo[16];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const float4 x4 = *reinterpret_cast<const float4*>(raw + (c0 + 4 * v) * 4);
+      x[4 * v + 0] = c0 + 4 * v + 0 < kl ? x4.x : 0.f;
+      x[4 * v + 1] = c0 + 4 * v + 1 < kl ? x4.y : 0.f;
+      x[4 * v + 2] = c0 + 4 * v + 2 < kl ? x4.z : 0.f;
+      x[4 * v + 3] = c0 + 4 * v + 3 < kl ? x4.w : 0.f;
     }
-    tc::mbar_init(&bars->acc_full, 1);
-    tc::mbar_init(&bars->acc_empty, 128);            // the 4 epilogue warps
-    tc::mbar_init(&bars->done, 1);
-    bars->abort = 0;
-    tc::fence_mbar_init();
-  }
-  if (warp == 4) tc::tmem_alloc(&bars->tmem, tmem_cols);
-  tc::tc_fence_before();
-  __syncthreads();
-  tc::tc_fence_after();
-  return bars->tmem;
-}
-
-// end of the kernel: the MMA issuer has waited for its last MMAs; free TMEM
-__device__ __forceinline__ void tc_teardown(TcBars* bars, int warp, uint32_t tmem, uint32_t tmem_cols) {
-  tc::tc_fence_before();
-  __syncthreads();
-  if (warp == 4) {
-    tc::tc_fence_after();
-    tc::tmem_dealloc(tmem, tmem_cols);
+    tc::split_n<11>(x, hi, lo);
+    tc::tmem_st16(ta + c0, hi);
+    tc::tmem_st16(ta + KC + c0, lo);
   }
 }
+__device__ __forceinline__ void conv1(const uint8_t* raw, int kl, uint32_t ta, int h, __nv_bfloat16*) {
+#pragma unroll
+  for (int c0 = 32 * h; c0 < 32 * h + 32; c0 += 16) {          // 16 columns = 32 values
+    uint32_t wv[16];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const uint4 u = *reinterpret_cast<const uint4*>(raw + 4 * (c0 + 4 * v));
+      const uint32_t us[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int k = 2 * (c0 + 4 * v + e);           // values k (low half) and k + 1 (high half)
+        uint32_t x = us[e];
+        if (k >= kl) x = 0u;
+        else if (k + 1 >= kl) x &= 0xFFFFu;
+        wv[4 * v + e] = x;
+      }
+    }
+    tc::tmem_st16(ta + c0, wv);
+  }
+}
 
-// the MMA issuer's last step: one commit and a bounded wait for it
-__device__ __forceinline__ void tc_mma_drain(TcBars* bars, int* err) {
-  tc::mma_commit(&bars->done);
-  if (!tc::mbar_wait(&bars->done, 0u, TC_WAIT)) tc_fail(err, bars, 16);
+// phase 2: slot k's tile row m sits at element meta[k].z + m of the raw
+// area when m is in [meta[k].x, meta[k].y) (the covered rows), else is 0
+__device__ __forceinline__ float slot_val(const uint8_t* rb, const int4* meta, int k, int m, float*) {
+  const int4 md = meta[k];
+  return (m >= md.x && m < md.y) ? reinterpret_cast<const float*>(rb)[md.z + m] : 0.f;
+}
+__device__ __forceinline__ uint32_t slot_val(const uint8_t* rb, const int4* meta, int k, int m, __nv_bfloat16*) {
+  const int4 md = meta[k];
+  return (m >= md.x && m < md.y) ? (uint32_t)reinterpret_cast<const uint16_t*>(rb)[md.z + m] : 0u;
+}
+__device__ __forceinline__ void conv2(const uint8_t* rb, const int4* meta, int m, uint32_t ta, int h, float* tag) {
+  constexpr int KC = TcT<float>::KC;
+#pragma unroll 1
+  for (int c0 = 32 * h; c0 < 32 * h + 32; c0 += 16) {
+    float x[16];
+    uint32_t hi[16], lo[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) x[j] = slot_val(rb, meta, c0 + j, m, tag);
+    tc::split_n<11>(x, hi, lo);
+    tc::tmem_st16(ta + c0, hi);
+    tc::tmem_st16(ta + KC + c0, lo);
+  }
+}
+__device__ __forceinline__ void conv2(const uint8_t* rb, const int4* meta, int m, uint32_t ta, int h,
+                                      __nv_bfloat16* tag) {
+#pragma unroll 1
+  for (int c0 = 32 * h; c0 < 32 * h + 32; c0 += 16) {
+    uint32_t wv[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int k = 2 * (c0 + j);
+      wv[j] = slot_val(rb, meta, k, m, tag) | (slot_val(rb, meta, k + 1, m, tag) << 16);
+    }
+    tc::tmem_st16(ta + c0, wv);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -221,205 +420,151 @@ struct P1Args {
 template <typename T, int NC>
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase1_kernel(P1Args<T, NC> a) {
   using Tr = TcT<T>;
-  using S = TcSmem<T, NC>;
-  constexpr int KE = Tr::KE;
-  constexpr int KC = TC_KB * KE;                    // K values per stage
+  using C = TcCfg<T, NC>;
+  constexpr int KE = Tr::KE, KC = Tr::KC;
   extern __shared__ __align__(1024) uint8_t smem[];
-  TcBars* bars = reinterpret_cast<TcBars*>(smem + S::BAR_OFF);
+  TcBars* bars = reinterpret_cast<TcBars*>(smem + C::BAR_OFF);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t tmem = tc_setup(bars, warp, S::TMEM_COLS);
+  const uint32_t tmem = tc_setup(bars, warp, C::S, 128);    // 128 producer cp.async arrivals
   const uint32_t sbase = tc::smem_u32(smem);
+  auto nk_of = [&](int64_t w) { return (int)((a.items[w].len + KC - 1) / KC); };
 
-  if (warp < 4) {
-    // ---------------- producers ----------------
-    const int tid = threadIdx.x;
-    uint32_t it = 0;                                // stage iterations issued
-    uint32_t fin = 0;                               // stage iterations finished (split + arrive)
-    auto finish = [&](uint32_t f) {
-      const int s = (int)(f % TC_STAGES);
-      if constexpr (Tr::SPLIT) {
-        // this thread's own chunks: A_hi in place, A_lo beside it
-#pragma unroll
-        for (int j = 0; j < TC_T * 128 * TC_KB / TC_PROD; ++j) {
-          const uint32_t off = (uint32_t)(tid + TC_PROD * j) * 16;
-          float4 v = *reinterpret_cast<const float4*>(smem + s * S::STAGE + off);
-          float4 h, l;
-          h.x = tc::tf32_rn(v.x); l.x = tc::tf32_rn(v.x - h.x);
-          h.y = tc::tf32_rn(v.y); l.y = tc::tf32_rn(v.y - h.y);
-          h.z = tc::tf32_rn(v.z); l.z = tc::tf32_rn(v.z - h.z);
-          h.w = tc::tf32_rn(v.w); l.w = tc::tf32_rn(v.w - h.w);
-          *reinterpret_cast<float4*>(smem + s * S::STAGE + off) = h;
-          *reinterpret_cast<float4*>(smem + s * S::STAGE + S::A_STAGE + off) = l;
-        }
-      }
-      tc::fence_proxy_async_smem();
-      tc::mbar_arrive(&bars->full[s]);
-    };
-    for (int64_t w = blockIdx.x; w < a.nitems; w += gridDim.x) {
-      const TcItem1 I = a.items[w];
-      const int q = (KE - (int)(I.seg0 % KE)) % KE;
-      const int64_t kb0 = ((int64_t)I.seg0 + q) / KE;
+  if (warp >= 8 && warp < 12) {
+    // ---------------- producers: the X tile (one bulk copy) and 256 bytes of each column ----------------
+    // thread pt copies 16-byte piece q of the columns cg, cg + 8, .., cg + 120
+    // (the column offsets are re-read every stage: L1 hits after the first,
+    // and the next tile's are prefetched into L1 while this one streams)
+    const int pt = threadIdx.x - TC_PROD0;
+    const int q = pt & 15, cg = pt >> 4;
+    uint32_t it = 0;
+    int64_t w = blockIdx.x;
+    TcItem1 I = w < a.nitems ? a.items[w] : TcItem1{};
+    bool stop = false;
+    while (w < a.nitems && !stop) {
+      const int64_t w2 = w + gridDim.x;
+      const TcItem1 I2 = w2 < a.nitems ? a.items[w2] : TcItem1{};
+      const int qs = (KE - (int)(I.seg0 % KE)) % KE;
+      const int64_t kb0 = ((int64_t)I.seg0 + qs) / KE;
+      const int64_t plen = pad_to((int64_t)I.len, KE);       // stored column length
       const int nk = (int)((I.len + KC - 1) / KC);
-      // the rows this thread feeds: chunk ci = tid + 128 j -> tile j / 4,
-      // row 8 (tid / 32) + tid % 8 + 32 (j % 4), K block (tid / 8) % 4
-      uint64_t coff[TC_T * 4];
-      bool cval[TC_T * 4];
-#pragma unroll
-      for (int j = 0; j < TC_T * 4; ++j) {
-        const int t = j / 4;
-        const int row = 8 * (tid / 32) + tid % 8 + 32 * (j % 4);
-        const uint32_t c = (uint32_t)(t * 128 + row);
-        cval[j] = c < I.ncol;
-        coff[j] = cval[j] ? a.cols[I.col0 + c].off : 0;
-      }
-      const int b = (tid / 8) % TC_KB;
-      for (int kc = 0; kc < nk; ++kc, ++it) {
-        const int s = (int)(it % TC_STAGES);
-        const uint32_t ph = (it / TC_STAGES) & 1u;
-        if (!tc::mbar_wait(&bars->empty[s], ph ^ 1u, TC_WAIT)) { tc_fail(a.err, bars, 1); break; }
-        if (tc_aborted(bars)) break;
-        const uint32_t abase = sbase + s * S::STAGE;
-        if (tid == 0) {
-          tc::mbar_arrive_expect_tx(&bars->full[s], S::B_STAGE);
-          const typename Tr::Bits* src = a.xt + (int64_t)q * a.xt_copy + (kb0 + (int64_t)kc * TC_KB) * (2 * NC * KE);
-          tc::bulk_g2s(abase + S::A_STAGE + S::A_LO, src, S::B_STAGE, &bars->full[s]);
+      for (int kc = 0; kc < nk; ++kc) {
+        const int s = (int)(it % C::S);
+        if (!tc_wait(bars, &bars->empty[s], ((it / C::S) & 1u) ^ 1u, a.err, 1)) { stop = true; break; }
+        const uint32_t st = sbase + (uint32_t)(s * C::STAGE);
+        const int64_t e0 = (int64_t)kc * KC;
+        if (pt == 0) {
+          tc::mbar_arrive_expect_tx(&bars->bfull[s], (uint32_t)C::B_BYTES);
+          tc::bulk_g2s(st, a.xt + (int64_t)qs * a.xt_copy + (kb0 + e0 / KE) * (2 * NC * KE), C::B_BYTES,
+                       &bars->bfull[s]);
         }
-        const int64_t e0 = (int64_t)kc * KC + b * KE;      // first element of this thread's K block
-        const int64_t left = (int64_t)I.len - e0;
-        const uint32_t bytes = left >= KE ? 16u : (left > 0 ? (uint32_t)left * (uint32_t)sizeof(T) : 0u);
+        const int64_t el = e0 + q * KE;                       // first element of this thread's piece
+        const bool in = el < plen;
+        const uint32_t dst = st + C::B_BYTES + q * 16;
 #pragma unroll
-        for (int j = 0; j < TC_T * 4; ++j) {
-          const uint32_t dst = abase + (uint32_t)(tid + TC_PROD * j) * 16;
-          const T* src = cval[j] && bytes ? a.pool + coff[j] + e0 : a.pool;
-          tc::cp_async16(dst, src, cval[j] ? bytes : 0u);
+        for (int j = 0; j < 16; ++j) {
+          const uint32_t c = (uint32_t)(cg + 8 * j);
+          const bool ok = in && c < I.ncol;
+          const uint64_t off = c < I.ncol ? __ldg(&a.cols[I.col0 + c].off) : 0;
+          tc::cp_async16(dst + c * C::RS1, ok ? (const void*)(a.pool + off + el) : (const void*)a.pool,
+                         ok ? 16u : 0u);
         }
-        tc::cp_async_commit();
-        if (it >= TC_STAGES - 1) {
-          tc::cp_async_wait<TC_STAGES - 1>();
-          finish(fin++);
-        }
-      }
-      if (tc_aborted(bars)) break;
-    }
-    // drain: finish the stages still in flight
-    tc::cp_async_wait<0>();
-    while (fin < it) finish(fin++);
-  } else if (warp == 8) {
-    // ---------------- MMA issuer ----------------
-    if (lane == 0) {
-      constexpr uint32_t LBO_A = 128, SBO_A = TC_KB * 128;       // K-major A tiles
-      constexpr uint32_t LBO_B = 2 * NC * 16, SBO_B = 128;        // K-major [hi | lo] X tiles
-      const uint32_t id_full = tc::idesc(Tr::FMT, 2 * NC, 0, 0);
-      const uint32_t id_half = tc::idesc(Tr::FMT, NC, 0, 0);
-      uint32_t it = 0, item = 0;
-      bool ok = true;
-      for (int64_t w = blockIdx.x; w < a.nitems && ok; w += gridDim.x, ++item) {
-        const TcItem1 I = a.items[w];
-        const int nk = (int)((I.len + KC - 1) / KC);
-        const int ntile = (int)((I.ncol + 127) / 128);
-        if (!tc::mbar_wait(&bars->acc_empty, (item & 1u) ^ 1u, TC_WAIT)) { tc_fail(a.err, bars, 2); ok = false; break; }
-        tc::tc_fence_after();
-        for (int kc = 0; kc < nk; ++kc, ++it) {
-          const int s = (int)(it % TC_STAGES);
-          const uint32_t ph = (it / TC_STAGES) & 1u;
-          if (!tc::mbar_wait(&bars->full[s], ph, TC_WAIT)) { tc_fail(a.err, bars, 4); ok = false; break; }
-          tc::tc_fence_after();
-          const uint32_t abase = sbase + s * S::STAGE;
-          const uint32_t bbase = abase + S::A_STAGE + S::A_LO;
-          for (int t = 0; t < ntile; ++t) {
+        tc::cp_async_mbar_arrive(&bars->full[s]);
+        ++it;
+        if (kc == 0 && q == 0) {
 #pragma unroll
-            for (int ks = 0; ks < TC_KB / 2; ++ks) {
-              const uint64_t bd = tc::smem_desc(bbase + ks * 2 * LBO_B, LBO_B, SBO_B);
-              const uint64_t ad = tc::smem_desc(abase + t * S::A_TILE + ks * 2 * LBO_A, LBO_A, SBO_A);
-              tc::mma<Tr::KIND>(tmem + t * 2 * NC, ad, bd, id_full, (kc > 0 || ks > 0) ? 1u : 0u);
-              if constexpr (Tr::SPLIT) {
-                const uint64_t al = tc::smem_desc(abase + S::A_STAGE + t * S::A_TILE + ks * 2 * LBO_A, LBO_A, SBO_A);
-                tc::mma<Tr::KIND>(tmem + t * 2 * NC, al, bd, id_half, 1u);
-              }
-            }
+          for (int j = 0; j < 16; ++j) {
+            const uint32_t c = (uint32_t)(cg + 8 * j);
+            if (c < I2.ncol) asm volatile("prefetch.global.L1 [%0];" ::"l"(&a.cols[I2.col0 + c]));
           }
-          tc::mma_commit(&bars->empty[s]);
         }
-        if (ok) tc::mma_commit(&bars->acc_full);
       }
-      tc_mma_drain(bars, a.err);
+      w = w2;
+      I = I2;
     }
-  } else {
-    // ---------------- epilogue (warps 4-7: TMEM lanes 32 (warp - 4) ..) ----------------
-    const int ew = warp - 4;
-    uint32_t item = 0;
-    for (int64_t w = blockIdx.x; w < a.nitems; w += gridDim.x, ++item) {
-      const TcItem1 I = a.items[w];
-      if (!tc::mbar_wait(&bars->acc_full, item & 1u, TC_WAIT)) { tc_fail(a.err, bars, 8); break; }
+    tc::cp_async_wait_all();
+    if (pt == 0) tc_copies_drain(bars, it, C::S, a.err);
+  } else if (warp == 12) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) tc_mma_role<T, NC>(bars, sbase, tmem, a.nitems, nk_of, a.err);
+  } else if (warp < 8) {
+    // ---------------- converters (thread = TMEM lane m = tile row = factor column m) + drain ----------------
+    const int m = 32 * (warp & 3) + lane, h = warp >> 2;
+    const uint32_t lb = (uint32_t)(32 * (warp & 3)) << 16;
+    // drain of tile jj: Z slots of row m, accumulator columns [h NC / 2, h NC / 2 + NC / 2)
+    auto drain = [&](const TcItem1& J, uint32_t jj) -> bool {
+      const uint32_t q = jj & 1u;
+      const bool valid = (uint32_t)m < J.ncol;
+      TcCol1 Cc{};
+      if (valid) Cc = a.cols[J.col0 + m];
+      if (!tc_wait_warp(bars, &bars->accfull[q], (jj >> 1) & 1u, a.err, 8)) return false;
       tc::tc_fence_after();
-      const int ntile = (int)((I.ncol + 127) / 128);
-      for (int t = 0; t < ntile; ++t) {
-        const uint32_t row = (uint32_t)(t * 128 + 32 * ew + lane);
-        const bool valid = row < I.ncol;
-        TcCol1 C{};
-        if (valid) C = a.cols[I.col0 + row];
+#pragma unroll 1
+      for (int j0 = h * (NC / 2); j0 < (h + 1) * (NC / 2); j0 += 8) {
+        float d0[8], d1[8];
+        const uint32_t ta = tmem + lb + (uint32_t)(C::ACC0 + q * 2 * NC + j0);
+        tc::tmem_ld8(ta, d0);
+        tc::tmem_ld8(ta + NC, d1);
+        if (valid) {
+          float zz[8];
+          uint32_t zh[8], zl[8];
 #pragma unroll
-        for (int j0 = 0; j0 < NC; j0 += 16) {
-          float d0[16], d1[16];
-          const uint32_t ta = tmem + ((uint32_t)(32 * ew) << 16) + (uint32_t)(t * 2 * NC + j0);
-          tc::tmem_ld16(ta, d0);
-          tc::tmem_ld16(ta + NC, d1);
-          if (valid) {
-            for (uint32_t zi = C.zp0; zi < C.zp1; ++zi) {
-              const uint32_t zp = a.zpl[zi];
-              typename Tr::Bits* zb = a.zt + (int64_t)(zp / KE) * (2 * NC * KE) + (zp % KE);
+          for (int jj2 = 0; jj2 < 8; ++jj2) zz[jj2] = d0[jj2] + d1[jj2];
+          tc::split_n<Tr::SIG>(zz, zh, zl);
+          for (uint32_t zi = Cc.zp0; zi < Cc.zp1; ++zi) {
+            const uint32_t zp = a.zpl[zi];
+            typename Tr::Bits* zb = a.zt + (int64_t)(zp / KE) * (2 * NC * KE) + (zp % KE);
 #pragma unroll
-              for (int j = 0; j < 16; ++j) {
-                const float z = d0[j] + d1[j];
-                const float h = Tr::hi(z);
-                zb[(j0 + j) * KE] = Tr::bits(h);
-                zb[NC * KE + (j0 + j) * KE] = Tr::bits(Tr::hi(z - h));
-              }
+            for (int jj2 = 0; jj2 < 8; ++jj2) {
+              zb[(j0 + jj2) * KE] = (typename Tr::Bits)(zh[jj2] >> Tr::SHIFT);
+              zb[NC * KE + (j0 + jj2) * KE] = (typename Tr::Bits)(zl[jj2] >> Tr::SHIFT);
             }
           }
         }
       }
       tc::tc_fence_before();
-      tc::mbar_arrive(&bars->acc_empty);
+      tc::mbar_arrive(&bars->accempty[q]);
+      return true;
+    };
+    uint32_t it = 0, j = 0;
+    bool stop = false, pend = false;
+    TcItem1 Ip{};
+    TcItem1 I = blockIdx.x < a.nitems ? a.items[blockIdx.x] : TcItem1{};
+    for (int64_t w = blockIdx.x; w < a.nitems && !stop; w += gridDim.x, ++j) {
+      const TcItem1 I2 = w + gridDim.x < a.nitems ? a.items[w + gridDim.x] : TcItem1{};
+      const int nk = (int)((I.len + KC - 1) / KC);
+      const bool row = (uint32_t)m < I.ncol;
+      // the previous tile is drained after stage kd of this one: converting
+      // stage 1 needed the A buffer of the previous tile's last stage back, so
+      // by then its MMAs (and its accumulator) are complete
+      const int kd = nk > 1 ? 1 : 0;
+      for (int kc = 0; kc < nk; ++kc, ++it) {
+        const int s = (int)(it % C::S), ab = (int)(it % TC_NA);
+        if (!tc_wait_warp(bars, &bars->full[s], (it / C::S) & 1u, a.err, 64)) { stop = true; break; }
+        if (!tc_wait_warp(bars, &bars->aempty[ab], ((it / TC_NA) & 1u) ^ 1u, a.err, 64)) { stop = true; break; }
+        tc::tc_fence_after();
+        const uint8_t* raw = smem + s * C::STAGE + C::B_BYTES + m * C::RS1;
+        const int kl = row ? (int)min((int64_t)KC, (int64_t)I.len - (int64_t)kc * KC) : 0;
+        conv1(raw, kl, tmem + lb + (uint32_t)(ab * Tr::ACOLS), h, (T*)nullptr);
+        tc::tmem_wait_st();
+        tc::tc_fence_before();
+        tc::mbar_arrive(&bars->afull[ab]);
+        if (pend && kc == kd) {
+          pend = false;
+          if (!drain(Ip, j - 1)) { stop = true; break; }
+        }
+      }
+      Ip = I;
+      pend = !stop;
+      I = I2;
     }
+    if (pend) drain(Ip, j - 1);
   }
-  tc_teardown(bars, warp, tmem, S::TMEM_COLS);
+  tc_teardown(bars, warp, tmem);
 }
 
 // ---------------------------------------------------------------------------
 // phase 2
 // ---------------------------------------------------------------------------
-// Phase-2 A tiles are M-major (a factor column's rows are contiguous).  The
-// 16-byte chunk ci of a 128-row tile holds rows KE g .. KE g + KE - 1 of its K
-// column k; a2_chunk gives (g, k) and the chunk's byte offset in the tile.
-//  BF16 (KE 8): no swizzle, core matrices of 8 K x 16 bytes: (k / 8) 2048 +
-//    g 128 + (k % 8) 16; descriptor LBO = 2048 (along K), SBO = 128 (along M).
-//  TF32 (KE 4): M-major TF32 operands take the 128-byte swizzle with 32-byte
-//    atoms (descriptor layout 1): atoms of 32 rows (128 bytes) x 4 K rows
-//    whose 32-byte pieces are permuted by XOR with k % 4; the 4 row atoms
-//    512 bytes apart (LBO), groups of 4 K 2048 bytes apart (SBO).  Eight
-//    consecutive chunks fill one 128-byte atom row (no bank conflicts) and
-//    read 128 contiguous bytes of one factor column.
-template <int KE>
-__device__ __forceinline__ uint32_t a2_chunk(int ci, int& g, int& k) {
-  if constexpr (KE == 8) {
-    k = 8 * (ci / 128) + (ci % 8);
-    g = (ci / 8) % 16;
-    return (uint32_t)ci * 16u;
-  } else {
-    const int g8 = ci % 8;
-    k = (ci / 8) % 16;
-    g = (ci / 128) * 8 + g8;
-    return (uint32_t)((g / 8) * 512 + (k / 4) * 2048 + (k % 4) * 128 + ((((g % 8) >> 1) ^ (k % 4)) << 5) +
-                      (g & 1) * 16);
-  }
-}
-// descriptor of K step ks (32 bytes of K) of the phase-2 A tile at `tile`
-template <int KE>
-__device__ __forceinline__ uint64_t a2_desc(uint32_t tile, int ks) {
-  if constexpr (KE == 8) return tc::smem_desc(tile + ks * 2 * 2048, 2048, 128, 0);
-  else return tc::smem_desc(tile + ks * 2 * 2048, 512, 2048, 1);
-}
 template <typename T, int NC>
 struct P2Args {
   const TcItem2* items;
@@ -436,213 +581,202 @@ struct P2Args {
 template <typename T, int NC>
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> a) {
   using Tr = TcT<T>;
-  using S = TcSmem<T, NC>;
-  constexpr int KE = Tr::KE;
-  constexpr int KC = TC_KB * KE;                    // K values (Z slots) per stage
+  using C = TcCfg<T, NC>;
+  constexpr int KE = Tr::KE, KC = Tr::KC, ES = C::ES;
   extern __shared__ __align__(1024) uint8_t smem[];
-  TcBars* bars = reinterpret_cast<TcBars*>(smem + S::BAR_OFF);
+  TcBars* bars = reinterpret_cast<TcBars*>(smem + C::BAR_OFF);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t tmem = tc_setup(bars, warp, S::TMEM_COLS);
+  const uint32_t tmem = tc_setup(bars, warp, C::S, 128 + 4);   // cp.async arrivals + 4 slot-table arrivals
   const uint32_t sbase = tc::smem_u32(smem);
+  auto nk_of = [&](int64_t w) {
+    const TcItem2 I = a.items[w];
+    return (int)((I.ze - (I.zb / KE) * KE + KC - 1) / KC);
+  };
 
-  if (warp < 4) {
-    const int tid = threadIdx.x;
-    uint32_t it = 0, fin = 0;
-    auto finish = [&](uint32_t f) {
-      const int s = (int)(f % TC_STAGES);
-      if constexpr (Tr::SPLIT) {
-        // exactly the chunks this thread filled (cp.async.wait_group covers
-        // only this thread's own copies)
-#pragma unroll
-        for (int j = 0; j < TC_T * 4; ++j) {
-          int g, k;
-          const uint32_t off = (uint32_t)((j / 4) * S::A_TILE) + a2_chunk<KE>(tid + TC_PROD * (j % 4), g, k);
-          float4 v = *reinterpret_cast<const float4*>(smem + s * S::STAGE + off);
-          float4 h, l;
-          h.x = tc::tf32_rn(v.x); l.x = tc::tf32_rn(v.x - h.x);
-          h.y = tc::tf32_rn(v.y); l.y = tc::tf32_rn(v.y - h.y);
-          h.z = tc::tf32_rn(v.z); l.z = tc::tf32_rn(v.z - h.z);
-          h.w = tc::tf32_rn(v.w); l.w = tc::tf32_rn(v.w - h.w);
-          *reinterpret_cast<float4*>(smem + s * S::STAGE + off) = h;
-          *reinterpret_cast<float4*>(smem + s * S::STAGE + S::A_STAGE + off) = l;
-        }
-      }
-      tc::fence_proxy_async_smem();
-      tc::mbar_arrive(&bars->full[s]);
+  if (warp >= 8 && warp < 12) {
+    // ---------------- producers: the Z tile (one bulk copy) and each slot's rows of the tile ----------------
+    // warp pw handles slots SPW pw .. SPW pw + SPW - 1 of a stage; lane i
+    // (< SPW) holds slot SPW pw + i's descriptor, loaded one stage ahead; per
+    // slot the warp copies the rows lane by lane (16 bytes a lane) and lane 0
+    // writes the slot table entry
+    constexpr int SPW = KC / 4;
+    static_assert(SPW <= 32, "one descriptor per lane");
+    const int pw = warp - 8;
+    uint32_t it = 0;
+    auto load_desc = [&](const TcItem2& J, int kc) {
+      const int64_t zp = (int64_t)(J.zb / KE) * KE + (int64_t)kc * KC + SPW * pw + (lane % SPW);
+      return (lane < SPW && zp >= (int64_t)J.zb && zp < (int64_t)J.ze) ? a.z2[zp] : TcZ2{0, 0, 0};
     };
-    for (int64_t w = blockIdx.x; w < a.nitems; w += gridDim.x) {
-      const TcItem2 I = a.items[w];
-      const int64_t zc0 = (int64_t)(I.zb / KE) * KE;
-      const int nk = (int)((I.ze - zc0 + KC - 1) / KC);
-      for (int kc = 0; kc < nk; ++kc, ++it) {
-        const int s = (int)(it % TC_STAGES);
-        const uint32_t ph = (it / TC_STAGES) & 1u;
-        if (!tc::mbar_wait(&bars->empty[s], ph ^ 1u, TC_WAIT)) { tc_fail(a.err, bars, 1); break; }
-        if (tc_aborted(bars)) break;
-        const uint32_t abase = sbase + s * S::STAGE;
-        const int64_t zc = zc0 + (int64_t)kc * KC;
-        if (tid == 0) {
-          tc::mbar_arrive_expect_tx(&bars->full[s], S::B_STAGE);
-          tc::bulk_g2s(abase + S::A_STAGE + S::A_LO, a.zt + (zc / KE) * (2 * NC * KE), S::B_STAGE, &bars->full[s]);
-        }
-        // chunk ci = tid + 128 (j % 4) of tile j / 4: rows KE g.. of K column k
-        int64_t zcur = -1;
-        TcZ2 Z{};
-#pragma unroll
-        for (int j = 0; j < TC_T * 4; ++j) {
-          const int t = j / 4;
-          const int ci = tid + TC_PROD * (j % 4);
-          int g, k;
-          const uint32_t coff = a2_chunk<KE>(ci, g, k);
-          const int64_t zp = zc + k;
-          uint8_t* dsm = smem + s * S::STAGE + t * S::A_TILE + coff;
-          const uint32_t dst = abase + (uint32_t)(t * S::A_TILE) + coff;
-          if (zp < (int64_t)I.zb || zp >= (int64_t)I.ze) {
-            *reinterpret_cast<uint4*>(dsm) = make_uint4(0u, 0u, 0u, 0u);
-            continue;
-          }
-          if (zp != zcur) { Z = a.z2[zp]; zcur = zp; }
-          const int i0 = t * 128 + g * KE;               // first window row of the chunk
-          const int64_t so = Z.a_off + (i0 - Z.rlo);     // source element of row i0
-          if (i0 >= Z.rlo && i0 + KE <= Z.rhi && (so % KE) == 0) {
-            tc::cp_async16(dst, a.pool + so, 16u);
-          } else if (i0 + KE <= Z.rlo || i0 >= Z.rhi) {
-            *reinterpret_cast<uint4*>(dsm) = make_uint4(0u, 0u, 0u, 0u);
-          } else {
-            // a partly covered or unaligned row group: element by element
-            union { typename Tr::Bits e[KE]; uint4 u; } v;
-#pragma unroll
-            for (int e = 0; e < KE; ++e) {
-              const int i = i0 + e;
-              v.e[e] = 0;
-              if (i >= Z.rlo && i < Z.rhi)
-                v.e[e] = *reinterpret_cast<const typename Tr::Bits*>(a.pool + Z.a_off + (i - Z.rlo));
-            }
-            *reinterpret_cast<uint4*>(dsm) = v.u;
-          }
-        }
-        tc::cp_async_commit();
-        if (it >= TC_STAGES - 1) {
-          tc::cp_async_wait<TC_STAGES - 1>();
-          finish(fin++);
-        }
+    int64_t w = blockIdx.x;
+    TcItem2 I = w < a.nitems ? a.items[w] : TcItem2{};
+    int nk = w < a.nitems ? nk_of(w) : 0;
+    TcItem2 In = w + gridDim.x < a.nitems ? a.items[w + gridDim.x] : TcItem2{};
+    TcZ2 cur = w < a.nitems ? load_desc(I, 0) : TcZ2{0, 0, 0};
+    int kc = 0;
+    while (w < a.nitems) {
+      // the next stage's cursor and descriptors
+      int64_t w2 = w;
+      int kc2 = kc + 1, nk2 = nk;
+      TcItem2 I2 = I;
+      if (kc2 == nk) {
+        w2 = w + gridDim.x;
+        kc2 = 0;
+        I2 = In;
+        nk2 = w2 < a.nitems ? (int)((I2.ze - (I2.zb / KE) * KE + KC - 1) / KC) : 0;
       }
-      if (tc_aborted(bars)) break;
-    }
-    tc::cp_async_wait<0>();
-    while (fin < it) finish(fin++);
-  } else if (warp == 8) {
-    if (lane == 0) {
-      constexpr uint32_t LBO_B = 2 * NC * 16, SBO_B = 128;
-      const uint32_t id_full = tc::idesc(Tr::FMT, 2 * NC, 1, 0);
-      const uint32_t id_half = tc::idesc(Tr::FMT, NC, 1, 0);
-      uint32_t it = 0, item = 0;
-      bool ok = true;
-      for (int64_t w = blockIdx.x; w < a.nitems && ok; w += gridDim.x, ++item) {
-        const TcItem2 I = a.items[w];
-        const int64_t zc0 = (int64_t)(I.zb / KE) * KE;
-        const int nk = (int)((I.ze - zc0 + KC - 1) / KC);
-        const int ntile = (int)((I.nrows + 127) / 128);
-        if (!tc::mbar_wait(&bars->acc_empty, (item & 1u) ^ 1u, TC_WAIT)) { tc_fail(a.err, bars, 2); ok = false; break; }
-        tc::tc_fence_after();
-        for (int kc = 0; kc < nk; ++kc, ++it) {
-          const int s = (int)(it % TC_STAGES);
-          const uint32_t ph = (it / TC_STAGES) & 1u;
-          if (!tc::mbar_wait(&bars->full[s], ph, TC_WAIT)) { tc_fail(a.err, bars, 4); ok = false; break; }
-          tc::tc_fence_after();
-          const uint32_t abase = sbase + s * S::STAGE;
-          const uint32_t bbase = abase + S::A_STAGE + S::A_LO;
-          for (int t = 0; t < ntile; ++t) {
-#pragma unroll
-            for (int ks = 0; ks < TC_KB / 2; ++ks) {
-              const uint64_t bd = tc::smem_desc(bbase + ks * 2 * LBO_B, LBO_B, SBO_B);
-              const uint64_t ad = a2_desc<KE>(abase + t * S::A_TILE, ks);
-              tc::mma<Tr::KIND>(tmem + t * 2 * NC, ad, bd, id_full, (kc > 0 || ks > 0) ? 1u : 0u);
-              if constexpr (Tr::SPLIT) {
-                const uint64_t al = a2_desc<KE>(abase + S::A_STAGE + t * S::A_TILE, ks);
-                tc::mma<Tr::KIND>(tmem + t * 2 * NC, al, bd, id_half, 1u);
-              }
-            }
-          }
-          tc::mma_commit(&bars->empty[s]);
-        }
-        if (ok) tc::mma_commit(&bars->acc_full);
+      const TcZ2 nxt = w2 < a.nitems ? load_desc(I2, kc2) : TcZ2{0, 0, 0};
+      // this stage
+      const int s = (int)(it % C::S);
+      if (!tc_wait_warp(bars, &bars->empty[s], ((it / C::S) & 1u) ^ 1u, a.err, 1)) break;
+      const uint32_t st = sbase + (uint32_t)(s * C::STAGE);
+      int4* meta = reinterpret_cast<int4*>(smem + s * C::STAGE + C::B_BYTES + C::RAW2);
+      const int64_t zc = (int64_t)(I.zb / KE) * KE + (int64_t)kc * KC;
+      if (pw == 0 && lane == 0) {
+        tc::mbar_arrive_expect_tx(&bars->bfull[s], (uint32_t)C::B_BYTES);
+        tc::bulk_g2s(st, a.zt + (zc / KE) * (2 * NC * KE), C::B_BYTES, &bars->bfull[s]);
       }
-      tc_mma_drain(bars, a.err);
+      // lane i (< SPW): slot SPW pw + i's copy and table entry
+      const int toff = (int)I.toff;
+      int64_t src = 0;
+      uint32_t dsto = 0, nb = 0;
+      if (lane < SPW) {
+        const int k = SPW * pw + lane;
+        const int r0 = max(cur.rlo, toff), r1 = min(cur.rhi, toff + 128);
+        int4 md = make_int4(0, 0, 0, 0);
+        if (r0 < r1) {
+          // element offset of window row i: g(i) = a_off + i - rlo; the raw row
+          // holds g(toff) - sh .. in 16-byte units (sh = g(toff) mod KE)
+          const int64_t gt = cur.a_off + (toff - cur.rlo);
+          const int shl = (int)(gt & (KE - 1));                 // KE is a power of two
+          const int64_t g0 = cur.a_off + (r0 - cur.rlo), g1 = cur.a_off + (r1 - cur.rlo);
+          const int64_t slo = g0 & ~(int64_t)(KE - 1);
+          const int64_t shi = (g1 + KE - 1) & ~(int64_t)(KE - 1);
+          src = slo;
+          dsto = (uint32_t)(C::B_BYTES + k * C::RS2 + (slo - (gt - shl)) * ES);
+          nb = (uint32_t)((shi - slo) * ES);
+          md = make_int4(r0 - toff, r1 - toff, k * (C::RS2 / ES) + shl, 0);
+        }
+        meta[k] = md;
+      }
+      // the copies, slot by slot, 16 bytes a lane (whole 128-byte lines per instruction)
+#pragma unroll 4
+      for (int i = 0; i < SPW; ++i) {
+        const uint32_t nbi = __shfl_sync(0xffffffffu, nb, i);
+        const int64_t srci = (int64_t)__shfl_sync(0xffffffffu, (long long)src, i);
+        const uint32_t dsti = __shfl_sync(0xffffffffu, dsto, i);
+        if ((uint32_t)lane * 16u < nbi) tc::cp_async16(st + dsti + lane * 16, a.pool + srci + lane * KE, 16u);
+        if (lane == 0 && nbi > 512u) tc::cp_async16(st + dsti + 512, a.pool + srci + 32 * KE, 16u);
+      }
+      __threadfence_block();                                  // the table entries before lane 0's release
+      __syncwarp();
+      tc::cp_async_mbar_arrive(&bars->full[s]);
+      if (lane == 0) tc::mbar_arrive(&bars->full[s]);        // the slot table (release)
+      ++it;
+      if (w2 != w) In = w2 + gridDim.x < a.nitems ? a.items[w2 + gridDim.x] : TcItem2{};
+      w = w2;
+      kc = kc2;
+      nk = nk2;
+      I = I2;
+      cur = nxt;
     }
-  } else {
-    const int ew = warp - 4;
-    uint32_t item = 0;
-    for (int64_t w = blockIdx.x; w < a.nitems; w += gridDim.x, ++item) {
-      const TcItem2 I = a.items[w];
-      if (!tc::mbar_wait(&bars->acc_full, item & 1u, TC_WAIT)) { tc_fail(a.err, bars, 8); break; }
+    tc::cp_async_wait_all();
+    if (pw == 0 && lane == 0) tc_copies_drain(bars, it, C::S, a.err);
+  } else if (warp == 12) {
+    if (lane == 0) tc_mma_role<T, NC>(bars, sbase, tmem, a.nitems, nk_of, a.err);
+  } else if (warp < 8) {
+    // ---------------- converters (thread = TMEM lane m = tile row m) + drain ----------------
+    const int m = 32 * (warp & 3) + lane, h = warp >> 2;
+    const uint32_t lb = (uint32_t)(32 * (warp & 3)) << 16;
+    // drain of tile jj: Y rows of the tile += accumulator columns of half h
+    auto drain = [&](const TcItem2& J, uint32_t jj) -> bool {
+      const uint32_t q = jj & 1u;
+      if (!tc_wait_warp(bars, &bars->accfull[q], (jj >> 1) & 1u, a.err, 8)) return false;
       tc::tc_fence_after();
-      const int ntile = (int)((I.nrows + 127) / 128);
-      for (int t = 0; t < ntile; ++t) {
-        const uint32_t row = (uint32_t)(t * 128 + 32 * ew + lane);
-        const bool valid = row < I.nrows;
-        double* yr = a.Y + (int64_t)I.row0 + row;
+      const bool valid = (uint32_t)m < J.nrows;
+      double* yr = a.Y + (int64_t)J.row0 + m;
+#pragma unroll 1
+      for (int j0 = h * (NC / 2); j0 < (h + 1) * (NC / 2); j0 += 8) {
+        float d0[8], d1[8];
+        const uint32_t ta = tmem + lb + (uint32_t)(C::ACC0 + q * 2 * NC + j0);
+        tc::tmem_ld8(ta, d0);
+        tc::tmem_ld8(ta + NC, d1);
+        if (valid) {
 #pragma unroll
-        for (int j0 = 0; j0 < NC; j0 += 16) {
-          float d0[16], d1[16];
-          const uint32_t ta = tmem + ((uint32_t)(32 * ew) << 16) + (uint32_t)(t * 2 * NC + j0);
-          tc::tmem_ld16(ta, d0);
-          tc::tmem_ld16(ta + NC, d1);
-          if (valid) {
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              const int col = a.cb * NC + j0 + j;
-              if (col < a.ncols) yr[(int64_t)col * a.ldy] += (double)(d0[j] + d1[j]);
-            }
+          for (int jj2 = 0; jj2 < 8; ++jj2) {
+            const int col = a.cb * NC + j0 + jj2;
+            if (col < a.ncols) yr[(int64_t)col * a.ldy] += (double)(d0[jj2] + d1[jj2]);
           }
         }
       }
       tc::tc_fence_before();
-      tc::mbar_arrive(&bars->acc_empty);
+      tc::mbar_arrive(&bars->accempty[q]);
+      return true;
+    };
+    uint32_t it = 0, j = 0;
+    bool stop = false, pend = false;
+    TcItem2 Ip{};
+    TcItem2 I = blockIdx.x < a.nitems ? a.items[blockIdx.x] : TcItem2{};
+    for (int64_t w = blockIdx.x; w < a.nitems && !stop; w += gridDim.x, ++j) {
+      const TcItem2 I2 = w + gridDim.x < a.nitems ? a.items[w + gridDim.x] : TcItem2{};
+      const int nk = (int)((I.ze - (I.zb / KE) * KE + KC - 1) / KC);
+      const int kd = nk > 1 ? 1 : 0;                 // as in phase 1
+      for (int kc = 0; kc < nk; ++kc, ++it) {
+        const int s = (int)(it % C::S), ab = (int)(it % TC_NA);
+        if (!tc_wait_warp(bars, &bars->full[s], (it / C::S) & 1u, a.err, 64)) { stop = true; break; }
+        if (!tc_wait_warp(bars, &bars->aempty[ab], ((it / TC_NA) & 1u) ^ 1u, a.err, 64)) { stop = true; break; }
+        tc::tc_fence_after();
+        const uint8_t* rb = smem + s * C::STAGE + C::B_BYTES;
+        conv2(rb, reinterpret_cast<const int4*>(rb + C::RAW2), m, tmem + lb + (uint32_t)(ab * Tr::ACOLS), h,
+              (T*)nullptr);
+        tc::tmem_wait_st();
+        tc::tc_fence_before();
+        tc::mbar_arrive(&bars->afull[ab]);
+        if (pend && kc == kd) {
+          pend = false;
+          if (!drain(Ip, j - 1)) { stop = true; break; }
+        }
+      }
+      Ip = I;
+      pend = !stop;
+      I = I2;
     }
+    if (pend) drain(Ip, j - 1);
   }
-  tc_teardown(bars, warp, tmem, S::TMEM_COLS);
+  tc_teardown(bars, warp, tmem);
 }
 
 // ---------------------------------------------------------------------------
 // Self-test of the operand layouts and descriptors used above: one 128 x 2NC
-// accumulator D = A B' over one pipeline stage's K, with A staged exactly as
-// phase 1 (K-major) or phase 2 (M-major) stage it and B as the X / Z tiles.
-// The tiles sit at the start of a 200 KB shared allocation (A at 0, B at
-// 96 KB), far inside it, so every address the descriptors can produce stays
-// in the allocation.
+// accumulator D = A B' over K = 2 MMAs, with B staged as the X / Z tiles and
+// A either as a K-major shared-memory tile (a_src 0) or in tensor memory as
+// the converters write it (a_src 2).  The tiles sit at the start of a 200 KB
+// shared allocation (A at 0, B at 96 KB), far inside it, so every address
+// the descriptors can produce stays in the allocation.
 // ---------------------------------------------------------------------------
 constexpr int SELF_SMEM = 200 * 1024;
 constexpr int SELF_B_OFF = 96 * 1024;
+constexpr int SELF_KB = 4;             // 16-byte K blocks of the test (two MMAs)
 
-template <typename T, int NC, bool A_MN>
+template <typename T, int NC, bool A_TMEM>
 __global__ void __launch_bounds__(128, 1) tc_selftest_kernel(const float* __restrict__ A, const float* __restrict__ B,
                                                            float* __restrict__ D, int* __restrict__ err) {
   using Tr = TcT<T>;
   constexpr int KE = Tr::KE;
-  constexpr int KC = TC_KB * KE;
+  constexpr int KC = SELF_KB * KE;
+  constexpr int DCOL = 128;            // accumulator columns [128, 128 + 2NC)
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t bar;
   __shared__ uint32_t tslot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   typename Tr::Bits* sa = reinterpret_cast<typename Tr::Bits*>(smem);
   typename Tr::Bits* sb = reinterpret_cast<typename Tr::Bits*>(smem + SELF_B_OFF);
-  // A (128 x KC, row-major input) in the tile layout of the kernels
-  for (int e = tid; e < 128 * KC; e += 128) {
-    const int i = e / KC, k = e % KC;
-    int off;                                           // element offset in the tile
-    if (!A_MN) {
-      // phase 1: row i, K block b: (i / 8) * KB * 128 + b * 128 + (i % 8) * 16 bytes
-      off = ((i / 8) * TC_KB * 128 + (k / KE) * 128 + (i % 8) * 16) / (int)sizeof(T) + k % KE;
-    } else {
-      // phase 2: the chunk of rows KE g .. of column k, laid out by a2_chunk
-      int ci = 0;
-      if (KE == 8) ci = (k / 8) * 128 + ((i / KE) % 16) * 8 + (k % 8);
-      else ci = ((i / KE) / 8) * 128 + (k % 16) * 8 + (i / KE) % 8;
-      int gg, kk;
-      off = (int)(a2_chunk<KE>(ci, gg, kk) / sizeof(T)) + i % KE;
+  if (!A_TMEM) {
+    // A (128 x KC, row-major input): row i, K block b at (i / 8) KB 128 + b 128 + (i % 8) 16 bytes
+    for (int e = tid; e < 128 * KC; e += 128) {
+      const int i = e / KC, k = e % KC;
+      const int off = ((i / 8) * SELF_KB * 128 + (k / KE) * 128 + (i % 8) * 16) / (int)sizeof(T) + k % KE;
+      sa[off] = Tr::bits(A[e]);
     }
-    sa[off] = Tr::bits(A[e]);
   }
   // B (2NC x KC, row-major input) as XT / ZT blocks: [b][n][e]
   for (int e = tid; e < 2 * NC * KC; e += 128) {
@@ -654,22 +788,42 @@ __global__ void __launch_bounds__(128, 1) tc_selftest_kernel(const float* __rest
     tc::fence_mbar_init();
   }
   tc::fence_proxy_async_smem();
-  if (warp == 0) tc::tmem_alloc(&tslot, 2 * NC < 32 ? 32 : 2 * NC);
+  if (warp == 0) tc::tmem_alloc(&tslot, 256);
   tc::tc_fence_before();
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = tslot;
+  const uint32_t lb = (uint32_t)(32 * warp) << 16;
+  if (A_TMEM) {
+    // row tid of A into TMEM lane tid, columns [0, KC) (TF32) or [0, KC / 2) (BF16 pairs)
+    uint32_t r[16];
+    if (Tr::SPLIT) {
+#pragma unroll
+      for (int c = 0; c < 16; ++c) r[c] = __float_as_uint(A[tid * KC + c]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 16; ++c)
+        r[c] = (uint32_t)Tr::bits(A[tid * KC + 2 * c]) | ((uint32_t)Tr::bits(A[tid * KC + 2 * c + 1]) << 16);
+    }
+    tc::tmem_st16(tmem + lb, r);
+    tc::tmem_wait_st();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
   if (tid == 0) {
     const uint32_t abase = tc::smem_u32(smem), bbase = tc::smem_u32(smem + SELF_B_OFF);
     constexpr uint32_t LBO_B = 2 * NC * 16, SBO_B = 128;
-    const uint32_t id = tc::idesc(Tr::FMT, 2 * NC, A_MN ? 1 : 0, 0);
+    const uint32_t id = tc::idesc(Tr::FMT, 2 * NC, 0, 0);
 #pragma unroll
-    for (int ks = 0; ks < TC_KB / 2; ++ks) {
+    for (int ks = 0; ks < SELF_KB / 2; ++ks) {
       const uint64_t bd = tc::smem_desc(bbase + ks * 2 * LBO_B, LBO_B, SBO_B);
-      uint64_t ad;
-      if (!A_MN) ad = tc::smem_desc(abase + ks * 2 * 128, 128, TC_KB * 128);
-      else ad = a2_desc<KE>(abase, ks);
-      tc::mma<Tr::KIND>(tmem, ad, bd, id, ks > 0 ? 1u : 0u);
+      if (A_TMEM) {
+        tc::mma_ts<Tr::KIND>(tmem + DCOL, tmem + ks * 8, bd, id, ks > 0 ? 1u : 0u);
+      } else {
+        const uint64_t ad = tc::smem_desc(abase + ks * 2 * 128, 128, SELF_KB * 128);
+        tc::mma<Tr::KIND>(tmem + DCOL, ad, bd, id, ks > 0 ? 1u : 0u);
+      }
     }
     tc::mma_commit(&bar);
   }
@@ -678,7 +832,7 @@ __global__ void __launch_bounds__(128, 1) tc_selftest_kernel(const float* __rest
   tc::tc_fence_after();
   for (int j0 = 0; j0 < 2 * NC; j0 += 16) {
     float d[16];
-    tc::tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)j0, d);
+    tc::tmem_ld16(tmem + lb + (uint32_t)(DCOL + j0), d);
 #pragma unroll
     for (int j = 0; j < 16; ++j) D[(32 * warp + lane) * 2 * NC + j0 + j] = d[j];
   }
@@ -686,13 +840,13 @@ __global__ void __launch_bounds__(128, 1) tc_selftest_kernel(const float* __rest
   __syncthreads();
   if (warp == 0) {
     tc::tc_fence_after();
-    tc::tmem_dealloc(tmem, 2 * NC < 32 ? 32 : 2 * NC);
+    tc::tmem_dealloc(tmem, 256);
   }
 }
 
-template <typename T, int NC, bool A_MN>
+template <typename T, int NC, bool A_TMEM>
 int run_selftest(const float* A, const float* B, float* D) {
-  constexpr int KC = TC_KB * TcT<T>::KE;
+  constexpr int KC = SELF_KB * TcT<T>::KE;
   float *dA = nullptr, *dB = nullptr, *dD = nullptr;
   int* dE = nullptr;
   struct Guard {
@@ -706,8 +860,8 @@ int run_selftest(const float* A, const float* B, float* D) {
   HM_CUDA_TRY(cudaMemset(dE, 0, sizeof(int)));
   HM_CUDA_TRY(cudaMemcpy(dA, A, sizeof(float) * 128 * KC, cudaMemcpyHostToDevice));
   HM_CUDA_TRY(cudaMemcpy(dB, B, sizeof(float) * 2 * NC * KC, cudaMemcpyHostToDevice));
-  HM_CUDA_TRY(smem_attr((const void*)tc_selftest_kernel<T, NC, A_MN>, SELF_SMEM));
-  tc_selftest_kernel<T, NC, A_MN><<<1, 128, SELF_SMEM>>>(dA, dB, dD, dE);
+  HM_CUDA_TRY(smem_attr((const void*)tc_selftest_kernel<T, NC, A_TMEM>, SELF_SMEM));
+  tc_selftest_kernel<T, NC, A_TMEM><<<1, 128, SELF_SMEM>>>(dA, dB, dD, dE);
   HM_CUDA_TRY(cudaGetLastError());
   HM_CUDA_TRY(cudaDeviceSynchronize());
   int e = 0;
@@ -719,15 +873,17 @@ int run_selftest(const float* A, const float* B, float* D) {
 
 }  // namespace
 
-int tc_selftest(int kind, int a_mn, int nc, const float* A, const float* B, float* D) {
+int tc_selftest(int kind, int a_src, int nc, const float* A, const float* B, float* D) {
+  if (a_src != 0 && a_src != 2) return fail(HM_ERR_ARG, "self-test: a_src 0 (shared memory) or 2 (tensor memory)");
+  const bool tm = a_src == 2;
   if (kind == 0) {
-    if (nc == 16) return a_mn ? run_selftest<float, 16, true>(A, B, D) : run_selftest<float, 16, false>(A, B, D);
-    if (nc == 64) return a_mn ? run_selftest<float, 64, true>(A, B, D) : run_selftest<float, 64, false>(A, B, D);
-  } else {
+    if (nc == 16) return tm ? run_selftest<float, 16, true>(A, B, D) : run_selftest<float, 16, false>(A, B, D);
+    if (nc == 64) return tm ? run_selftest<float, 64, true>(A, B, D) : run_selftest<float, 64, false>(A, B, D);
+  } else if (kind == 1) {
     if (nc == 16)
-      return a_mn ? run_selftest<__nv_bfloat16, 16, true>(A, B, D) : run_selftest<__nv_bfloat16, 16, false>(A, B, D);
+      return tm ? run_selftest<__nv_bfloat16, 16, true>(A, B, D) : run_selftest<__nv_bfloat16, 16, false>(A, B, D);
     if (nc == 64)
-      return a_mn ? run_selftest<__nv_bfloat16, 64, true>(A, B, D) : run_selftest<__nv_bfloat16, 64, false>(A, B, D);
+      return tm ? run_selftest<__nv_bfloat16, 64, true>(A, B, D) : run_selftest<__nv_bfloat16, 64, false>(A, B, D);
   }
   return fail(HM_ERR_ARG, "self-test: kind 0 (tf32) or 1 (bf16), nc 16 or 64");
 }
@@ -759,8 +915,7 @@ static int upload_vec(V** d, const std::vector<V>& v) {
 static int build_tc_plan(hm_handle* h, int trans, TcPlan** out) {
   const int eb = elem_bytes(h->storage);
   struct Lf { int64_t li; int64_t zoff; };
-  // low-rank leaves in pool order with their z offsets (the order of the
-  // CUDA-core plans: leaves sorted by row group)
+  // low-rank leaves in pool order with their z offsets
   std::vector<int64_t> order(h->leaves.size());
   for (size_t i = 0; i < order.size(); ++i) order[i] = (int64_t)i;
   std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
@@ -776,7 +931,8 @@ static int build_tc_plan(hm_handle* h, int trans, TcPlan** out) {
   }
   const int64_t zlen = z;
   TcPlan* P = new TcPlan();
-  // ---- phase 2: windows of TC_WR output rows; Z slots window by window
+  // ---- phase 2: windows of TC_WR output rows; Z slots window by window,
+  // items = the 128-row tiles of a window that some slot covers
   const int64_t n = h->n;
   const int64_t nwin = (n + TC_WR - 1) / TC_WR;
   std::vector<std::vector<int32_t>> per(nwin);      // rk indices touching each window
@@ -797,15 +953,15 @@ static int build_tc_plan(hm_handle* h, int trans, TcPlan** out) {
   std::vector<uint32_t> zpl(zp_count[zlen]), fillpos(zp_count.begin(), zp_count.end() - 1);
   for (int64_t w = 0; w < nwin; ++w) {
     if (per[w].empty()) continue;
-    TcItem2 I{};
-    I.row0 = (uint32_t)(w * TC_WR);
-    I.nrows = (uint32_t)std::min<int64_t>(TC_WR, n - w * TC_WR);
-    I.zb = (uint32_t)z2.size();
+    const uint32_t zb = (uint32_t)z2.size();
+    const int64_t wrows = std::min<int64_t>(TC_WR, n - w * TC_WR);
+    bool tile_used[TC_WR / 128] = {false, false, false, false};
     for (int32_t i : per[w]) {
       const Leaf& L = h->leaves[rk[i].li];
       const int64_t npad = col_pad(L.n, eb), mpad = col_pad(L.m, eb);
       const int64_t o0 = trans ? L.col0 : L.row0, o1 = o0 + (trans ? L.n : L.m);
       const int64_t lo = std::max<int64_t>(o0, w * TC_WR), hi = std::min<int64_t>(o1, (w + 1) * TC_WR);
+      for (int64_t t = (lo - w * TC_WR) / 128; t * 128 < hi - w * TC_WR; ++t) tile_used[t] = true;
       for (int r = 0; r < L.k; ++r) {
         // F2: A (m x k, stride mpad) for H*x, B (n x k, stride npad) for H'*x
         const int64_t col = trans ? L.off + (int64_t)r * npad : L.off + npad * L.k + (int64_t)r * mpad;
@@ -813,17 +969,25 @@ static int build_tc_plan(hm_handle* h, int trans, TcPlan** out) {
         Z.a_off = col + (lo - o0);
         Z.rlo = (int32_t)(lo - w * TC_WR);
         Z.rhi = (int32_t)(hi - w * TC_WR);
-        if ((o0 % (16 / eb)) != 0) P->aligned = false;
         zpl[fillpos[rk[i].zoff + r]++] = (uint32_t)z2.size();
         z2.push_back(Z);
       }
     }
-    I.ze = (uint32_t)z2.size();
-    it2.push_back(I);
+    const uint32_t ze = (uint32_t)z2.size();
+    for (int t = 0; t < TC_WR / 128 && t * 128 < wrows; ++t) {
+      if (!tile_used[t]) continue;
+      TcItem2 I{};
+      I.row0 = (uint32_t)(w * TC_WR + t * 128);
+      I.nrows = (uint32_t)std::min<int64_t>(128, wrows - t * 128);
+      I.zb = zb;
+      I.ze = ze;
+      I.toff = (uint32_t)(t * 128);
+      it2.push_back(I);
+    }
     std::vector<int32_t>().swap(per[w]);
   }
   if (z2.size() > (size_t)UINT32_MAX / 2) { delete P; return fail(HM_ERR_UNSUPPORTED, "too many low-rank terms for the tensor-core plan"); }
-  // ---- phase 1: factor columns of F1 grouped by input segment
+  // ---- phase 1: factor columns of F1 grouped by input segment, 128 per tile
   std::vector<int32_t> ord1(rk.size());
   for (size_t i = 0; i < rk.size(); ++i) ord1[i] = (int32_t)i;
   auto seg = [&](int32_t i) {
@@ -841,22 +1005,22 @@ static int build_tc_plan(hm_handle* h, int trans, TcPlan** out) {
       const Leaf& L = h->leaves[rk[ord1[j]].li];
       const int64_t npad = col_pad(L.n, eb), mpad = col_pad(L.m, eb);
       for (int r = 0; r < L.k; ++r) {
-        TcCol1 C{};
-        C.off = trans ? (uint64_t)(L.off + npad * L.k + (int64_t)r * mpad) : (uint64_t)(L.off + (int64_t)r * npad);
-        C.zp0 = zp_count[rk[ord1[j]].zoff + r];
-        C.zp1 = zp_count[rk[ord1[j]].zoff + r + 1];
-        col1.push_back(C);
+        TcCol1 Cc{};
+        Cc.off = trans ? (uint64_t)(L.off + npad * L.k + (int64_t)r * mpad) : (uint64_t)(L.off + (int64_t)r * npad);
+        Cc.zp0 = zp_count[rk[ord1[j]].zoff + r];
+        Cc.zp1 = zp_count[rk[ord1[j]].zoff + r + 1];
+        col1.push_back(Cc);
       }
       ++j;
     }
     const uint32_t c1 = (uint32_t)col1.size();
-    for (uint32_t c = c0; c < c1; c += 128 * TC_T) {
+    for (uint32_t c = c0; c < c1; c += 128) {
       TcItem1 I{};
       I.col0 = c;
-      I.ncol = std::min<uint32_t>(128 * TC_T, c1 - c);
+      I.ncol = std::min<uint32_t>(128, c1 - c);
       I.seg0 = (uint32_t)sg.first;
       I.len = (uint32_t)sg.second;
-      it1.push_back(I);
+      if (I.len > 0) it1.push_back(I);
     }
     i = j;
   }
@@ -882,15 +1046,15 @@ static int build_tc_plan(hm_handle* h, int trans, TcPlan** out) {
 template <typename T, int NC>
 static int launch_tc(hm_handle* h, TcPlan& P, const double* d_x, double* d_y, int64_t ncols, cudaStream_t st) {
   using Bits = typename TcT<T>::Bits;
-  using S = TcSmem<T, NC>;
-  constexpr int KE = TcT<T>::KE;
+  using C = TcCfg<T, NC>;
+  constexpr int KE = TcT<T>::KE, KC = TcT<T>::KC;
   const int64_t n = h->n;
-  const int64_t nkb = (n + 2 * KE) / KE + TC_KB + 2;            // XT blocks per shifted copy
+  const int64_t nkb = (n + KE + KC) / KE + 2;                   // XT blocks per shifted copy
   const int64_t xt_copy = nkb * 2 * NC * KE;
-  const int64_t zkb = (P.nz2 + KE - 1) / KE + TC_KB + 2;        // Z blocks (with zero padding)
+  const int64_t zkb = (P.nz2 + KC) / KE + 2;                    // Z blocks (with zero padding)
   const size_t xt_bytes = sizeof(Bits) * (size_t)(KE * xt_copy);
   const size_t zt_bytes = sizeof(Bits) * (size_t)(zkb * 2 * NC * KE);
-  const size_t need = xt_bytes + zt_bytes + 256;
+  const size_t need = (xt_bytes + 255) / 256 * 256 + zt_bytes;
   if (h->tc_bytes < need) {
     if (h->d_tc) cudaFree(h->d_tc);
     h->d_tc = nullptr;
@@ -904,12 +1068,12 @@ static int launch_tc(hm_handle* h, TcPlan& P, const double* d_x, double* d_y, in
     HM_CUDA_TRY(cudaMemsetAsync(h->d_tc_err, 0, sizeof(int), st));
   }
   Bits* xt = (Bits*)h->d_tc;
-  Bits* zt = (Bits*)((char*)h->d_tc + ((xt_bytes + 255) / 256) * 256);
+  Bits* zt = (Bits*)((char*)h->d_tc + (xt_bytes + 255) / 256 * 256);
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
-  HM_CUDA_TRY(smem_attr((const void*)tc_phase1_kernel<T, NC>, S::BYTES));
-  HM_CUDA_TRY(smem_attr((const void*)tc_phase2_kernel<T, NC>, S::BYTES));
-  // Z padding past the last slot stays zero (its A columns are zero too, and
+  HM_CUDA_TRY(smem_attr((const void*)tc_phase1_kernel<T, NC>, C::BYTES));
+  HM_CUDA_TRY(smem_attr((const void*)tc_phase2_kernel<T, NC>, C::BYTES));
+  // Z padding past the last slot stays zero (its A rows are zero too, and
   // 0 * garbage could be NaN)
   {
     const int64_t z0 = (P.nz2 / KE) * (2 * NC * KE);
@@ -923,11 +1087,11 @@ static int launch_tc(hm_handle* h, TcPlan& P, const double* d_x, double* d_y, in
         d_x, n, n, (int)ncols, cb, xt, nkb);
     if (P.nitem1 > 0) {
       P1Args<T, NC> a1{P.d_item1, P.nitem1, P.d_col1, P.d_zpl, (const T*)h->d_rk, xt, xt_copy, zt, h->d_tc_err};
-      tc_phase1_kernel<T, NC><<<(unsigned)std::min<int64_t>(nsm, P.nitem1), TC_THREADS, S::BYTES, st>>>(a1);
+      tc_phase1_kernel<T, NC><<<(unsigned)std::min<int64_t>(nsm, P.nitem1), TC_THREADS, C::BYTES, st>>>(a1);
     }
     if (P.nitem2 > 0) {
       P2Args<T, NC> a2{P.d_item2, P.nitem2, P.d_z2, (const T*)h->d_rk, zt, d_y, n, (int)ncols, cb, h->d_tc_err};
-      tc_phase2_kernel<T, NC><<<(unsigned)std::min<int64_t>(nsm, P.nitem2), TC_THREADS, S::BYTES, st>>>(a2);
+      tc_phase2_kernel<T, NC><<<(unsigned)std::min<int64_t>(nsm, P.nitem2), TC_THREADS, C::BYTES, st>>>(a2);
     }
   }
   HM_CUDA_TRY(cudaGetLastError());

@@ -74,6 +74,12 @@ __device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, uint32_
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// one arrival on `bar` once every cp.async issued so far by this thread has
+// landed (the barrier's expected count includes it: .noinc)
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
@@ -135,6 +141,27 @@ __device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a_desc, uint64_t b
   }
 }
 
+// The same MMA with A read from tensor memory: a_tmem addresses lane 0 and the
+// first column of a 128-lane A tile (row i of A in lane i, K along the
+// columns: one TF32 value or two packed BF16 values per 32-bit column).
+template <int KIND>
+__device__ __forceinline__ void mma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc_v,
+                                       uint32_t accumulate) {
+  if constexpr (KIND == 0) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(b_desc), "r"(idesc_v), "r"(accumulate)
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(b_desc), "r"(idesc_v), "r"(accumulate)
+        : "memory");
+  }
+}
+
 // arrive once on `bar` when every MMA issued so far by this thread is done
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
@@ -168,6 +195,29 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 32 lanes x 8 consecutive 32-bit columns
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// the converse: thread t of the warp writes 16 consecutive 32-bit columns of
+// lane (lane base + t); tmem_wait_st waits until this thread's stores landed
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+      "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 // ---------------------------------------------------------------------------
 // operand splits for near-FP32 products on TF32 / BF16 tensor cores
 // (Ootomo & Yokota 2022, "Recovering single precision accuracy from Tensor
@@ -175,13 +225,59 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 // (low mantissa bits zero), lo = x - hi (exact in FP32) rounded the same way.
 // Both parts are exact values of the narrow format, so the tensor core's own
 // input conversion leaves them unchanged.
+//
+// The rounding is Veltkamp's splitting (Dekker 1971; Boldo 2006 shows the
+// high part is a rounding to nearest): with t = (2^(24-SIG) + 1) x in FP32,
+// hi = t - (t - x) has at most SIG significant bits.  Three full-rate FP32
+// operations instead of a conversion instruction, which issues on the
+// quarter-rate XU pipe and was the limit of the operand converters.  The
+// operations are written as intrinsics so that no FMA contraction changes
+// them.  Past |x| = 2^100 (where t could overflow) the mantissa is rounded
+// on its bits; NaN stays NaN.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float tf32_rn(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r & 0xFFFFE000u);
+template <int SIG>
+__device__ __forceinline__ float round_sig(float x) {
+  constexpr float SIGMA = (float)((1u << (24 - SIG)) + 1u);
+  constexpr uint32_t half = 1u << (23 - SIG), mask = ~((1u << (24 - SIG)) - 1u);
+  const float t = __fmul_rn(x, SIGMA);
+  const float v = __fsub_rn(t, __fsub_rn(t, x));
+  const uint32_t b = __float_as_uint(x);
+  const float r = x == x ? __uint_as_float((b + half) & mask) : __uint_as_float(b | 0x00400000u);
+  return fabsf(x) <= 0x1p100f ? v : r;      // selects, no branch
 }
-__device__ __forceinline__ float bf16_rn(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+__device__ __forceinline__ float tf32_rn(float x) { return round_sig<11>(x); }
+__device__ __forceinline__ float bf16_rn(float x) { return round_sig<8>(x); }
+
+// The split x = hi + lo of N values (hi to SIG bits, lo = x - hi rounded to
+// SIG bits), as 32-bit patterns.  The bound |x| <= 2^100 is checked once for
+// all N values; below it the three-operation form alone runs (NaN stays NaN).
+template <int SIG>
+__device__ __forceinline__ float veltkamp_hi(float x) {
+  constexpr float SIGMA = (float)((1u << (24 - SIG)) + 1u);
+  const float t = __fmul_rn(x, SIGMA);
+  return __fsub_rn(t, __fsub_rn(t, x));
+}
+template <int SIG, int N>
+__device__ __forceinline__ void split_n(const float (&x)[N], uint32_t (&hi)[N], uint32_t (&lo)[N]) {
+  float mx = 0.f;
+#pragma unroll
+  for (int e = 0; e < N; ++e) mx = fmaxf(mx, fabsf(x[e]));
+  if (mx <= 0x1p100f) {
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+      const float h = veltkamp_hi<SIG>(x[e]);
+      hi[e] = __float_as_uint(h);
+      lo[e] = __float_as_uint(veltkamp_hi<SIG>(__fsub_rn(x[e], h)));
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+      const float h = round_sig<SIG>(x[e]);
+      hi[e] = __float_as_uint(h);
+      lo[e] = __float_as_uint(round_sig<SIG>(__fsub_rn(x[e], h)));
+    }
+  }
+}
 
 }  // namespace tc
 }  // namespace hm

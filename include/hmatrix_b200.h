@@ -230,10 +230,11 @@ int hm_status(hm_handle* h, void* stream);
 /* Self-test of the tensor-core operand layouts of the multi-RHS matvec, on
  * the current device: D = A B' for A 128 x KC and B 2nc x KC (row-major
  * FP32 host arrays, KC = 16 for kind 0 = TF32, 32 for kind 1 = BF16, whose
- * inputs must be exact BF16 values), with A staged in the kernels' K-major
- * (a_mn = 0) or M-major (a_mn = 1) tile layout; D is 128 x 2nc row-major,
+ * inputs must be exact BF16 values), B staged as the kernels' X / Z tiles and
+ * A either as a K-major shared-memory tile (a_src = 0) or in tensor memory as
+ * the kernels' converters write it (a_src = 2); D is 128 x 2nc row-major,
  * nc = 16 or 64.  No counterpart in the reference. */
-int hm_tc_selftest(int32_t kind, int32_t a_mn, int32_t nc, const float* A, const float* B, float* D);
+int hm_tc_selftest(int32_t kind, int32_t a_src, int32_t nc, const float* A, const float* B, float* D);
 
 /* R = B - H*X (trans=0) or B - H'*X (trans=1) for n x ncols column-major
  * blocks, every product and sum carried in twice the FP64 precision (error-free

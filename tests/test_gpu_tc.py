@@ -4,8 +4,8 @@
 the stacked factor products run as tensor-core GEMMs.  Checked:
 
 * the operand layouts and descriptors on one tile (hm_tc_selftest) against
-  numpy, for both kinds (TF32, BF16) and both A layouts (K-major of phase 1,
-  M-major of phase 2);
+  numpy, for both kinds (TF32, BF16), B as the X / Z tiles and A in shared
+  memory (K-major) or in tensor memory (as the converters write it);
 * H*X and H'*X on the tensor cores against the CUDA-core block kernels on the
   same stored factors (HM_FLAG_MV_SIMT) and against the FP64-factor product:
   FP32 factors use three TF32 products per term and FP32 accumulation; the
@@ -42,20 +42,20 @@ def _tf32(x):
 
 
 @pytest.mark.parametrize("kind", [0, 1])
-@pytest.mark.parametrize("a_mn", [0, 1])
+@pytest.mark.parametrize("a_src", [0, 2])
 @pytest.mark.parametrize("nc", [16, 64])
-def test_tc_layout_selftest(kind, a_mn, nc):
+def test_tc_layout_selftest(kind, a_src, nc):
     from hmatrix import _lib
-    rng = np.random.default_rng(100 + 10 * kind + a_mn + nc)
+    rng = np.random.default_rng(100 + 10 * kind + a_src + nc)
     K = 16 if kind == 0 else 32
     rnd = _tf32 if kind == 0 else _bf16
     A = rnd(rng.standard_normal((128, K)).astype(np.float32))
     B = rnd(rng.standard_normal((2 * nc, K)).astype(np.float32))
     D = np.zeros((128, 2 * nc), np.float32)
     p = lambda a: C.c_void_p(a.ctypes.data)
-    _lib.check(_lib.lib().hm_tc_selftest(kind, a_mn, nc, p(A), p(B), p(D)))
+    _lib.check(_lib.lib().hm_tc_selftest(kind, a_src, nc, p(A), p(B), p(D)))
     R = A.astype(np.float64) @ B.astype(np.float64).T
-    assert np.abs(D - R).max() <= 1e-5 * np.abs(R).max(), (kind, a_mn, nc)
+    assert np.abs(D - R).max() <= 1e-5 * np.abs(R).max(), (kind, a_src, nc)
 
 
 def _build(storage, tree, n):
