@@ -537,6 +537,7 @@ int hm_scale(hm_handle* h, double u) {
   if (!h) return fail(HM_ERR_ARG, "NULL handle");
   if (h->factorized) return fail(HM_ERR_STATE, "Hmatrix is frozen after factorization");
   DeviceGuard g(h->device);
+  tc_factors_changed(h);
   return apply_scale(h, u);
 }
 

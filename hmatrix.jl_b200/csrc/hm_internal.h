@@ -288,6 +288,8 @@ int matvec_multi_device(hm_handle* h, const double* d_x, double* d_y, int64_t nc
                         bool simt = false);
 // the low-rank part of Y = H X on the tensor cores, added into Y (hm_matvec_tc.cu)
 int matvec_multi_tc(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st);
+int tc_prepare(hm_handle* h, int trans, bool* usable);
+void tc_factors_changed(hm_handle* h);
 int tc_status(hm_handle* h, cudaStream_t st);
 int tc_selftest(int kind, int a_src, int nc, const float* A, const float* B, float* D);
 void free_tc_plan(TcPlan*& p);

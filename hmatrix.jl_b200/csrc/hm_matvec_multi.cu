@@ -639,24 +639,30 @@ int multi_t(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int tra
 
 }  // namespace
 
-// FP64 factors (no tensor-core kind for FP64), or simt: the CUDA-core block
-// kernels for the whole product.  FP32/BF16 factors: the dense leaves on the
-// CUDA cores (they write every row of Y), then the low-rank part on the
-// tensor cores (added into Y).
+// FP64 factors (no tensor-core kind for FP64), simt, or factors beyond the
+// tensor-core path's range (2^100): the CUDA-core block kernels for the whole
+// product.  FP32/BF16 factors: the dense leaves on the CUDA cores (they write
+// every row of Y), then the low-rank part on the tensor cores (added into Y).
 int matvec_multi_device(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st,
                         bool simt) {
   if (ncols <= 0) return HM_OK;
   if ((h->n + 2) * pad_to(ncols, 16) > (int64_t)1 << 40) return fail(HM_ERR_UNSUPPORTED, "right-hand side block too large");
   switch (h->storage) {
     case HM_F64: return multi_t<double>(h, d_x, d_y, ncols, trans, st);
-    case HM_F32:
-      if (simt) return multi_t<float>(h, d_x, d_y, ncols, trans, st);
+    case HM_F32: {
+      bool tc = false;
+      if (!simt) HM_TRY(tc_prepare(h, trans, &tc));
+      if (!tc) return multi_t<float>(h, d_x, d_y, ncols, trans, st);
       HM_TRY(multi_t<float>(h, d_x, d_y, ncols, trans, st, true));
       return matvec_multi_tc(h, d_x, d_y, ncols, trans, st);
-    default:
-      if (simt) return multi_t<__nv_bfloat16>(h, d_x, d_y, ncols, trans, st);
+    }
+    default: {
+      bool tc = false;
+      if (!simt) HM_TRY(tc_prepare(h, trans, &tc));
+      if (!tc) return multi_t<__nv_bfloat16>(h, d_x, d_y, ncols, trans, st);
       HM_TRY(multi_t<__nv_bfloat16>(h, d_x, d_y, ncols, trans, st, true));
       return matvec_multi_tc(h, d_x, d_y, ncols, trans, st);
+    }
   }
 }
 

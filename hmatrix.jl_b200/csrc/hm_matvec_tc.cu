@@ -83,14 +83,19 @@ struct TcPlan {
   int64_t nz2 = 0;
   TcItem2* d_item2 = nullptr;
   int64_t nitem2 = 0;
+  bool checked = false;    // `usable` is up to date with the factor pool
+  bool usable = false;     // every factor entry is at most 2^100 in magnitude (no NaN)
 };
 
 namespace {
 
 constexpr int TC_WR = 512;           // rows of a phase-2 window
-constexpr int TC_THREADS = 416;      // warps 0-7 convert + drain, 8-11 produce, 12 MMA
-constexpr int TC_PROD0 = 256;        // first producer thread
-constexpr int TC_NA = 2;             // TMEM A buffers
+constexpr int TC_PW = 4;                          // producer warps
+constexpr int TC_MMA_WARP = 8 + TC_PW;             // warps 0-7 convert + drain, 8 .. produce, then MMA
+constexpr int TC_THREADS = 32 * (TC_MMA_WARP + 1);
+constexpr int TC_PROD0 = 256;                      // first producer thread
+constexpr int TC_NPROD = 32 * TC_PW;
+constexpr int TC_NA_MAX = 4;         // TMEM A buffers, at most
 constexpr int TC_TMEM_COLS = 512;    // one CTA per SM (shared memory), so all of TMEM
 constexpr uint32_t TC_WAIT = 1u << 22;   // polls of a bounded mbarrier wait
 
@@ -140,19 +145,24 @@ struct TcCfg {
   static constexpr int STAGE = (B_BYTES + RAW + 1023) / 1024 * 1024;
   static constexpr int BAR_OFF = S * STAGE;
   static constexpr int BYTES = BAR_OFF + 512;
-  static constexpr int ACC0 = TC_NA * Tr::ACOLS;             // first accumulator column
+  // as many TMEM A buffers as fit beside the two accumulators (at most 4):
+  // the converters run up to NA stages ahead of the MMAs' completion
+  static constexpr int NA_FIT = (TC_TMEM_COLS - 2 * 2 * NC) / Tr::ACOLS;
+  static constexpr int NA = NA_FIT < TC_NA_MAX ? NA_FIT : TC_NA_MAX;
+  static constexpr int ACC0 = NA * Tr::ACOLS;                // first accumulator column
+  static_assert(NA >= 2, "two A buffers at least");
   static_assert(BYTES <= 227 * 1024, "stages exceed the shared memory of a CTA");
   static_assert(ACC0 + 2 * 2 * NC <= TC_TMEM_COLS, "A buffers and accumulators exceed TMEM");
   static_assert(RS1 % 16 == 0 && RS2 % 16 == 0 && B_BYTES % 16 == 0, "bulk copies move 16-byte units");
-  static_assert(KC % 4 == 0 && KC % Tr::KM == 0, "a stage is whole MMAs and whole producer warps");
+  static_assert(KC % TC_PW == 0 && KC % Tr::KM == 0, "a stage is whole MMAs and whole producer warps");
 };
 
 struct TcBars {
   uint64_t full[5];        // raw stage landed (the producers' cp.async arrivals)
   uint64_t bfull[5];       // the stage's B tile landed (bulk-copy bytes + one arrival)
   uint64_t empty[5];       // the MMAs that read the stage's B tile finished (tcgen05.commit)
-  uint64_t afull[TC_NA];   // A buffer written (256 converter threads)
-  uint64_t aempty[TC_NA];  // the MMAs that read the A buffer finished
+  uint64_t afull[TC_NA_MAX];   // A buffer written (256 converter threads)
+  uint64_t aempty[TC_NA_MAX];  // the MMAs that read the A buffer finished
   uint64_t accfull[2];     // accumulator complete (commit after a tile's last MMA)
   uint64_t accempty[2];    // accumulator drained (256 converter threads)
   uint64_t done;           // the MMA issuer's last commit: every MMA finished
@@ -195,7 +205,7 @@ __device__ __forceinline__ uint32_t tc_setup(TcBars* b, int warp, int nstage, ui
       tc::mbar_init(&b->bfull[s], 1);
       tc::mbar_init(&b->empty[s], 1);
     }
-    for (int q = 0; q < TC_NA; ++q) {
+    for (int q = 0; q < TC_NA_MAX; ++q) {
       tc::mbar_init(&b->afull[q], 256);
       tc::mbar_init(&b->aempty[q], 1);
     }
@@ -255,9 +265,9 @@ __device__ __forceinline__ void tc_mma_role(TcBars* b, uint32_t sbase, uint32_t 
     tc::tc_fence_after();
     const uint32_t dacc = tmem + (uint32_t)C::ACC0 + q * 2 * NC;
     for (int kc = 0; kc < nk; ++kc, ++it) {
-      const int s = (int)(it % C::S), a = (int)(it % TC_NA);
+      const int s = (int)(it % C::S), a = (int)(it % C::NA);
       if (!tc_wait(b, &b->bfull[s], (it / C::S) & 1u, err, 4)) { ok = false; break; }
-      if (!tc_wait(b, &b->afull[a], (it / TC_NA) & 1u, err, 4)) { ok = false; break; }
+      if (!tc_wait(b, &b->afull[a], (it / C::NA) & 1u, err, 4)) { ok = false; break; }
       tc::tc_fence_after();
       const uint32_t bbase = sbase + (uint32_t)(s * C::STAGE);
       const uint32_t abuf = tmem + (uint32_t)(a * Tr::ACOLS);
@@ -309,6 +319,19 @@ __global__ void tc_xt_kernel(const double* __restrict__ X, int64_t n, int64_t ld
   }
 }
 
+// max |x| over the factor pool as an FP32 bit pattern (NaN sorts above every
+// number): the converters split without a magnitude check, which is exact
+// while |x| <= 2^100
+template <typename T>
+__global__ void pool_maxabs_kernel(const T* __restrict__ p, int64_t cnt, unsigned* __restrict__ out) {
+  unsigned m = 0;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, __float_as_uint(fabsf((float)p[e])));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
 // zero the Z tiles from block kb0 on (the padding after the last slot)
 template <typename T>
 __global__ void tc_zero_kernel(typename TcT<T>::Bits* __restrict__ p, int64_t cnt) {
@@ -333,12 +356,16 @@ __device__ __forceinline__ void conv1(const uint8_t* raw, int kl, uint32_t ta, i
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
       const float4 x4 = *reinterpret_cast<const float4*>(raw + (c0 + 4 * v) * 4);
-      x[4 * v + 0] = c0 + 4 * v + 0 < kl ? x4.x : 0.f;
-      x[4 * v + 1] = c0 + 4 * v + 1 < kl ? x4.y : 0.f;
-      x[4 * v + 2] = c0 + 4 * v + 2 < kl ? x4.z : 0.f;
-      x[4 * v + 3] = c0 + 4 * v + 3 < kl ? x4.w : 0.f;
+      x[4 * v + 0] = x4.x;
+      x[4 * v + 1] = x4.y;
+      x[4 * v + 2] = x4.z;
+      x[4 * v + 3] = x4.w;
     }
-    tc::split_n<11>(x, hi, lo);
+    if (c0 + 16 > kl) {
+#pragma unroll
+      for (int e = 0; e < 16; ++e) x[e] = c0 + e < kl ? x[e] : 0.f;
+    }
+    tc::split_fast<11>(x, hi, lo);        // factor magnitudes were checked when the plan was built
     tc::tmem_st16(ta + c0, hi);
     tc::tmem_st16(ta + KC + c0, lo);
   }
@@ -365,14 +392,16 @@ __device__ __forceinline__ void conv1(const uint8_t* raw, int kl, uint32_t ta, i
 }
 
 // phase 2: slot k's tile row m sits at element meta[k].z + m of the raw
-// area when m is in [meta[k].x, meta[k].y) (the covered rows), else is 0
+// area when m - meta[k].x < meta[k].y (the covered rows), else is 0
 __device__ __forceinline__ float slot_val(const uint8_t* rb, const int4* meta, int k, int m, float*) {
   const int4 md = meta[k];
-  return (m >= md.x && m < md.y) ? reinterpret_cast<const float*>(rb)[md.z + m] : 0.f;
+  const float v = reinterpret_cast<const float*>(rb)[md.z + m];
+  return (uint32_t)(m - md.x) < (uint32_t)md.y ? v : 0.f;
 }
 __device__ __forceinline__ uint32_t slot_val(const uint8_t* rb, const int4* meta, int k, int m, __nv_bfloat16*) {
   const int4 md = meta[k];
-  return (m >= md.x && m < md.y) ? (uint32_t)reinterpret_cast<const uint16_t*>(rb)[md.z + m] : 0u;
+  const uint32_t v = reinterpret_cast<const uint16_t*>(rb)[md.z + m];
+  return (uint32_t)(m - md.x) < (uint32_t)md.y ? v : 0u;
 }
 __device__ __forceinline__ void conv2(const uint8_t* rb, const int4* meta, int m, uint32_t ta, int h, float* tag) {
   constexpr int KC = TcT<float>::KC;
@@ -382,7 +411,7 @@ __device__ __forceinline__ void conv2(const uint8_t* rb, const int4* meta, int m
     uint32_t hi[16], lo[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) x[j] = slot_val(rb, meta, c0 + j, m, tag);
-    tc::split_n<11>(x, hi, lo);
+    tc::split_fast<11>(x, hi, lo);        // factor magnitudes were checked when the plan was built
     tc::tmem_st16(ta + c0, hi);
     tc::tmem_st16(ta + KC + c0, lo);
   }
@@ -425,15 +454,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase1_kernel(P1Args<T, NC> 
   extern __shared__ __align__(1024) uint8_t smem[];
   TcBars* bars = reinterpret_cast<TcBars*>(smem + C::BAR_OFF);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t tmem = tc_setup(bars, warp, C::S, 128);    // 128 producer cp.async arrivals
+  const uint32_t tmem = tc_setup(bars, warp, C::S, TC_NPROD);    // the producers' cp.async arrivals
   const uint32_t sbase = tc::smem_u32(smem);
   auto nk_of = [&](int64_t w) { return (int)((a.items[w].len + KC - 1) / KC); };
 
-  if (warp >= 8 && warp < 12) {
+  if (warp >= 8 && warp < TC_MMA_WARP) {
     // ---------------- producers: the X tile (one bulk copy) and 256 bytes of each column ----------------
-    // thread pt copies 16-byte piece q of the columns cg, cg + 8, .., cg + 120
-    // (the column offsets are re-read every stage: L1 hits after the first,
-    // and the next tile's are prefetched into L1 while this one streams)
+    // thread pt copies 16-byte piece q of the columns cg, cg + CG, .., (CG = 2 TC_PW column groups)
+    // (the tile's column offsets are loaded into registers once per tile:
+    // re-reading them every stage put a load latency in front of each stage's
+    // copies; the first stage's wait is covered by the stages already queued)
+    constexpr int CG = TC_NPROD / 16, CPT = 128 / CG;      // column groups, columns per thread
     const int pt = threadIdx.x - TC_PROD0;
     const int q = pt & 15, cg = pt >> 4;
     uint32_t it = 0;
@@ -447,6 +478,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase1_kernel(P1Args<T, NC> 
       const int64_t kb0 = ((int64_t)I.seg0 + qs) / KE;
       const int64_t plen = pad_to((int64_t)I.len, KE);       // stored column length
       const int nk = (int)((I.len + KC - 1) / KC);
+      uint64_t coff[CPT];
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        const uint32_t c = (uint32_t)(cg + CG * j);
+        coff[j] = c < I.ncol ? __ldg(&a.cols[I.col0 + c].off) : 0;
+      }
       for (int kc = 0; kc < nk; ++kc) {
         const int s = (int)(it % C::S);
         if (!tc_wait(bars, &bars->empty[s], ((it / C::S) & 1u) ^ 1u, a.err, 1)) { stop = true; break; }
@@ -461,20 +498,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase1_kernel(P1Args<T, NC> 
         const bool in = el < plen;
         const uint32_t dst = st + C::B_BYTES + q * 16;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const uint32_t c = (uint32_t)(cg + 8 * j);
+        for (int j = 0; j < CPT; ++j) {
+          const uint32_t c = (uint32_t)(cg + CG * j);
           const bool ok = in && c < I.ncol;
-          const uint64_t off = c < I.ncol ? __ldg(&a.cols[I.col0 + c].off) : 0;
-          tc::cp_async16(dst + c * C::RS1, ok ? (const void*)(a.pool + off + el) : (const void*)a.pool,
+          tc::cp_async16(dst + c * C::RS1, ok ? (const void*)(a.pool + coff[j] + el) : (const void*)a.pool,
                          ok ? 16u : 0u);
         }
         tc::cp_async_mbar_arrive(&bars->full[s]);
         ++it;
         if (kc == 0 && q == 0) {
+          // the next tile's column entries into L2 while this one streams
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const uint32_t c = (uint32_t)(cg + 8 * j);
-            if (c < I2.ncol) asm volatile("prefetch.global.L1 [%0];" ::"l"(&a.cols[I2.col0 + c]));
+          for (int j = 0; j < CPT; ++j) {
+            const uint32_t c = (uint32_t)(cg + CG * j);
+            if (c < I2.ncol) asm volatile("prefetch.global.L2 [%0];" ::"l"(&a.cols[I2.col0 + c]));
           }
         }
       }
@@ -483,7 +520,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase1_kernel(P1Args<T, NC> 
     }
     tc::cp_async_wait_all();
     if (pt == 0) tc_copies_drain(bars, it, C::S, a.err);
-  } else if (warp == 12) {
+  } else if (warp == TC_MMA_WARP) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) tc_mma_role<T, NC>(bars, sbase, tmem, a.nitems, nk_of, a.err);
   } else if (warp < 8) {
@@ -534,13 +571,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase1_kernel(P1Args<T, NC> 
       const int nk = (int)((I.len + KC - 1) / KC);
       const bool row = (uint32_t)m < I.ncol;
       // the previous tile is drained after stage kd of this one: converting
-      // stage 1 needed the A buffer of the previous tile's last stage back, so
-      // by then its MMAs (and its accumulator) are complete
-      const int kd = nk > 1 ? 1 : 0;
+      // stage NA - 1 needed the A buffer of the previous tile's last stage
+      // back, so by then its MMAs (and its accumulator) are complete
+      const int kd = min(C::NA - 1, nk - 1);
       for (int kc = 0; kc < nk; ++kc, ++it) {
-        const int s = (int)(it % C::S), ab = (int)(it % TC_NA);
+        const int s = (int)(it % C::S), ab = (int)(it % C::NA);
         if (!tc_wait_warp(bars, &bars->full[s], (it / C::S) & 1u, a.err, 64)) { stop = true; break; }
-        if (!tc_wait_warp(bars, &bars->aempty[ab], ((it / TC_NA) & 1u) ^ 1u, a.err, 64)) { stop = true; break; }
+        if (!tc_wait_warp(bars, &bars->aempty[ab], ((it / C::NA) & 1u) ^ 1u, a.err, 64)) { stop = true; break; }
         tc::tc_fence_after();
         const uint8_t* raw = smem + s * C::STAGE + C::B_BYTES + m * C::RS1;
         const int kl = row ? (int)min((int64_t)KC, (int64_t)I.len - (int64_t)kc * KC) : 0;
@@ -586,20 +623,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
   extern __shared__ __align__(1024) uint8_t smem[];
   TcBars* bars = reinterpret_cast<TcBars*>(smem + C::BAR_OFF);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t tmem = tc_setup(bars, warp, C::S, 128 + 4);   // cp.async arrivals + 4 slot-table arrivals
+  const uint32_t tmem = tc_setup(bars, warp, C::S, TC_NPROD + TC_PW);   // cp.async arrivals + slot-table arrivals
   const uint32_t sbase = tc::smem_u32(smem);
   auto nk_of = [&](int64_t w) {
     const TcItem2 I = a.items[w];
     return (int)((I.ze - (I.zb / KE) * KE + KC - 1) / KC);
   };
 
-  if (warp >= 8 && warp < 12) {
+  if (warp >= 8 && warp < TC_MMA_WARP) {
     // ---------------- producers: the Z tile (one bulk copy) and each slot's rows of the tile ----------------
     // warp pw handles slots SPW pw .. SPW pw + SPW - 1 of a stage; lane i
     // (< SPW) holds slot SPW pw + i's descriptor, loaded one stage ahead; per
     // slot the warp copies the rows lane by lane (16 bytes a lane) and lane 0
     // writes the slot table entry
-    constexpr int SPW = KC / 4;
+    constexpr int SPW = KC / TC_PW;
     static_assert(SPW <= 32, "one descriptor per lane");
     const int pw = warp - 8;
     uint32_t it = 0;
@@ -625,6 +662,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
         nk2 = w2 < a.nitems ? (int)((I2.ze - (I2.zb / KE) * KE + KC - 1) / KC) : 0;
       }
       const TcZ2 nxt = w2 < a.nitems ? load_desc(I2, kc2) : TcZ2{0, 0, 0};
+      {
+        // the descriptors of the stage after that into L2 (one 128-byte line
+        // holds 8 of them)
+        const int64_t zq = (int64_t)(I2.zb / KE) * KE + (int64_t)(kc2 + 1) * KC + SPW * pw + 8 * lane;
+        if (w2 < a.nitems && 8 * lane < SPW && zq < (int64_t)I2.ze)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(a.z2 + zq));
+      }
       // this stage
       const int s = (int)(it % C::S);
       if (!tc_wait_warp(bars, &bars->empty[s], ((it / C::S) & 1u) ^ 1u, a.err, 1)) break;
@@ -654,7 +698,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
           src = slo;
           dsto = (uint32_t)(C::B_BYTES + k * C::RS2 + (slo - (gt - shl)) * ES);
           nb = (uint32_t)((shi - slo) * ES);
-          md = make_int4(r0 - toff, r1 - toff, k * (C::RS2 / ES) + shl, 0);
+          md = make_int4(r0 - toff, r1 - r0, k * (C::RS2 / ES) + shl, 0);
         }
         meta[k] = md;
       }
@@ -681,7 +725,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
     }
     tc::cp_async_wait_all();
     if (pw == 0 && lane == 0) tc_copies_drain(bars, it, C::S, a.err);
-  } else if (warp == 12) {
+  } else if (warp == TC_MMA_WARP) {
     if (lane == 0) tc_mma_role<T, NC>(bars, sbase, tmem, a.nitems, nk_of, a.err);
   } else if (warp < 8) {
     // ---------------- converters (thread = TMEM lane m = tile row m) + drain ----------------
@@ -719,11 +763,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
     for (int64_t w = blockIdx.x; w < a.nitems && !stop; w += gridDim.x, ++j) {
       const TcItem2 I2 = w + gridDim.x < a.nitems ? a.items[w + gridDim.x] : TcItem2{};
       const int nk = (int)((I.ze - (I.zb / KE) * KE + KC - 1) / KC);
-      const int kd = nk > 1 ? 1 : 0;                 // as in phase 1
+      const int kd = min(C::NA - 1, nk - 1);         // as in phase 1
       for (int kc = 0; kc < nk; ++kc, ++it) {
-        const int s = (int)(it % C::S), ab = (int)(it % TC_NA);
+        const int s = (int)(it % C::S), ab = (int)(it % C::NA);
         if (!tc_wait_warp(bars, &bars->full[s], (it / C::S) & 1u, a.err, 64)) { stop = true; break; }
-        if (!tc_wait_warp(bars, &bars->aempty[ab], ((it / TC_NA) & 1u) ^ 1u, a.err, 64)) { stop = true; break; }
+        if (!tc_wait_warp(bars, &bars->aempty[ab], ((it / C::NA) & 1u) ^ 1u, a.err, 64)) { stop = true; break; }
         tc::tc_fence_after();
         const uint8_t* rb = smem + s * C::STAGE + C::B_BYTES;
         conv2(rb, reinterpret_cast<const int4*>(rb + C::RAW2), m, tmem + lb + (uint32_t)(ab * Tr::ACOLS), h,
@@ -1040,6 +1084,37 @@ static int build_tc_plan(hm_handle* h, int trans, TcPlan** out) {
   return HM_OK;
 }
 
+// The factor magnitudes the converters' split relies on, measured once per
+// state of the factor pool.
+static int check_pool(hm_handle* h, TcPlan* P) {
+  const int eb = elem_bytes(h->storage);
+  {
+    const int64_t cnt = (int64_t)(h->rk_bytes / (size_t)eb);
+    unsigned* d_m = nullptr;
+    unsigned mbits = 0;
+    cudaError_t e = cudaMalloc(&d_m, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(d_m, 0, sizeof(unsigned));
+    if (e == cudaSuccess && cnt > 0) {
+      const unsigned g = (unsigned)std::min<int64_t>((cnt + 255) / 256, 148 * 16);
+      if (h->storage == HM_F32) pool_maxabs_kernel<float><<<g, 256>>>((const float*)h->d_rk, cnt, d_m);
+      else pool_maxabs_kernel<__nv_bfloat16><<<g, 256>>>((const __nv_bfloat16*)h->d_rk, cnt, d_m);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(&mbits, d_m, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    if (d_m) cudaFree(d_m);
+    if (e != cudaSuccess) return fail(HM_ERR_CUDA, std::string("tensor-core plan: ") + cudaGetErrorString(e));
+    P->usable = mbits <= 0x71800000u;           // 2^100
+    P->checked = true;
+  }
+  return HM_OK;
+}
+
+// the factor pool changed (hm_scale): the magnitude check runs again
+void tc_factors_changed(hm_handle* h) {
+  if (h->tc_fwd) h->tc_fwd->checked = false;
+  if (h->tc_bwd) h->tc_bwd->checked = false;
+}
+
 // ---------------------------------------------------------------------------
 // launch
 // ---------------------------------------------------------------------------
@@ -1110,6 +1185,19 @@ static int tc_dispatch(hm_handle* h, TcPlan& P, const double* d_x, double* d_y, 
   return launch_tc<T, 64>(h, P, d_x, d_y, ncols, st);
 }
 
+// Builds the plan of a direction on first use and reports whether the
+// tensor-core path applies (FP32/BF16 factors, all of them at most 2^100 in
+// magnitude); otherwise the caller takes the CUDA-core block kernels.
+int tc_prepare(hm_handle* h, int trans, bool* usable) {
+  *usable = false;
+  if (h->storage != HM_F32 && h->storage != HM_BF16) return HM_OK;
+  TcPlan*& P = trans ? h->tc_bwd : h->tc_fwd;
+  if (!P) HM_TRY(build_tc_plan(h, trans, &P));
+  if (!P->checked) HM_TRY(check_pool(h, P));
+  *usable = P->usable;
+  return HM_OK;
+}
+
 // Y += the low-rank part of H X (H' X) on the tensor cores; the caller has
 // written the dense part into Y.
 int matvec_multi_tc(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st) {
@@ -1117,6 +1205,8 @@ int matvec_multi_tc(hm_handle* h, const double* d_x, double* d_y, int64_t ncols,
     return fail(HM_ERR_UNSUPPORTED, "tensor-core matvec: FP32 or BF16 factors only");
   TcPlan*& P = trans ? h->tc_bwd : h->tc_fwd;
   if (!P) HM_TRY(build_tc_plan(h, trans, &P));
+  if (!P->checked) HM_TRY(check_pool(h, P));
+  if (!P->usable) return fail(HM_ERR_UNSUPPORTED, "tensor-core matvec: a factor entry exceeds 2^100 or is NaN");
   if (h->storage == HM_F32) return tc_dispatch<float>(h, *P, d_x, d_y, ncols, st);
   return tc_dispatch<__nv_bfloat16>(h, *P, d_x, d_y, ncols, st);
 }

@@ -257,6 +257,25 @@ __device__ __forceinline__ float veltkamp_hi(float x) {
   const float t = __fmul_rn(x, SIGMA);
   return __fsub_rn(t, __fsub_rn(t, x));
 }
+// The split of values known to be finite and at most 2^100 in magnitude
+// (the factor pool, checked when a plan is built): rounding to SIG bits on
+// the bit pattern (add half a unit of the last kept bit, clear the rest:
+// round to nearest, ties away from zero; a carry into the exponent is the
+// correct rounding up), lo = x - hi exact in FP32 and rounded the same way.
+// Two integer operations per rounding instead of three FP32 operations.
+// (Packed FP32x2 arithmetic does not serve here: the assembler contracts the
+// Veltkamp sequence into fused operations, which returns hi = x.)
+template <int SIG, int N>
+__device__ __forceinline__ void split_fast(const float (&x)[N], uint32_t (&hi)[N], uint32_t (&lo)[N]) {
+  constexpr uint32_t half = 1u << (23 - SIG), mask = ~((1u << (24 - SIG)) - 1u);
+#pragma unroll
+  for (int e = 0; e < N; ++e) {
+    const uint32_t h = (__float_as_uint(x[e]) + half) & mask;
+    const float d = __fsub_rn(x[e], __uint_as_float(h));
+    hi[e] = h;
+    lo[e] = (__float_as_uint(d) + half) & mask;
+  }
+}
 template <int SIG, int N>
 __device__ __forceinline__ void split_n(const float (&x)[N], uint32_t (&hi)[N], uint32_t (&lo)[N]) {
   float mx = 0.f;

@@ -101,6 +101,24 @@ def test_tc_against_fp64_factors():
     assert H32.info().factorized == 0
 
 
+def test_tc_range_fallback():
+    # factors beyond 2^100 in magnitude take the CUDA-core block kernels (the
+    # converters' hi/lo split is exact only below 2^100); the check is redone
+    # when hm_scale changes the factors of a handle that already multiplied
+    from hmatrix import _lib
+    n = 4096
+    _, H = _build("F32", "bisect", n)
+    X = np.random.default_rng(24).standard_normal((n, 16))
+    Y = H * X                                   # tensor cores (plan built, factors in range)
+    _lib.check(_lib.lib().hm_scale(H._h, 2.0 ** 110))
+    Yb = H * X
+    assert np.all(np.isfinite(Yb))
+    assert np.array_equal(Yb, _simt(H, X, False))
+    assert np.abs(Yb * 2.0 ** -110 - Y).max() <= 1e-5 * np.abs(Y).max()
+    _lib.check(_lib.lib().hm_scale(H._h, 2.0 ** -110))
+    assert np.abs(H * X - Y).max() <= 1e-12 * np.abs(Y).max()     # back in range: tensor cores again
+
+
 def test_tc_device_pointers_and_status():
     import torch
     import hmatrix as hm
