@@ -98,6 +98,11 @@ constexpr int TC_NPROD = 32 * TC_PW;
 constexpr int TC_NA_MAX = 4;         // TMEM A buffers, at most
 constexpr int TC_TMEM_COLS = 512;    // one CTA per SM (shared memory), so all of TMEM
 constexpr uint32_t TC_WAIT = 1u << 22;   // polls of a bounded mbarrier wait
+// Phase 2 adds its FP32 accumulator into the FP64 Y every TC_KSEG2 stages
+// (512 Z slots for FP32 factors, 1024 for BF16): a window's K runs over every
+// leaf that touches it (thousands of terms at n = 2^20), and one FP32 sum over
+// all of them would lose accuracy as n grows.
+constexpr int TC_KSEG2 = 8;
 
 template <typename T> struct TcT;
 template <> struct TcT<float> {
@@ -246,41 +251,46 @@ __device__ __forceinline__ void tc_copies_drain(TcBars* b, uint32_t it, int nsta
 }
 
 // MMA issuer (one thread): per tile, K stages of A (TMEM) x B (shared
-// memory) into accumulator q = tile parity; nk_of(w) gives tile w's stages.
+// memory); nk_of(w) gives tile w's stages.  Every kseg stages of a tile form
+// one accumulation segment: a fresh accumulator (q = segment parity) that the
+// converters drain when it completes.
 template <typename T, int NC, typename NkOf>
 __device__ __forceinline__ void tc_mma_role(TcBars* b, uint32_t sbase, uint32_t tmem, int64_t nitems, NkOf nk_of,
-                                            int* err) {
+                                            int kseg, int* err) {
   using Tr = TcT<T>;
   using C = TcCfg<T, NC>;
   constexpr uint32_t LBO_B = 2 * NC * 16, SBO_B = 128;        // K-major [hi | lo] B tiles
   const uint32_t id_full = tc::idesc(Tr::FMT, 2 * NC, 0, 0);
   const uint32_t id_half = tc::idesc(Tr::FMT, NC, 0, 0);
-  uint32_t it = 0, j = 0;
+  uint32_t it = 0, j = 0;                                      // stages, segments
   bool ok = true;
   int nk = blockIdx.x < nitems ? nk_of(blockIdx.x) : 0;
-  for (int64_t w = blockIdx.x; w < nitems && ok; w += gridDim.x, ++j) {
+  for (int64_t w = blockIdx.x; w < nitems && ok; w += gridDim.x) {
     const int nk_next = w + gridDim.x < nitems ? nk_of(w + gridDim.x) : 0;   // loaded ahead of its use
-    const uint32_t q = j & 1u;
-    if (!tc_wait(b, &b->accempty[q], ((j >> 1) & 1u) ^ 1u, err, 2)) break;
-    tc::tc_fence_after();
-    const uint32_t dacc = tmem + (uint32_t)C::ACC0 + q * 2 * NC;
-    for (int kc = 0; kc < nk; ++kc, ++it) {
-      const int s = (int)(it % C::S), a = (int)(it % C::NA);
-      if (!tc_wait(b, &b->bfull[s], (it / C::S) & 1u, err, 4)) { ok = false; break; }
-      if (!tc_wait(b, &b->afull[a], (it / C::NA) & 1u, err, 4)) { ok = false; break; }
+    for (int k0 = 0; k0 < nk && ok; k0 += kseg, ++j) {
+      const int k1 = min(nk, k0 + kseg);
+      const uint32_t q = j & 1u;
+      if (!tc_wait(b, &b->accempty[q], ((j >> 1) & 1u) ^ 1u, err, 2)) { ok = false; break; }
       tc::tc_fence_after();
-      const uint32_t bbase = sbase + (uint32_t)(s * C::STAGE);
-      const uint32_t abuf = tmem + (uint32_t)(a * Tr::ACOLS);
+      const uint32_t dacc = tmem + (uint32_t)C::ACC0 + q * 2 * NC;
+      for (int kc = k0; kc < k1; ++kc, ++it) {
+        const int s = (int)(it % C::S), a = (int)(it % C::NA);
+        if (!tc_wait(b, &b->bfull[s], (it / C::S) & 1u, err, 4)) { ok = false; break; }
+        if (!tc_wait(b, &b->afull[a], (it / C::NA) & 1u, err, 4)) { ok = false; break; }
+        tc::tc_fence_after();
+        const uint32_t bbase = sbase + (uint32_t)(s * C::STAGE);
+        const uint32_t abuf = tmem + (uint32_t)(a * Tr::ACOLS);
 #pragma unroll
-      for (int ks = 0; ks < Tr::KC / Tr::KM; ++ks) {
-        const uint64_t bd = tc::smem_desc(bbase + ks * 2 * LBO_B, LBO_B, SBO_B);
-        tc::mma_ts<Tr::KIND>(dacc, abuf + ks * 8, bd, id_full, (kc > 0 || ks > 0) ? 1u : 0u);
-        if constexpr (Tr::SPLIT) tc::mma_ts<Tr::KIND>(dacc, abuf + Tr::KC + ks * 8, bd, id_half, 1u);
+        for (int ks = 0; ks < Tr::KC / Tr::KM; ++ks) {
+          const uint64_t bd = tc::smem_desc(bbase + ks * 2 * LBO_B, LBO_B, SBO_B);
+          tc::mma_ts<Tr::KIND>(dacc, abuf + ks * 8, bd, id_full, (kc > k0 || ks > 0) ? 1u : 0u);
+          if constexpr (Tr::SPLIT) tc::mma_ts<Tr::KIND>(dacc, abuf + Tr::KC + ks * 8, bd, id_half, 1u);
+        }
+        tc::mma_commit(&b->empty[s]);
+        tc::mma_commit(&b->aempty[a]);
       }
-      tc::mma_commit(&b->empty[s]);
-      tc::mma_commit(&b->aempty[a]);
+      if (ok) tc::mma_commit(&b->accfull[q]);
     }
-    if (ok) tc::mma_commit(&b->accfull[q]);
     nk = nk_next;
   }
   tc::mma_commit(&b->done);
@@ -522,7 +532,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase1_kernel(P1Args<T, NC> 
     if (pt == 0) tc_copies_drain(bars, it, C::S, a.err);
   } else if (warp == TC_MMA_WARP) {
     // ---------------- MMA issuer ----------------
-    if (lane == 0) tc_mma_role<T, NC>(bars, sbase, tmem, a.nitems, nk_of, a.err);
+    if (lane == 0) tc_mma_role<T, NC>(bars, sbase, tmem, a.nitems, nk_of, 1 << 30, a.err);   // one segment a tile
   } else if (warp < 8) {
     // ---------------- converters (thread = TMEM lane m = tile row = factor column m) + drain ----------------
     const int m = 32 * (warp & 3) + lane, h = warp >> 2;
@@ -726,7 +736,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
     tc::cp_async_wait_all();
     if (pw == 0 && lane == 0) tc_copies_drain(bars, it, C::S, a.err);
   } else if (warp == TC_MMA_WARP) {
-    if (lane == 0) tc_mma_role<T, NC>(bars, sbase, tmem, a.nitems, nk_of, a.err);
+    if (lane == 0) tc_mma_role<T, NC>(bars, sbase, tmem, a.nitems, nk_of, TC_KSEG2, a.err);
   } else if (warp < 8) {
     // ---------------- converters (thread = TMEM lane m = tile row m) + drain ----------------
     const int m = 32 * (warp & 3) + lane, h = warp >> 2;
@@ -756,32 +766,35 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
       tc::mbar_arrive(&bars->accempty[q]);
       return true;
     };
-    uint32_t it = 0, j = 0;
+    uint32_t it = 0, j = 0;                              // stages, accumulation segments
     bool stop = false, pend = false;
     TcItem2 Ip{};
     TcItem2 I = blockIdx.x < a.nitems ? a.items[blockIdx.x] : TcItem2{};
-    for (int64_t w = blockIdx.x; w < a.nitems && !stop; w += gridDim.x, ++j) {
+    for (int64_t w = blockIdx.x; w < a.nitems && !stop; w += gridDim.x) {
       const TcItem2 I2 = w + gridDim.x < a.nitems ? a.items[w + gridDim.x] : TcItem2{};
       const int nk = (int)((I.ze - (I.zb / KE) * KE + KC - 1) / KC);
-      const int kd = min(C::NA - 1, nk - 1);         // as in phase 1
-      for (int kc = 0; kc < nk; ++kc, ++it) {
-        const int s = (int)(it % C::S), ab = (int)(it % C::NA);
-        if (!tc_wait_warp(bars, &bars->full[s], (it / C::S) & 1u, a.err, 64)) { stop = true; break; }
-        if (!tc_wait_warp(bars, &bars->aempty[ab], ((it / C::NA) & 1u) ^ 1u, a.err, 64)) { stop = true; break; }
-        tc::tc_fence_after();
-        const uint8_t* rb = smem + s * C::STAGE + C::B_BYTES;
-        conv2(rb, reinterpret_cast<const int4*>(rb + C::RAW2), m, tmem + lb + (uint32_t)(ab * Tr::ACOLS), h,
-              (T*)nullptr);
-        tc::tmem_wait_st();
-        tc::tc_fence_before();
-        tc::mbar_arrive(&bars->afull[ab]);
-        if (pend && kc == kd) {
-          pend = false;
-          if (!drain(Ip, j - 1)) { stop = true; break; }
+      for (int k0 = 0; k0 < nk && !stop; k0 += TC_KSEG2, ++j) {
+        const int k1 = min(nk, k0 + TC_KSEG2);
+        const int kd = k0 + min(C::NA - 1, k1 - k0 - 1);  // as in phase 1, per segment
+        for (int kc = k0; kc < k1; ++kc, ++it) {
+          const int s = (int)(it % C::S), ab = (int)(it % C::NA);
+          if (!tc_wait_warp(bars, &bars->full[s], (it / C::S) & 1u, a.err, 64)) { stop = true; break; }
+          if (!tc_wait_warp(bars, &bars->aempty[ab], ((it / C::NA) & 1u) ^ 1u, a.err, 64)) { stop = true; break; }
+          tc::tc_fence_after();
+          const uint8_t* rb = smem + s * C::STAGE + C::B_BYTES;
+          conv2(rb, reinterpret_cast<const int4*>(rb + C::RAW2), m, tmem + lb + (uint32_t)(ab * Tr::ACOLS), h,
+                (T*)nullptr);
+          tc::tmem_wait_st();
+          tc::tc_fence_before();
+          tc::mbar_arrive(&bars->afull[ab]);
+          if (pend && kc == kd) {
+            pend = false;
+            if (!drain(Ip, j - 1)) { stop = true; break; }
+          }
         }
+        Ip = I;
+        pend = !stop;
       }
-      Ip = I;
-      pend = !stop;
       I = I2;
     }
     if (pend) drain(Ip, j - 1);

@@ -101,6 +101,19 @@ def test_tc_against_fp64_factors():
     assert H32.info().factorized == 0
 
 
+def test_tc_long_windows():
+    # at n = 2^17 a 512-row window holds about 800 Z slots: phase 2 adds its FP32
+    # accumulator into the FP64 Y every 512 slots, so the product stays near the
+    # FP32 storage level against the FP64-factor product
+    n = 1 << 17
+    _, H32 = _build("F32", "bisect", n)
+    _, H64 = _build("F64", "bisect", n)
+    X = np.random.default_rng(25).standard_normal((n, 16))
+    R = H64 * X
+    err = np.linalg.norm(H32 * X - R) / np.linalg.norm(R)
+    assert err <= 5e-6, err
+
+
 def test_tc_range_fallback():
     # factors beyond 2^100 in magnitude take the CUDA-core block kernels (the
     # converters' hi/lo split is exact only below 2^100); the check is redone
