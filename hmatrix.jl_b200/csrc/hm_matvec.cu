@@ -606,19 +606,26 @@ __global__ void __launch_bounds__(256) mvdd_phase1_kernel(const P1Desc* __restri
   }
 }
 
-// r = b - (sum over the window's leaves) per output row, one thread a row
+// r = b - (sum over the window's leaves) per output row, one thread a row; a
+// window is split over MVDD_SPLIT CTAs of MV_WROWS / MVDD_SPLIT rows (the
+// double-double sums are latency-bound: one CTA per window left most SMs idle)
+constexpr int MVDD_SPLIT = 8;
+constexpr int MVDD_ROWS = MV_WROWS / MVDD_SPLIT;
 template <typename T, typename TD>
-__global__ void __launch_bounds__(512) mvdd_phase2_kernel(const MvWin* __restrict__ win,
-                                                          const P2Desc* __restrict__ d, const T* __restrict__ rk,
-                                                          const TD* __restrict__ dn, const double* __restrict__ zh,
-                                                          const double* __restrict__ zl,
-                                                          const double* __restrict__ x,
-                                                          const double* __restrict__ bvec, double* __restrict__ rvec) {
-  const MvWin W = win[blockIdx.x];
-  for (uint32_t row = threadIdx.x; row < W.nrows; row += blockDim.x) {
+__global__ void __launch_bounds__(MVDD_ROWS) mvdd_phase2_kernel(const MvWin* __restrict__ win,
+                                                                const P2Desc* __restrict__ d, const T* __restrict__ rk,
+                                                                const TD* __restrict__ dn, const double* __restrict__ zh,
+                                                                const double* __restrict__ zl,
+                                                                const double* __restrict__ x,
+                                                                const double* __restrict__ bvec, double* __restrict__ rvec) {
+  const MvWin W = win[blockIdx.x / MVDD_SPLIT];
+  const int r0 = (int)(blockIdx.x % MVDD_SPLIT) * MVDD_ROWS;      // this CTA's rows [r0, r0 + MVDD_ROWS)
+  const uint32_t row = (uint32_t)(r0 + threadIdx.x);
+  if (row < W.nrows) {
     double p = 0.0, c = 0.0;
     for (uint32_t e = W.begin; e < W.end; ++e) {
       const P2Desc D = d[e];
+      if (D.row_off >= r0 + MVDD_ROWS || D.row_off + (int)D.m <= r0) continue;   // the whole CTA skips it
       const int lr = (int)row - D.row_off;
       if (lr < 0 || lr >= (int)D.m) continue;
       if (D.type == P2_RK) {
@@ -663,8 +670,8 @@ static int residual_t(hm_handle* h, const double* d_x, const double* d_b, double
     const int64_t blocks = std::min<int64_t>((P.np1 + 7) / 8, (int64_t)nsm * 8);
     mvdd_phase1_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(P.d_p1, P.np1, (const T*)h->d_rk, d_x, zh, zl);
   }
-  mvdd_phase2_kernel<T, TD><<<(unsigned)P.nwin, 512, 0, st>>>(P.d_win, P.d_p2, (const T*)h->d_rk,
-                                                              (const TD*)h->d_dense, zh, zl, d_x, d_b, d_r);
+  mvdd_phase2_kernel<T, TD><<<(unsigned)(P.nwin * MVDD_SPLIT), MVDD_ROWS, 0, st>>>(
+      P.d_win, P.d_p2, (const T*)h->d_rk, (const TD*)h->d_dense, zh, zl, d_x, d_b, d_r);
   HM_CUDA_TRY(cudaGetLastError());
   return HM_OK;
 }
