@@ -167,6 +167,8 @@ struct MvPlan {
   int32_t nwin = 0;
   P2Desc* d_p2d = nullptr;         // the dense descriptors alone, window by window (built on first use)
   MvWin* d_wind = nullptr;         // windows over d_p2d (nwin of them)
+  P2Desc* d_p2r = nullptr;         // the low-rank descriptors alone, window by window (built with d_p2d)
+  MvWin* d_winr = nullptr;         // windows over d_p2r
 };
 
 struct LuState;            // H-LU data (hm_lu.cu)
@@ -289,6 +291,8 @@ int matvec_multi_device(hm_handle* h, const double* d_x, double* d_y, int64_t nc
 // the low-rank part of Y = H X on the tensor cores, added into Y (hm_matvec_tc.cu)
 int matvec_multi_tc(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st);
 int tc_prepare(hm_handle* h, int trans, bool* usable);
+// Splits a plan's window lists into dense-only and low-rank-only lists (once).
+int split_p2(MvPlan& P);
 void tc_factors_changed(hm_handle* h);
 int tc_status(hm_handle* h, cudaStream_t st);
 int tc_selftest(int kind, int a_src, int nc, const float* A, const float* B, float* D);

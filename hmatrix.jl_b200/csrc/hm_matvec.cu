@@ -27,7 +27,7 @@ namespace hm {
 // ---------------------------------------------------------------------------
 template <typename T> struct MvT;
 template <> struct MvT<double> {
-  static constexpr int VW = 2, U = 4;
+  static constexpr int VW = 2, U = 4, NR = 2;       // NR: factor columns a warp streams together
   using X = double;
   using R = double2;
   struct XV { double2 a; };
@@ -39,7 +39,7 @@ template <> struct MvT<double> {
   }
 };
 template <> struct MvT<float> {
-  static constexpr int VW = 4, U = 4;
+  static constexpr int VW = 4, U = 4, NR = 2;
   using X = float;
   using R = float4;
   struct XV { float4 a; };
@@ -56,7 +56,7 @@ template <> struct MvT<float> {
 __device__ __forceinline__ float bf_lo(uint32_t w) { return __uint_as_float(w << 16); }
 __device__ __forceinline__ float bf_hi(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
 template <> struct MvT<__nv_bfloat16> {
-  static constexpr int VW = 8, U = 2;
+  static constexpr int VW = 8, U = 2, NR = 4;       // a BF16 vector is half the bytes: twice the columns
   using X = float;
   using R = uint4;
   struct XV { float4 a, b; };
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(256, HM_P1_MINB) mv_phase1_kernel(const P1Desc
                                                         int64_t xs_stride, double* __restrict__ z) {
   using Tr = MvT<T>;
   using TX = typename Tr::X;
-  constexpr int VW = Tr::VW, U = Tr::U;
+  constexpr int VW = Tr::VW, U = Tr::U, NR = Tr::NR;
   constexpr int XA = 16 / (int)sizeof(TX);
   const int lane = threadIdx.x & 31;
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -112,20 +112,25 @@ __global__ void __launch_bounds__(256, HM_P1_MINB) mv_phase1_kernel(const P1Desc
     const TX* xb = xs + q * xs_stride + D.seg0 + q;
     const int nvec = (int)(D.stride / VW);
     const T* F = pool + D.off;
-    for (int r = 0; r < D.k; r += 2) {
-      const bool two = (r + 1) < D.k;
-      const T* f0 = F + (int64_t)r * D.stride;
-      const T* f1 = two ? f0 + D.stride : f0;
-      double s0 = 0.0, s1 = 0.0;
+    for (int r = 0; r < D.k; r += NR) {
+      // NR columns r .. r + NR - 1 (those past the rank point at column r and are
+      // neither read, beyond the first two, nor written)
+      const T* fc[NR];
+#pragma unroll
+      for (int j = 0; j < NR; ++j) fc[j] = F + (int64_t)(r + j < D.k ? r + j : r) * D.stride;
+      double sc[NR];
+#pragma unroll
+      for (int j = 0; j < NR; ++j) sc[j] = 0.0;
       for (int v0 = lane; v0 < nvec; v0 += 32 * U) {
-        typename Tr::R a[U], c[U];
+        typename Tr::R a[NR][U];
         typename Tr::XV xv[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const int v = v0 + 32 * u;
           if (v < nvec) {
-            a[u] = Tr::ld(f0 + (int64_t)v * VW);
-            c[u] = Tr::ld(f1 + (int64_t)v * VW);
+#pragma unroll
+            for (int j = 0; j < NR; ++j)
+              if (j < 2 || r + j < D.k) a[j][u] = Tr::ld(fc[j] + (int64_t)v * VW);   // no reads past the rank
             xv[u] = Tr::ldx(xb + (int64_t)v * VW);
           }
         }
@@ -133,30 +138,33 @@ __global__ void __launch_bounds__(256, HM_P1_MINB) mv_phase1_kernel(const P1Desc
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             if (v0 + 32 * u < nvec) {
-              s0 = Tr::dot(a[u], xv[u], s0);
-              s1 = Tr::dot(c[u], xv[u], s1);
+#pragma unroll
+              for (int j = 0; j < NR; ++j) sc[j] = Tr::dot(a[j][u], xv[u], sc[j]);
             }
           }
         } else {
-          // FP32 products and partial sums over the U vectors in flight (16
-          // elements a lane), folded into the FP64 sums once per group
-          float f0 = 0.f, f1 = 0.f;
+          // FP32 products and partial sums over the U vectors in flight,
+          // folded into the FP64 sums once per group
+          float fp[NR];
+#pragma unroll
+          for (int j = 0; j < NR; ++j) fp[j] = 0.f;
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             if (v0 + 32 * u < nvec) {
-              f0 = Tr::dotf(a[u], xv[u], f0);
-              f1 = Tr::dotf(c[u], xv[u], f1);
+#pragma unroll
+              for (int j = 0; j < NR; ++j) fp[j] = Tr::dotf(a[j][u], xv[u], fp[j]);
             }
           }
-          s0 += (double)f0;
-          s1 += (double)f1;
+#pragma unroll
+          for (int j = 0; j < NR; ++j) sc[j] += (double)fp[j];
         }
       }
-      s0 = warp_sum(s0);
-      s1 = warp_sum(s1);
+#pragma unroll
+      for (int j = 0; j < NR; ++j) sc[j] = warp_sum(sc[j]);
       if (lane == 0) {
-        z[D.zoff + r] = s0;
-        if (two) z[D.zoff + r + 1] = s1;
+#pragma unroll
+        for (int j = 0; j < NR; ++j)
+          if (r + j < D.k) z[D.zoff + r + j] = sc[j];
       }
     }
   }
@@ -398,6 +406,8 @@ void free_mv_plan(MvPlan& p) {
   if (p.d_win) cudaFree(p.d_win);
   if (p.d_p2d) cudaFree(p.d_p2d);
   if (p.d_wind) cudaFree(p.d_wind);
+  if (p.d_p2r) cudaFree(p.d_p2r);
+  if (p.d_winr) cudaFree(p.d_winr);
   p = MvPlan{};
 }
 
@@ -502,11 +512,210 @@ static int ensure_xs(hm_handle* h, size_t bytes) {
   return HM_OK;
 }
 
+// The window lists split by leaf kind: the dense leaves alone (the passes that
+// treat them separately: tensor-core calls, BF16 single-column products) and
+// the low-rank leaves alone.
+int split_p2(MvPlan& P) {
+  if (P.d_wind || P.nwin == 0) return HM_OK;
+  std::vector<P2Desc> v((size_t)P.np2);
+  std::vector<MvWin> win((size_t)P.nwin);
+  if (P.np2 > 0) HM_CUDA_TRY(cudaMemcpy(v.data(), P.d_p2, sizeof(P2Desc) * v.size(), cudaMemcpyDeviceToHost));
+  HM_CUDA_TRY(cudaMemcpy(win.data(), P.d_win, sizeof(MvWin) * win.size(), cudaMemcpyDeviceToHost));
+  std::vector<P2Desc> dd, rr;
+  std::vector<MvWin> wd(win), wr(win);
+  for (size_t w = 0; w < win.size(); ++w) {
+    wd[w].begin = (uint32_t)dd.size();
+    wr[w].begin = (uint32_t)rr.size();
+    for (uint32_t i = win[w].begin; i < win[w].end; ++i) (v[i].type == P2_RK ? rr : dd).push_back(v[i]);
+    wd[w].end = (uint32_t)dd.size();
+    wr[w].end = (uint32_t)rr.size();
+  }
+  if (dd.empty()) dd.push_back(P2Desc{});        // keeps the pointers valid; no window refers to them
+  if (rr.empty()) rr.push_back(P2Desc{});
+  HM_CUDA_TRY(cudaMalloc(&P.d_p2r, sizeof(P2Desc) * rr.size()));
+  HM_CUDA_TRY(cudaMemcpy(P.d_p2r, rr.data(), sizeof(P2Desc) * rr.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(cudaMalloc(&P.d_winr, sizeof(MvWin) * wr.size()));
+  HM_CUDA_TRY(cudaMemcpy(P.d_winr, wr.data(), sizeof(MvWin) * wr.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(cudaMalloc(&P.d_p2d, sizeof(P2Desc) * dd.size()));
+  HM_CUDA_TRY(cudaMemcpy(P.d_p2d, dd.data(), sizeof(P2Desc) * dd.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(cudaMalloc(&P.d_wind, sizeof(MvWin) * wd.size()));   // last: marks the split as complete
+  HM_CUDA_TRY(cudaMemcpy(P.d_wind, wd.data(), sizeof(MvWin) * wd.size(), cudaMemcpyHostToDevice));
+  return HM_OK;
+}
+
+// y = the dense leaves' part of H x (one column): a warp per 32 output rows
+// walks its window's dense descriptors; the leaves covering its rows are read
+// column by column (32 consecutive rows a load, eight columns in flight).
+template <typename TD>
+__global__ void __launch_bounds__(256) mv_dense1_kernel(const MvWin* __restrict__ win, const P2Desc* __restrict__ d,
+                                                        const TD* __restrict__ dn, const double* __restrict__ x,
+                                                        int64_t nslab, double* __restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (gw >= nslab) return;
+  const int64_t grow = gw * 32;
+  const MvWin W = win[grow / MV_WROWS];
+  const int r0 = (int)(grow - W.row0), r = r0 + lane;
+  double acc = 0.0;
+  for (uint32_t i = W.begin; i < W.end; ++i) {
+    const P2Desc D = d[i];
+    if (D.row_off >= r0 + 32 || D.row_off + (int)D.m <= r0) continue;
+    const int lr = r - D.row_off;
+    const bool mine = lr >= 0 && lr < (int)D.m;
+    const bool tr = D.type == P2_DENSE_T;
+    const TD* col = dn + D.off + (mine ? (tr ? (int64_t)lr * D.ld : (int64_t)lr) : 0);
+    const int64_t cs = tr ? 1 : (int64_t)D.ld;
+    const double* xs = x + D.aux;
+    uint32_t c = 0;
+    for (; c + 8 <= D.cnt; c += 8) {
+      double v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = mine ? (double)__ldcs(col + (int64_t)(c + u) * cs) : 0.0;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc = fma(v[u], __ldg(xs + c + u), acc);
+    }
+    for (; c < D.cnt; ++c) acc = fma(mine ? (double)__ldcs(col + (int64_t)c * cs) : 0.0, __ldg(xs + c), acc);
+  }
+  if (r < (int)W.nrows) y[W.row0 + r] = acc;
+}
+
+// BF16 factors: y += the low-rank leaves' part, each lane owning 8
+// consecutive output rows (one 16-byte load of 8 BF16 values where the leaf
+// starts on an 8-row boundary of the window, two 8-byte loads on a 4-row
+// boundary, element loads elsewhere; padding rows hold zeros).  Twice the rows
+// of the 4-row kernel per entry: BF16 halves the bytes of an entry, and the
+// 4-row form ran out of issue slots before HBM.
+template <int SPLIT> struct P2Shape8 {
+  static constexpr int CROWS = MV_WROWS / SPLIT;   // rows of one CTA
+  static constexpr int WARPS = CROWS / 256;        // 32 lanes x 8 rows a warp
+  static constexpr int EMAX = 1024 / SPLIT;
+};
+template <int SPLIT>
+__global__ void __launch_bounds__(P2Shape8<SPLIT>::WARPS * 32) mv_phase2_bf16_kernel(
+    const MvWin* __restrict__ win, const P2Desc* __restrict__ d, const __nv_bfloat16* __restrict__ rk,
+    const double* __restrict__ z, double* __restrict__ y) {
+  constexpr int U = 8;
+  constexpr int CROWS = P2Shape8<SPLIT>::CROWS, EMAX = P2Shape8<SPLIT>::EMAX;
+  __shared__ P2Desc sd[P2_NB];
+  __shared__ int spre[P2_NB + 1];
+  __shared__ uint64_t e_off[EMAX];
+  __shared__ int32_t e_ro[EMAX];
+  __shared__ uint32_t e_m[EMAX];
+  __shared__ double e_z[EMAX];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const MvWin W = win[blockIdx.x / SPLIT];
+  const int h0 = (int)(blockIdx.x % SPLIT) * CROWS;
+  const int base = h0 + 8 * (warp * 32 + lane);
+  const uint16_t* rkb = reinterpret_cast<const uint16_t*>(rk);
+  double acc[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) acc[q] = 0.0;
+  for (uint32_t b0 = W.begin; b0 < W.end; b0 += P2_NB) {
+    const int nb = (int)min((uint32_t)P2_NB, W.end - b0);
+    __syncthreads();
+    if (warp == 0) {
+      int cnt = 0;
+      if (lane < nb) {
+        sd[lane] = d[b0 + lane];
+        const int r0 = sd[lane].row_off, r1 = r0 + (int)sd[lane].m;
+        cnt = (r1 > h0 && r0 < h0 + CROWS) ? (int)sd[lane].cnt : 0;
+      }
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      spre[lane + 1] = incl;
+      if (lane == 0) spre[0] = 0;
+    }
+    __syncthreads();
+    const int total = spre[nb];
+    for (int e0 = 0; e0 < total; e0 += EMAX) {
+      const int ne = min(EMAX, total - e0);
+      if (e0 > 0) __syncthreads();
+      for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+        const int ge = e0 + e;
+        int lo = 0, hi = nb - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (spre[mid] <= ge) lo = mid; else hi = mid - 1;
+        }
+        const P2Desc& D = sd[lo];
+        const int c = ge - spre[lo];
+        e_off[e] = D.off + (uint64_t)c * D.ld;
+        e_z[e] = z[D.aux + c];
+        e_ro[e] = D.row_off;
+        e_m[e] = D.m;
+      }
+      __syncthreads();
+      for (int e = 0; e < ne; e += U) {
+        uint4 raw[U];
+        double zz[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          raw[u] = make_uint4(0u, 0u, 0u, 0u);
+          zz[u] = 0.0;
+          const int ee = e + u;
+          if (ee < ne) {
+            const int ro = e_ro[ee];
+            const int mm = (int)e_m[ee];
+            const uint64_t o = e_off[ee];
+            const int lr = base - ro;
+            zz[u] = e_z[ee];
+            if ((ro & 7) == 0) {
+              if (lr >= 0 && lr < mm) raw[u] = __ldcs(reinterpret_cast<const uint4*>(rk + o + lr));
+            } else if ((ro & 3) == 0) {
+              if (lr >= 0 && lr < mm) {
+                const uint2 a = __ldcs(reinterpret_cast<const uint2*>(rk + o + lr));
+                raw[u].x = a.x; raw[u].y = a.y;
+              }
+              if (lr + 4 >= 0 && lr + 4 < mm) {
+                const uint2 b = __ldcs(reinterpret_cast<const uint2*>(rk + o + lr + 4));
+                raw[u].z = b.x; raw[u].w = b.y;
+              }
+            } else {
+              uint32_t wv[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+              for (int q = 0; q < 8; ++q) {
+                const int r = lr + q;
+                if (r >= 0 && r < mm) wv[q >> 1] |= (uint32_t)rkb[o + (uint64_t)r] << (16 * (q & 1));
+              }
+              raw[u] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+            }
+          }
+        }
+        // FP32 products and partial sums over the entries in flight, folded
+        // into the FP64 row sums once per group
+        float part[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) part[q] = 0.f;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const float zf = (float)zz[u];
+          const uint32_t w4[4] = {raw[u].x, raw[u].y, raw[u].z, raw[u].w};
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            part[2 * q] = fmaf(bf_lo(w4[q]), zf, part[2 * q]);
+            part[2 * q + 1] = fmaf(bf_hi(w4[q]), zf, part[2 * q + 1]);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[q] += (double)part[q];
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q)
+    if (base + q < (int)W.nrows) y[W.row0 + base + q] += acc[q];
+}
+
 template <typename T>
 static int matvec_t(hm_handle* h, const double* d_x, double* d_y, int trans, cudaStream_t st, cudaEvent_t* ev) {
   using TX = typename MvT<T>::X;
   constexpr int XA = 16 / (int)sizeof(TX);
-  const MvPlan& P = trans ? h->bwd : h->fwd;
+  MvPlan& P = trans ? h->bwd : h->fwd;
+  if (std::is_same<T, __nv_bfloat16>::value) HM_TRY(split_p2(P));
   const int64_t stride = pad_to(h->n + 64, 64);
   HM_TRY(ensure_xs(h, sizeof(TX) * stride * XA));
   TX* xs = (TX*)h->d_xs;
@@ -532,15 +741,28 @@ static int matvec_t(hm_handle* h, const double* d_x, double* d_y, int trans, cud
   if (ev) HM_CUDA_TRY(cudaEventRecord(ev[2], st));
   // dense leaves are FP64 with FP64 factors and FP32 otherwise
   using TD = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
-  auto p2 = [&](auto split) {
-    constexpr int S = decltype(split)::value;
-    mv_phase2_kernel<T, TD, S><<<(unsigned)(P.nwin * S), P2Shape<S>::WARPS * 32, 0, st>>>(
-        P.d_win, P.d_p2, (const T*)h->d_rk, (const TD*)h->d_dense, h->d_z, d_x, d_y);
-  };
-  switch (h->tune.p2_split) {
-    case 2: p2(std::integral_constant<int, 2>{}); break;
-    case 8: p2(std::integral_constant<int, 8>{}); break;
-    default: p2(std::integral_constant<int, 4>{});
+  if constexpr (std::is_same<T, __nv_bfloat16>::value) {
+    // dense leaves (FP32) first, written into y; then the BF16 low-rank part added
+    const int64_t nslab = (h->n + 31) / 32;
+    mv_dense1_kernel<float><<<(unsigned)((nslab + 7) / 8), 256, 0, st>>>(P.d_wind, P.d_p2d,
+                                                                         (const float*)h->d_dense, d_x, nslab, d_y);
+    if (h->tune.p2_split == 2)
+      mv_phase2_bf16_kernel<2><<<(unsigned)(P.nwin * 2), P2Shape8<2>::WARPS * 32, 0, st>>>(
+          P.d_winr, P.d_p2r, (const __nv_bfloat16*)h->d_rk, h->d_z, d_y);
+    else                                       // splits 4 and 8: one warp a quarter window
+      mv_phase2_bf16_kernel<4><<<(unsigned)(P.nwin * 4), P2Shape8<4>::WARPS * 32, 0, st>>>(
+          P.d_winr, P.d_p2r, (const __nv_bfloat16*)h->d_rk, h->d_z, d_y);
+  } else {
+    auto p2 = [&](auto split) {
+      constexpr int S = decltype(split)::value;
+      mv_phase2_kernel<T, TD, S><<<(unsigned)(P.nwin * S), P2Shape<S>::WARPS * 32, 0, st>>>(
+          P.d_win, P.d_p2, (const T*)h->d_rk, (const TD*)h->d_dense, h->d_z, d_x, d_y);
+    };
+    switch (h->tune.p2_split) {
+      case 2: p2(std::integral_constant<int, 2>{}); break;
+      case 8: p2(std::integral_constant<int, 8>{}); break;
+      default: p2(std::integral_constant<int, 4>{});
+    }
   }
   if (ev) HM_CUDA_TRY(cudaEventRecord(ev[3], st));
   HM_CUDA_TRY(cudaGetLastError());

@@ -549,30 +549,6 @@ static int ensure_sorted_p1(MvPlan& P) {
   return HM_OK;
 }
 
-// The dense-leaf descriptors alone, window by window (the tensor-core path
-// adds the low-rank part itself, so its CUDA-core pass skips those entirely).
-static int ensure_dense_p2(MvPlan& P) {
-  if (P.d_wind || P.nwin == 0) return HM_OK;
-  std::vector<P2Desc> v((size_t)P.np2);
-  std::vector<MvWin> win((size_t)P.nwin);
-  if (P.np2 > 0) HM_CUDA_TRY(cudaMemcpy(v.data(), P.d_p2, sizeof(P2Desc) * v.size(), cudaMemcpyDeviceToHost));
-  HM_CUDA_TRY(cudaMemcpy(win.data(), P.d_win, sizeof(MvWin) * win.size(), cudaMemcpyDeviceToHost));
-  std::vector<P2Desc> d;
-  for (MvWin& W : win) {
-    const uint32_t b = (uint32_t)d.size();
-    for (uint32_t i = W.begin; i < W.end; ++i)
-      if (v[i].type != P2_RK) d.push_back(v[i]);
-    W.begin = b;
-    W.end = (uint32_t)d.size();
-  }
-  if (d.empty()) d.push_back(P2Desc{});          // keeps the pointer valid; no window refers to it
-  HM_CUDA_TRY(cudaMalloc(&P.d_p2d, sizeof(P2Desc) * d.size()));
-  HM_CUDA_TRY(cudaMemcpy(P.d_p2d, d.data(), sizeof(P2Desc) * d.size(), cudaMemcpyHostToDevice));
-  HM_CUDA_TRY(cudaMalloc(&P.d_wind, sizeof(MvWin) * win.size()));
-  HM_CUDA_TRY(cudaMemcpy(P.d_wind, win.data(), sizeof(MvWin) * win.size(), cudaMemcpyHostToDevice));
-  return HM_OK;
-}
-
 template <typename T, int CB>
 int launch_multi(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, int trans, cudaStream_t st,
                  bool dense_only = false) {
@@ -603,7 +579,7 @@ int launch_multi(hm_handle* h, const double* d_x, double* d_y, int64_t ncols, in
   const int64_t nblk = (int64_t)P.nwin * 2 * ncb;
   if (nblk > (int64_t)INT32_MAX) return fail(HM_ERR_UNSUPPORTED, "too many phase-2 blocks");
   if (dense_only) {
-    HM_TRY(ensure_dense_p2(P));
+    HM_TRY(split_p2(P));
     const int64_t ntile = (h->n + 127) / 128;
     const int64_t blocks = ntile * ncb;
     if (blocks > (int64_t)INT32_MAX) return fail(HM_ERR_UNSUPPORTED, "too many dense-pass blocks");
