@@ -150,14 +150,23 @@ struct TcCfg {
   static constexpr int STAGE = (B_BYTES + RAW + 1023) / 1024 * 1024;
   static constexpr int BAR_OFF = S * STAGE;
   static constexpr int BYTES = BAR_OFF + 512;
-  // as many TMEM A buffers as fit beside the two accumulators (at most 4):
-  // the converters run up to NA stages ahead of the MMAs' completion
-  static constexpr int NA_FIT = (TC_TMEM_COLS - 2 * 2 * NC) / Tr::ACOLS;
+  // Accumulation chains: the MMAs into one accumulator run one after the
+  // other, and a chain of small MMAs (N = 2 NC) is slower than the stream of
+  // factor bytes; two independent accumulators per tile (FP32: the hi and the
+  // lo products; BF16: even and odd K steps) halve the chain, where TMEM
+  // holds them beside two A buffers.  An accumulator buffer is ACCW columns:
+  // chain 0 (2 NC) then chain 1 (NC for the lo products, 2 NC for BF16).
+  static constexpr int ACCW2 = 2 * NC + (Tr::SPLIT ? NC : 2 * NC);
+  static constexpr int NCH = 2 * Tr::ACOLS + 2 * ACCW2 <= TC_TMEM_COLS ? 2 : 1;
+  static constexpr int ACCW = NCH == 2 ? ACCW2 : 2 * NC;
+  // as many TMEM A buffers as fit beside the two accumulator buffers (at most
+  // 4): the converters run up to NA stages ahead of the MMAs' completion
+  static constexpr int NA_FIT = (TC_TMEM_COLS - 2 * ACCW) / Tr::ACOLS;
   static constexpr int NA = NA_FIT < TC_NA_MAX ? NA_FIT : TC_NA_MAX;
   static constexpr int ACC0 = NA * Tr::ACOLS;                // first accumulator column
   static_assert(NA >= 2, "two A buffers at least");
   static_assert(BYTES <= 227 * 1024, "stages exceed the shared memory of a CTA");
-  static_assert(ACC0 + 2 * 2 * NC <= TC_TMEM_COLS, "A buffers and accumulators exceed TMEM");
+  static_assert(ACC0 + 2 * ACCW <= TC_TMEM_COLS, "A buffers and accumulators exceed TMEM");
   static_assert(RS1 % 16 == 0 && RS2 % 16 == 0 && B_BYTES % 16 == 0, "bulk copies move 16-byte units");
   static_assert(KC % TC_PW == 0 && KC % Tr::KM == 0, "a stage is whole MMAs and whole producer warps");
 };
@@ -272,7 +281,7 @@ __device__ __forceinline__ void tc_mma_role(TcBars* b, uint32_t sbase, uint32_t 
       const uint32_t q = j & 1u;
       if (!tc_wait(b, &b->accempty[q], ((j >> 1) & 1u) ^ 1u, err, 2)) { ok = false; break; }
       tc::tc_fence_after();
-      const uint32_t dacc = tmem + (uint32_t)C::ACC0 + q * 2 * NC;
+      const uint32_t dacc = tmem + (uint32_t)C::ACC0 + q * C::ACCW;
       for (int kc = k0; kc < k1; ++kc, ++it) {
         const int s = (int)(it % C::S), a = (int)(it % C::NA);
         if (!tc_wait(b, &b->bfull[s], (it / C::S) & 1u, err, 4)) { ok = false; break; }
@@ -283,8 +292,19 @@ __device__ __forceinline__ void tc_mma_role(TcBars* b, uint32_t sbase, uint32_t 
 #pragma unroll
         for (int ks = 0; ks < Tr::KC / Tr::KM; ++ks) {
           const uint64_t bd = tc::smem_desc(bbase + ks * 2 * LBO_B, LBO_B, SBO_B);
-          tc::mma_ts<Tr::KIND>(dacc, abuf + ks * 8, bd, id_full, (kc > k0 || ks > 0) ? 1u : 0u);
-          if constexpr (Tr::SPLIT) tc::mma_ts<Tr::KIND>(dacc, abuf + Tr::KC + ks * 8, bd, id_half, 1u);
+          if constexpr (Tr::SPLIT) {
+            // hi products into chain 0, lo products into chain 1 (or chain 0)
+            tc::mma_ts<Tr::KIND>(dacc, abuf + ks * 8, bd, id_full, (kc > k0 || ks > 0) ? 1u : 0u);
+            if constexpr (C::NCH == 2)
+              tc::mma_ts<Tr::KIND>(dacc + 2 * NC, abuf + Tr::KC + ks * 8, bd, id_half, (kc > k0 || ks > 0) ? 1u : 0u);
+            else
+              tc::mma_ts<Tr::KIND>(dacc, abuf + Tr::KC + ks * 8, bd, id_half, 1u);
+          } else {
+            // K steps alternate between the chains
+            const uint32_t ch = C::NCH == 2 ? (uint32_t)(ks & 1) : 0u;
+            tc::mma_ts<Tr::KIND>(dacc + ch * 2 * NC, abuf + ks * 8, bd, id_full,
+                                 (kc > k0 || ks >= C::NCH) ? 1u : 0u);
+          }
         }
         tc::mma_commit(&b->empty[s]);
         tc::mma_commit(&b->aempty[a]);
@@ -347,6 +367,28 @@ template <typename T>
 __global__ void tc_zero_kernel(typename TcT<T>::Bits* __restrict__ p, int64_t cnt) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x)
     p[e] = 0;
+}
+
+// The accumulator of columns [j0, j0 + 8) of one tile row (this thread's
+// lane): the sum of the chains' partial products (tcgen05.ld, warp-wide).
+template <typename T, int NC>
+__device__ __forceinline__ void acc_load8(uint32_t ta, float (&d)[8]) {
+  using C = TcCfg<T, NC>;
+  float a[8], b[8];
+  tc::tmem_ld8(ta, a);                         // chain 0, first half: hi x X_hi (FP32) / x X_1 (BF16)
+  tc::tmem_ld8(ta + NC, b);                    // chain 0, second half: hi x X_lo / x X_2
+#pragma unroll
+  for (int i = 0; i < 8; ++i) d[i] = a[i] + b[i];
+  if constexpr (C::NCH == 2) {
+    tc::tmem_ld8(ta + 2 * NC, a);              // chain 1: lo x X_hi (FP32) / odd K steps x X_1 (BF16)
+#pragma unroll
+    for (int i = 0; i < 8; ++i) d[i] += a[i];
+    if constexpr (!TcT<T>::SPLIT) {
+      tc::tmem_ld8(ta + 3 * NC, b);            // odd K steps x X_2
+#pragma unroll
+      for (int i = 0; i < 8; ++i) d[i] += b[i];
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -547,15 +589,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase1_kernel(P1Args<T, NC> 
       tc::tc_fence_after();
 #pragma unroll 1
       for (int j0 = h * (NC / 2); j0 < (h + 1) * (NC / 2); j0 += 8) {
-        float d0[8], d1[8];
-        const uint32_t ta = tmem + lb + (uint32_t)(C::ACC0 + q * 2 * NC + j0);
-        tc::tmem_ld8(ta, d0);
-        tc::tmem_ld8(ta + NC, d1);
+        float zz[8];
+        acc_load8<T, NC>(tmem + lb + (uint32_t)(C::ACC0 + q * C::ACCW + j0), zz);
         if (valid) {
-          float zz[8];
           uint32_t zh[8], zl[8];
-#pragma unroll
-          for (int jj2 = 0; jj2 < 8; ++jj2) zz[jj2] = d0[jj2] + d1[jj2];
           tc::split_n<Tr::SIG>(zz, zh, zl);
           for (uint32_t zi = Cc.zp0; zi < Cc.zp1; ++zi) {
             const uint32_t zp = a.zpl[zi];
@@ -750,15 +787,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
       double* yr = a.Y + (int64_t)J.row0 + m;
 #pragma unroll 1
       for (int j0 = h * (NC / 2); j0 < (h + 1) * (NC / 2); j0 += 8) {
-        float d0[8], d1[8];
-        const uint32_t ta = tmem + lb + (uint32_t)(C::ACC0 + q * 2 * NC + j0);
-        tc::tmem_ld8(ta, d0);
-        tc::tmem_ld8(ta + NC, d1);
+        float dd[8];
+        acc_load8<T, NC>(tmem + lb + (uint32_t)(C::ACC0 + q * C::ACCW + j0), dd);
         if (valid) {
 #pragma unroll
           for (int jj2 = 0; jj2 < 8; ++jj2) {
             const int col = a.cb * NC + j0 + jj2;
-            if (col < a.ncols) yr[(int64_t)col * a.ldy] += (double)(d0[jj2] + d1[jj2]);
+            if (col < a.ncols) yr[(int64_t)col * a.ldy] += (double)dd[jj2];
           }
         }
       }
