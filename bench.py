@@ -759,11 +759,6 @@ def run_ours(a):
                 extra[s]["multi_rhs_tensor_cores"] = mr
             del H2
             torch.cuda.empty_cache()
-    kmeans = None
-    if not a.no_kmeans and world == 1:
-        H = None
-        torch.cuda.empty_cache()
-        kmeans = kmeans_leg(a, torch, peak)
     lu = None
     if not a.no_lu and world == 1:
         H = None
@@ -789,6 +784,14 @@ def run_ours(a):
         H = None
         torch.cuda.empty_cache()
         c4 = gradient_leg(a.c4_n, torch)
+    # the KMeans-tree matrix (180 GB of FP64 factors at n = 2^20) last: run
+    # before the H-LU legs it left the FP64 factorisation timed at twice its
+    # time in a fresh process
+    kmeans = None
+    if not a.no_kmeans and world == 1:
+        H = None
+        torch.cuda.empty_cache()
+        kmeans = kmeans_leg(a, torch, peak)
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()

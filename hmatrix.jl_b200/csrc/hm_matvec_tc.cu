@@ -98,11 +98,13 @@ constexpr int TC_NPROD = 32 * TC_PW;
 constexpr int TC_NA_MAX = 4;         // TMEM A buffers, at most
 constexpr int TC_TMEM_COLS = 512;    // one CTA per SM (shared memory), so all of TMEM
 constexpr uint32_t TC_WAIT = 1u << 22;   // polls of a bounded mbarrier wait
-// Phase 2 adds its FP32 accumulator into the FP64 Y every TC_KSEG2 stages
-// (512 Z slots for FP32 factors, 1024 for BF16): a window's K runs over every
-// leaf that touches it (thousands of terms at n = 2^20), and one FP32 sum over
-// all of them would lose accuracy as n grows.
-constexpr int TC_KSEG2 = 8;
+// Phase 2 adds its FP32 accumulator into the FP64 Y every NC / 2 stages
+// (32 NC Z slots for FP32 factors, 64 NC for BF16): a window's K runs over
+// every leaf that touches it (thousands of terms at n = 2^20), and one FP32 sum
+// over all of them would lose accuracy as n grows.  The segment grows with the
+// column block so that the Y traffic of the adds (16 NC bytes a tile row) stays
+// an eighth of the factor bytes a segment streams.
+template <int NC> constexpr int tc_kseg2() { return NC / 2; }
 
 template <typename T> struct TcT;
 template <> struct TcT<float> {
@@ -773,7 +775,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
     tc::cp_async_wait_all();
     if (pw == 0 && lane == 0) tc_copies_drain(bars, it, C::S, a.err);
   } else if (warp == TC_MMA_WARP) {
-    if (lane == 0) tc_mma_role<T, NC>(bars, sbase, tmem, a.nitems, nk_of, TC_KSEG2, a.err);
+    if (lane == 0) tc_mma_role<T, NC>(bars, sbase, tmem, a.nitems, nk_of, tc_kseg2<NC>(), a.err);
   } else if (warp < 8) {
     // ---------------- converters (thread = TMEM lane m = tile row m) + drain ----------------
     const int m = 32 * (warp & 3) + lane, h = warp >> 2;
@@ -808,8 +810,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_phase2_kernel(P2Args<T, NC> 
     for (int64_t w = blockIdx.x; w < a.nitems && !stop; w += gridDim.x) {
       const TcItem2 I2 = w + gridDim.x < a.nitems ? a.items[w + gridDim.x] : TcItem2{};
       const int nk = (int)((I.ze - (I.zb / KE) * KE + KC - 1) / KC);
-      for (int k0 = 0; k0 < nk && !stop; k0 += TC_KSEG2, ++j) {
-        const int k1 = min(nk, k0 + TC_KSEG2);
+      for (int k0 = 0; k0 < nk && !stop; k0 += tc_kseg2<NC>(), ++j) {
+        const int k1 = min(nk, k0 + tc_kseg2<NC>());
         const int kd = k0 + min(C::NA - 1, k1 - k0 - 1);  // as in phase 1, per segment
         for (int kc = k0; kc < k1; ++kc, ++it) {
           const int s = (int)(it % C::S), ab = (int)(it % C::NA);

@@ -103,8 +103,8 @@ def test_tc_against_fp64_factors():
 
 def test_tc_long_windows():
     # at n = 2^17 a 512-row window holds about 800 Z slots: phase 2 adds its FP32
-    # accumulator into the FP64 Y every 512 slots, so the product stays near the
-    # FP32 storage level against the FP64-factor product
+    # accumulator into the FP64 Y every 512 slots (16 columns), so the product
+    # stays near the FP32 storage level against the FP64-factor product
     n = 1 << 17
     _, H32 = _build("F32", "bisect", n)
     _, H64 = _build("F64", "bisect", n)
