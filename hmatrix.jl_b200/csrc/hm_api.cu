@@ -449,16 +449,21 @@ int hm_autotune(hm_handle* h, int64_t ncols, int32_t calls, double* times) {
   hm_handle::Tune keep = h->tune;
   const int splits[3] = {2, 4, 8}, waves[3] = {1, 2, 4};
   if (times)
-    for (int i = 0; i < 12; ++i) times[i] = -1.0;
+    for (int i = 0; i < 15; ++i) times[i] = -1.0;
+  auto try_shape = [&](int split, int b, int slot) -> int {
+    h->tune.p2_split = split;
+    h->tune.p1_waves = waves[b];
+    const float ms = time_calls(h, calls, [&] { return matvec_device(h, x, y, 0, h->stream); });
+    if (ms < 0) { h->tune = keep; return fail(HM_ERR_CUDA, "autotune: a timed matvec failed"); }
+    if (times) times[slot] = ms;
+    if (best < 0 || ms < best) { best = ms; keep.p2_split = split; keep.p1_waves = waves[b]; }
+    return HM_OK;
+  };
   for (int a = 0; a < 3; ++a)
-    for (int b = 0; b < 3; ++b) {
-      h->tune.p2_split = splits[a];
-      h->tune.p1_waves = waves[b];
-      const float ms = time_calls(h, calls, [&] { return matvec_device(h, x, y, 0, h->stream); });
-      if (ms < 0) { h->tune = keep; return fail(HM_ERR_CUDA, "autotune: a timed matvec failed"); }
-      if (times) times[3 * a + b] = ms;
-      if (best < 0 || ms < best) { best = ms; keep.p2_split = splits[a]; keep.p1_waves = waves[b]; }
-    }
+    for (int b = 0; b < 3; ++b) HM_TRY(try_shape(splits[a], b, 3 * a + b));
+  // phase 2 by tree clusters (FP64 and FP32 factors; BF16 factors have their own phase 2)
+  if (h->storage != HM_BF16)
+    for (int b = 0; b < 3; ++b) HM_TRY(try_shape(1, b, 12 + b));
   h->tune = keep;
   // several columns on the tensor cores: the column block
   if (ncols > 1 && (h->storage == HM_F32 || h->storage == HM_BF16)) {
@@ -479,6 +484,18 @@ int hm_autotune(hm_handle* h, int64_t ncols, int32_t calls, double* times) {
     HM_TRY(tc_status(h, h->stream));
   }
   h->tune.tuned = 1;
+  return HM_OK;
+}
+
+int hm_set_tune(hm_handle* h, int32_t p2_split, int32_t p1_waves) {
+  if (!h) return fail(HM_ERR_ARG, "invalid argument");
+  if (p2_split != 1 && p2_split != 2 && p2_split != 4 && p2_split != 8)
+    return fail(HM_ERR_ARG, "phase-2 shape must be 1, 2, 4 or 8");
+  if (p1_waves != 1 && p1_waves != 2 && p1_waves != 4) return fail(HM_ERR_ARG, "phase-1 waves must be 1, 2 or 4");
+  if (p2_split == 1 && h->storage == HM_BF16)
+    return fail(HM_ERR_UNSUPPORTED, "phase 2 by tree clusters needs FP64 or FP32 factors");
+  h->tune.p2_split = p2_split;
+  h->tune.p1_waves = p1_waves;
   return HM_OK;
 }
 

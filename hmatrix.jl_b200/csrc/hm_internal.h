@@ -169,6 +169,13 @@ struct MvPlan {
   MvWin* d_wind = nullptr;         // windows over d_p2d (nwin of them)
   P2Desc* d_p2r = nullptr;         // the low-rank descriptors alone, window by window (built with d_p2d)
   MvWin* d_winr = nullptr;         // windows over d_p2r
+  // phase 2 by tree clusters (hm_autotune's phase-2 shape 1; built on first
+  // use): a unit is a 128-row chunk of an output cluster that is some leaf's
+  // cluster, with exactly the leaves of that cluster; one warp per unit
+  bool cl_built = false;
+  P2Desc* d_cd = nullptr;          // descriptors, unit by unit (offsets moved to the chunk's first row)
+  MvWin* d_cu = nullptr;           // units: rows [row0, row0 + nrows), descriptors [begin, end)
+  std::vector<int32_t> cl_level;   // units of tree level i: [cl_level[i], cl_level[i + 1])
 };
 
 struct LuState;            // H-LU data (hm_lu.cu)
@@ -225,7 +232,7 @@ struct hm_handle {
   int64_t piv_count = 0;
 
   struct Tune {                    // launch shapes chosen by hm_autotune (hm_api.cu)
-    int p2_split = 4;              // phase-2 CTAs per 1024-row window (2, 4, 8)
+    int p2_split = 4;              // phase-2 CTAs per 1024-row window (2, 4, 8); 1: by tree clusters
     int p1_waves = 1;              // phase-1 grid in resident waves (1, 2, 4)
     int tc_nc[3] = {0, 0, 0};      // tensor-core column block for c <= 16, <= 32, > 32 (0: by c)
     int tuned = 0;

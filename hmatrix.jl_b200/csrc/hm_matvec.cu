@@ -395,6 +395,176 @@ __global__ void __launch_bounds__(P2Shape<SPLIT>::WARPS * 32) mv_phase2_kernel(c
 }
 
 // ---------------------------------------------------------------------------
+// phase 2 by tree clusters: one warp per unit (at most 128 rows of one output
+// cluster and all the leaves of that cluster), R = 1, 2 or 4 consecutive rows
+// a lane by the unit's size.  Every entry starts on the unit's first row, so a
+// lane's R values come in one aligned load (columns are padded to a multiple
+// of 4 elements and 16 bytes; values past the unit's last row are loaded but
+// never stored).  The result is added into y.
+// ---------------------------------------------------------------------------
+constexpr int CL_E = 64;       // expanded (leaf, column) entries per warp round
+constexpr int CL_WARPS = 8;
+
+template <int R> __device__ __forceinline__ void cl_ld(const double* p, double (&v)[R]) {
+  if constexpr (R == 1) {
+    v[0] = __ldcs(p);
+  } else if constexpr (R == 2) {
+    const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+    v[0] = a.x; v[1] = a.y;
+  } else {
+    const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+}
+template <int R> __device__ __forceinline__ void cl_ld(const float* p, float (&v)[R]) {
+  if constexpr (R == 1) {
+    v[0] = __ldcs(p);
+  } else if constexpr (R == 2) {
+    const float2 a = __ldcs(reinterpret_cast<const float2*>(p));
+    v[0] = a.x; v[1] = a.y;
+  } else {
+    const float4 a = __ldcs(reinterpret_cast<const float4*>(p));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  }
+}
+
+struct ClSmem {                 // one warp's staging
+  P2Desc sd[32];
+  int spre[33];
+  uint32_t e_rs[CL_E];
+  uint64_t e_off[CL_E];
+  double e_z[CL_E];
+};
+
+template <typename T, int R>
+__device__ __forceinline__ void cl_unit(const MvWin& W, const P2Desc* __restrict__ d, const T* __restrict__ rk,
+                                        const T* __restrict__ dn, const double* __restrict__ z,
+                                        const double* __restrict__ x, double* __restrict__ y, ClSmem& sm, int lane) {
+  constexpr int U0 = (sizeof(T) == 8 ? 16 : 32) / R;   // 128 bytes in flight a lane, 8 entries at most
+  constexpr int U = U0 > 8 ? 8 : U0;
+  const int base = R * lane;
+  const int nrows = (int)W.nrows;
+  const bool act = base < nrows;
+  double acc[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) acc[q] = 0.0;
+  for (uint32_t b0 = W.begin; b0 < W.end; b0 += 32) {
+    const int nb = (int)min(32u, W.end - b0);
+    __syncwarp();
+    int cnt = 0;
+    if (lane < nb) {
+      sm.sd[lane] = d[b0 + lane];
+      cnt = (int)sm.sd[lane].cnt;
+    }
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    sm.spre[lane + 1] = incl;
+    if (lane == 0) sm.spre[0] = 0;
+    __syncwarp();
+    const int total = sm.spre[nb];
+    for (int e0 = 0; e0 < total; e0 += CL_E) {
+      const int ne = min(CL_E, total - e0);
+      __syncwarp();
+      for (int e = lane; e < ne; e += 32) {
+        const int ge = e0 + e;
+        int lo = 0, hi = nb - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (sm.spre[mid] <= ge) lo = mid; else hi = mid - 1;
+        }
+        const P2Desc& D = sm.sd[lo];
+        const int c = ge - sm.spre[lo];
+        if (D.type == P2_RK) {
+          sm.e_off[e] = D.off + (uint64_t)c * D.ld;
+          sm.e_rs[e] = 1;
+          sm.e_z[e] = z[D.aux + c];
+        } else if (D.type == P2_DENSE) {
+          sm.e_off[e] = (D.off + (uint64_t)c * D.ld) | P2_DENSE_FLAG;
+          sm.e_rs[e] = 1;
+          sm.e_z[e] = x[D.aux + c];
+        } else {
+          sm.e_off[e] = (D.off + (uint64_t)c) | P2_DENSE_FLAG;
+          sm.e_rs[e] = D.ld;
+          sm.e_z[e] = x[D.aux + c];
+        }
+      }
+      __syncwarp();
+      if (!act) continue;
+      for (int e = 0; e < ne; e += U) {
+        T v[U][R];
+        T zz[U];                               // the FP32 path multiplies by z rounded to FP32
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+#pragma unroll
+          for (int q = 0; q < R; ++q) v[u][q] = T(0);
+          zz[u] = T(0);
+          const int ee = e + u;
+          if (ee < ne) {
+            const uint64_t o = sm.e_off[ee];
+            const uint32_t rs = sm.e_rs[ee];
+            const T* p = (o & P2_DENSE_FLAG) ? dn + (o & ~P2_DENSE_FLAG) : rk + o;
+            zz[u] = (T)sm.e_z[ee];
+            if (rs == 1) {
+              cl_ld<R>(p + base, v[u]);
+            } else {
+#pragma unroll
+              for (int q = 0; q < R; ++q)
+                if (base + q < nrows) v[u][q] = __ldg(p + (uint64_t)(base + q) * rs);
+            }
+          }
+        }
+        if constexpr (std::is_same<T, double>::value) {
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int q = 0; q < R; ++q) acc[q] = fma(v[u][q], zz[u], acc[q]);
+        } else {
+          // FP32 products and partial sums over the U entries in flight,
+          // folded into the FP64 row sums once per group
+          float part[R];
+#pragma unroll
+          for (int q = 0; q < R; ++q) part[q] = 0.f;
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+#pragma unroll
+            for (int q = 0; q < R; ++q) part[q] = fmaf(v[u][q], zz[u], part[q]);
+          }
+#pragma unroll
+          for (int q = 0; q < R; ++q) acc[q] += (double)part[q];
+        }
+      }
+    }
+  }
+  if (act) {
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+      if (base + q < nrows) y[W.row0 + base + q] += acc[q];
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(CL_WARPS * 32, 3) mv_phase2c_kernel(const MvWin* __restrict__ units, int nu,
+                                                                   const P2Desc* __restrict__ d,
+                                                                   const T* __restrict__ rk, const T* __restrict__ dn,
+                                                                   const double* __restrict__ z,
+                                                                   const double* __restrict__ x,
+                                                                   double* __restrict__ y) {
+  __shared__ ClSmem sm[CL_WARPS];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int u = blockIdx.x * CL_WARPS + warp;
+  if (u >= nu) return;                         // warps are independent: no block barrier follows
+  const MvWin W = units[u];
+  if (W.nrows > 64) cl_unit<T, 4>(W, d, rk, dn, z, x, y, sm[warp], lane);
+  else if (W.nrows > 32) cl_unit<T, 2>(W, d, rk, dn, z, x, y, sm[warp], lane);
+  else cl_unit<T, 1>(W, d, rk, dn, z, x, y, sm[warp], lane);
+}
+
+// ---------------------------------------------------------------------------
 // plan construction
 // ---------------------------------------------------------------------------
 void free_mv_plan(MvPlan& p) {
@@ -408,7 +578,91 @@ void free_mv_plan(MvPlan& p) {
   if (p.d_wind) cudaFree(p.d_wind);
   if (p.d_p2r) cudaFree(p.d_p2r);
   if (p.d_winr) cudaFree(p.d_winr);
+  if (p.d_cd) cudaFree(p.d_cd);
+  if (p.d_cu) cudaFree(p.d_cu);
   p = MvPlan{};
+}
+
+// Phase 2 by tree clusters (MvPlan::cl_*).  The leaves are grouped by their
+// output cluster (the row cluster for H*x, the column cluster for H'*x) and the
+// cluster is cut into 128-row units, so every entry of a unit covers all the
+// unit's rows from its first: each lane's rows come in one aligned vector load
+// wherever the cluster boundaries fall.  Units of one tree level are disjoint;
+// the levels run one launch after another and add into y.  z offsets follow
+// the pool order of the low-rank leaves, as in build_mv_descriptors.
+constexpr int CL_ROWS = 128;                   // rows of a unit at most (32 lanes x 4 rows)
+static int build_cluster_plan(hm_handle* h, int trans, MvPlan& P) {
+  const int eb = elem_bytes(h->storage), deb = dense_elem_bytes(h->storage);
+  std::vector<int64_t> rk;                       // low-rank leaves in pool order
+  for (size_t i = 0; i < h->leaves.size(); ++i)
+    if (h->leaves[i].type == T_RK) rk.push_back((int64_t)i);
+  std::stable_sort(rk.begin(), rk.end(), [&](int64_t a, int64_t b) { return h->leaves[a].off < h->leaves[b].off; });
+  std::vector<uint32_t> zoff(h->leaves.size(), 0);
+  int64_t z = 0;
+  for (int64_t li : rk) { zoff[li] = (uint32_t)z; z += h->leaves[li].k; }
+  const int64_t ncl = (int64_t)h->cl_s.size();
+  std::vector<std::vector<int64_t>> by(ncl);     // leaves by output cluster
+  int32_t maxdepth = 0;
+  for (size_t i = 0; i < h->leaves.size(); ++i) {
+    const Leaf& L = h->leaves[i];
+    if (L.type == T_RK && L.k == 0) continue;
+    const int32_t c = trans ? L.t : L.s;
+    by[c].push_back((int64_t)i);
+    maxdepth = std::max(maxdepth, h->cl_depth[c]);
+  }
+  std::vector<std::vector<int64_t>> lev(maxdepth + 1);   // clusters by tree level, in row order
+  for (int64_t c = 0; c < ncl; ++c)
+    if (!by[c].empty()) lev[h->cl_depth[c]].push_back(c);
+  for (auto& v : lev)
+    std::sort(v.begin(), v.end(), [&](int64_t a, int64_t b) { return h->cl_s[a] < h->cl_s[b]; });
+  std::vector<P2Desc> d;
+  std::vector<MvWin> w;
+  P.cl_level.assign(1, 0);
+  for (int32_t l = maxdepth; l >= 0; --l) {
+    for (int64_t c : lev[l]) {
+      const int64_t c0 = h->cl_s[c], m = h->cl_e[c] - h->cl_s[c];
+      for (int64_t r0 = 0; r0 < m; r0 += CL_ROWS) {
+        MvWin W{};
+        W.row0 = (uint32_t)(c0 + r0);
+        W.nrows = (uint32_t)std::min<int64_t>(CL_ROWS, m - r0);
+        W.begin = (uint32_t)d.size();
+        for (int64_t li : by[c]) {
+          const Leaf& L = h->leaves[li];
+          const int64_t npad = col_pad(L.n, eb), mpad = col_pad(L.m, eb);
+          P2Desc D{};
+          D.m = W.nrows;
+          if (L.type == T_RK) {
+            D.type = P2_RK;
+            D.off = (trans ? L.off : L.off + npad * L.k) + r0;
+            D.ld = (uint32_t)(trans ? npad : mpad);
+            D.aux = zoff[li];
+            D.cnt = (uint32_t)L.k;
+          } else {
+            const int64_t ldc = col_pad(L.m, deb);
+            D.type = trans ? P2_DENSE_T : P2_DENSE;
+            D.off = L.off + (trans ? r0 * ldc : r0);
+            D.ld = (uint32_t)ldc;
+            D.aux = (uint32_t)(trans ? L.row0 : L.col0);
+            D.cnt = (uint32_t)(trans ? L.m : L.n);
+          }
+          d.push_back(D);
+        }
+        W.end = (uint32_t)d.size();
+        w.push_back(W);
+      }
+    }
+    P.cl_level.push_back((int32_t)w.size());
+  }
+  if (d.size() > (size_t)UINT32_MAX || w.size() > (size_t)INT32_MAX)
+    return fail(HM_ERR_UNSUPPORTED, "too many cluster descriptors");
+  if (d.empty()) d.push_back(P2Desc{});
+  if (w.empty()) w.push_back(MvWin{});
+  HM_CUDA_TRY(cudaMalloc(&P.d_cd, sizeof(P2Desc) * d.size()));
+  HM_CUDA_TRY(cudaMemcpy(P.d_cd, d.data(), sizeof(P2Desc) * d.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(cudaMalloc(&P.d_cu, sizeof(MvWin) * w.size()));
+  HM_CUDA_TRY(cudaMemcpy(P.d_cu, w.data(), sizeof(MvWin) * w.size(), cudaMemcpyHostToDevice));
+  P.cl_built = true;
+  return HM_OK;
 }
 
 int build_mv_descriptors(hm_handle* h, const std::vector<int64_t>& order, int trans) {
@@ -752,6 +1006,15 @@ static int matvec_t(hm_handle* h, const double* d_x, double* d_y, int trans, cud
     else                                       // splits 4 and 8: one warp a quarter window
       mv_phase2_bf16_kernel<4><<<(unsigned)(P.nwin * 4), P2Shape8<4>::WARPS * 32, 0, st>>>(
           P.d_winr, P.d_p2r, (const __nv_bfloat16*)h->d_rk, h->d_z, d_y);
+  } else if (h->tune.p2_split == 1) {
+    if (!P.cl_built) HM_TRY(build_cluster_plan(h, trans, P));
+    HM_CUDA_TRY(cudaMemsetAsync(d_y, 0, sizeof(double) * h->n, st));
+    for (size_t l = 0; l + 1 < P.cl_level.size(); ++l) {
+      const int u0 = P.cl_level[l], nu = P.cl_level[l + 1] - u0;
+      if (nu == 0) continue;
+      mv_phase2c_kernel<T><<<(unsigned)((nu + CL_WARPS - 1) / CL_WARPS), CL_WARPS * 32, 0, st>>>(
+          P.d_cu + u0, nu, P.d_cd, (const T*)h->d_rk, (const T*)h->d_dense, h->d_z, d_x, d_y);
+    }
   } else {
     auto p2 = [&](auto split) {
       constexpr int S = decltype(split)::value;

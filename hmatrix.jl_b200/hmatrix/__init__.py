@@ -214,12 +214,15 @@ class Hmat:
     def autotune(self, ncols=1, calls=5):
         """Choose the matvec launch shapes on this H-matrix's own data
         (hm_autotune); returns the timing table {name: ms} and the choice."""
-        t = np.zeros(12)
+        t = np.zeros(15)
         check(lib().hm_autotune(self._h, int(ncols), int(calls), _ptr(t)))
         table = {}
         for a, sp in enumerate((2, 4, 8)):
             for b, wv in enumerate((1, 2, 4)):
                 table["split%d_waves%d" % (sp, wv)] = float(t[3 * a + b])
+        for b, wv in enumerate((1, 2, 4)):
+            if t[12 + b] >= 0:
+                table["clusters_waves%d" % wv] = float(t[12 + b])
         for q, nc in enumerate((16, 32, 64)):
             if t[9 + q] >= 0:
                 table["tc_nc%d_cols%d" % (nc, ncols)] = float(t[9 + q])
@@ -227,6 +230,11 @@ class Hmat:
         choice = {"p2_split": o.tune_p2_split, "p1_waves": o.tune_p1_waves,
                   "tc_nc": [int(v) for v in o.tune_tc_nc]}
         return table, choice
+
+    def set_tune(self, p2_split, p1_waves=1):
+        """Pin the single-column matvec launch shapes (hm_set_tune): p2_split
+        2, 4 or 8 CTAs per phase-2 window, or 1 for phase 2 by tree clusters."""
+        check(lib().hm_set_tune(self._h, int(p2_split), int(p1_waves)))
 
     def residual(self, x, b, trans=False):
         """b - H x (b - H' x) summed in twice the FP64 precision (hm_residual):

@@ -33,7 +33,7 @@ STATUS_NAMES = {
 # every symbol include/hmatrix_b200.h declares
 EXPORTED = [
     "hm_version", "hm_last_error", "hm_default_params", "hm_new", "hm_new_like", "hm_partition", "hm_destroy", "hm_info",
-    "hm_leaves", "hm_leaf_factors", "hm_to_dense", "hm_matvec", "hm_autotune", "hm_residual", "hm_status", "hm_tc_selftest", "hm_matvec_profile", "hm_exact_rows",
+    "hm_leaves", "hm_leaf_factors", "hm_to_dense", "hm_matvec", "hm_autotune", "hm_set_tune", "hm_residual", "hm_status", "hm_tc_selftest", "hm_matvec_profile", "hm_exact_rows",
     "hm_add_identity", "hm_scale", "hm_copy", "hm_coarsen", "hm_add", "hm_save", "hm_load", "hm_load_user", "hm_lu", "hm_lu_perm", "hm_solve", "hm_solve_refined",
     "hm_batch_lu", "hm_batch_solve", "hm_batch_solve_refined", "hm_batch_matvec",
     "aca_wrapper",
@@ -99,6 +99,7 @@ def lib():
     L.hm_matvec.argtypes = [vp, vp, vp, C.c_int64, C.c_int32, C.c_uint32, vp]
     L.hm_status.argtypes = [vp, vp]
     L.hm_autotune.argtypes = [vp, C.c_int64, C.c_int32, vp]
+    L.hm_set_tune.argtypes = [vp, C.c_int32, C.c_int32]
     L.hm_residual.argtypes = [vp, vp, vp, vp, C.c_int64, C.c_int32, C.c_uint32, vp]
     L.hm_tc_selftest.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, vp, vp]
     L.hm_matvec_profile.argtypes = [vp, vp, vp, C.c_int32, vp, C.POINTER(C.c_float)]

@@ -122,7 +122,8 @@ typedef struct hm_info_t {
     int64_t lu_tiles;         /* after lu!: tiles of the tile schedule (0: the recursion ran) */
     int64_t lu_rank_cap;      /* after lu!: column capacity of the low-rank factors */
     int64_t tune_p2_split;    /* launch shapes of the matvec (hm_autotune): CTAs per
-                                 1024-row window of phase 2 (2, 4, 8)             */
+                                 1024-row window of phase 2 (2, 4, 8), or 1 for
+                                 phase 2 by tree clusters                          */
     int64_t tune_p1_waves;    /* phase-1 grid in resident waves (1, 2, 4)       */
     int64_t tune_tc_nc[3];    /* tensor-core column block for <= 16, <= 32 and
                                  more columns (0: not tuned, the default rule)    */
@@ -212,14 +213,24 @@ int hm_matvec(hm_handle* h, const double* X, double* Y, int64_t ncols,
 
 /* Autotuner of the matvec launch shapes on this handle's own data: times
  * `calls` matvecs (CUDA events, after two untimed ones) for every phase-2
- * split (2, 4, 8 CTAs per window) and phase-1 grid (1, 2, 4 resident waves)
- * and keeps the fastest; with ncols > 1 and FP32/BF16 factors, also the
- * tensor-core column block (16, 32, 64) for that many columns.  The choice
- * stays with the handle (hm_info reports it).  times (may be NULL) receives 12
- * mean milliseconds: [3 a + b] for split (2, 4, 8)[a] and waves (1, 2, 4)[b],
- * [9 + q] for column block (16, 32, 64)[q] (-1: not tried).  No counterpart in
- * the reference. */
+ * shape (2, 4, 8 CTAs per 1024-row window, or, with FP64/FP32 factors, one
+ * warp per 128-row chunk of an output cluster, tree level by tree level) and
+ * phase-1 grid (1, 2, 4 resident waves) and keeps the fastest; with ncols > 1
+ * and FP32/BF16 factors, also the tensor-core column block (16, 32, 64) for
+ * that many columns.  The choice stays with the handle (hm_info reports it).
+ * The window shapes give bit-identical results; the cluster shape sums the
+ * same products in another order.  times (may be NULL) receives 15 mean
+ * milliseconds: [3 a + b] for split (2, 4, 8)[a] and waves (1, 2, 4)[b],
+ * [9 + q] for column block (16, 32, 64)[q], [12 + b] for the cluster shape and
+ * waves (1, 2, 4)[b] (-1: not tried).  No counterpart in the reference. */
 int hm_autotune(hm_handle* h, int64_t ncols, int32_t calls, double* times);
+
+/* Sets the single-column matvec launch shapes by hand (a choice hm_autotune
+ * made earlier on the same data, say): p2_split 2, 4 or 8 CTAs per phase-2
+ * window, or 1 for phase 2 by tree clusters (not with BF16 factors:
+ * HM_ERR_UNSUPPORTED); p1_waves 1, 2 or 4.  Other values: HM_ERR_ARG.  No
+ * counterpart in the reference. */
+int hm_set_tune(hm_handle* h, int32_t p2_split, int32_t p1_waves);
 
 /* Waits for `stream` (NULL: the handle's stream) and reports, once, whether a
  * bounded wait inside the tensor-core kernels gave up since the last check
