@@ -446,6 +446,16 @@ int build_matvec_plans(hm_handle* h) {
   }
   HM_TRY(build_mv_descriptors(h, order, /*trans=*/0));
   HM_TRY(build_mv_descriptors(h, order, /*trans=*/1));
+  // phase-2 shape until hm_autotune: row windows when every leaf starts on a
+  // 64-row boundary (bisection of 2^k points), where a window's leaves tile it
+  // in aligned pieces; otherwise (KMeans trees, other sizes) by tree clusters,
+  // which keeps every load aligned and every lane busy whatever the
+  // boundaries (BF16 factors have their own phase 2)
+  if (!h->tune.tuned) {
+    bool aligned = true;
+    for (const Leaf& L : h->leaves) aligned = aligned && (L.row0 % 64 == 0) && (L.col0 % 64 == 0);
+    h->tune.p2_split = (aligned || h->storage == HM_BF16) ? 4 : 1;
+  }
   return HM_OK;
 }
 

@@ -30,6 +30,15 @@ cudaError_t smem_attr(const void* kernel, int bytes);
                                          cudaGetErrorString(_e));              \
   } while (0)
 
+// Host -> device copy of pageable memory that has landed when it returns.  A
+// pageable cudaMemcpy may return with its DMA still in flight on the legacy
+// stream, which the handle's non-blocking streams do not wait for; plans and
+// tables uploaded this way are read by kernels on those streams right after.
+inline cudaError_t h2d_sync(void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(cudaStreamLegacy);
+}
+
 #define HM_TRY(expr)                                                           \
   do {                                                                         \
     int _s = (expr);                                                           \

@@ -658,9 +658,9 @@ static int build_cluster_plan(hm_handle* h, int trans, MvPlan& P) {
   if (d.empty()) d.push_back(P2Desc{});
   if (w.empty()) w.push_back(MvWin{});
   HM_CUDA_TRY(cudaMalloc(&P.d_cd, sizeof(P2Desc) * d.size()));
-  HM_CUDA_TRY(cudaMemcpy(P.d_cd, d.data(), sizeof(P2Desc) * d.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(h2d_sync(P.d_cd, d.data(), sizeof(P2Desc) * d.size()));
   HM_CUDA_TRY(cudaMalloc(&P.d_cu, sizeof(MvWin) * w.size()));
-  HM_CUDA_TRY(cudaMemcpy(P.d_cu, w.data(), sizeof(MvWin) * w.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(h2d_sync(P.d_cu, w.data(), sizeof(MvWin) * w.size()));
   P.cl_built = true;
   return HM_OK;
 }
@@ -742,14 +742,14 @@ int build_mv_descriptors(hm_handle* h, const std::vector<int64_t>& order, int tr
   P.nwin = (int32_t)nwin;
   if (!p1.empty()) {
     HM_CUDA_TRY(cudaMalloc(&P.d_p1, sizeof(P1Desc) * p1.size()));
-    HM_CUDA_TRY(cudaMemcpy(P.d_p1, p1.data(), sizeof(P1Desc) * p1.size(), cudaMemcpyHostToDevice));
+    HM_CUDA_TRY(h2d_sync(P.d_p1, p1.data(), sizeof(P1Desc) * p1.size()));
   }
   if (!p2.empty()) {
     HM_CUDA_TRY(cudaMalloc(&P.d_p2, sizeof(P2Desc) * p2.size()));
-    HM_CUDA_TRY(cudaMemcpy(P.d_p2, p2.data(), sizeof(P2Desc) * p2.size(), cudaMemcpyHostToDevice));
+    HM_CUDA_TRY(h2d_sync(P.d_p2, p2.data(), sizeof(P2Desc) * p2.size()));
   }
   HM_CUDA_TRY(cudaMalloc(&P.d_win, sizeof(MvWin) * nwin));
-  HM_CUDA_TRY(cudaMemcpy(P.d_win, wins.data(), sizeof(MvWin) * nwin, cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(h2d_sync(P.d_win, wins.data(), sizeof(MvWin) * nwin));
   return HM_OK;
 }
 
@@ -787,13 +787,13 @@ int split_p2(MvPlan& P) {
   if (dd.empty()) dd.push_back(P2Desc{});        // keeps the pointers valid; no window refers to them
   if (rr.empty()) rr.push_back(P2Desc{});
   HM_CUDA_TRY(cudaMalloc(&P.d_p2r, sizeof(P2Desc) * rr.size()));
-  HM_CUDA_TRY(cudaMemcpy(P.d_p2r, rr.data(), sizeof(P2Desc) * rr.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(h2d_sync(P.d_p2r, rr.data(), sizeof(P2Desc) * rr.size()));
   HM_CUDA_TRY(cudaMalloc(&P.d_winr, sizeof(MvWin) * wr.size()));
-  HM_CUDA_TRY(cudaMemcpy(P.d_winr, wr.data(), sizeof(MvWin) * wr.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(h2d_sync(P.d_winr, wr.data(), sizeof(MvWin) * wr.size()));
   HM_CUDA_TRY(cudaMalloc(&P.d_p2d, sizeof(P2Desc) * dd.size()));
-  HM_CUDA_TRY(cudaMemcpy(P.d_p2d, dd.data(), sizeof(P2Desc) * dd.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(h2d_sync(P.d_p2d, dd.data(), sizeof(P2Desc) * dd.size()));
   HM_CUDA_TRY(cudaMalloc(&P.d_wind, sizeof(MvWin) * wd.size()));   // last: marks the split as complete
-  HM_CUDA_TRY(cudaMemcpy(P.d_wind, wd.data(), sizeof(MvWin) * wd.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(h2d_sync(P.d_wind, wd.data(), sizeof(MvWin) * wd.size()));
   return HM_OK;
 }
 
@@ -1304,9 +1304,9 @@ int apply_shift(hm_handle* h, double lam) {
     HM_CUDA_TRY(cudaMalloc(&d_o, 8 * offs.size()));
     HM_CUDA_TRY(cudaMalloc(&d_m, 4 * ms.size()));
     HM_CUDA_TRY(cudaMalloc(&d_l, 4 * lds.size()));
-    HM_CUDA_TRY(cudaMemcpy(d_o, offs.data(), 8 * offs.size(), cudaMemcpyHostToDevice));
-    HM_CUDA_TRY(cudaMemcpy(d_m, ms.data(), 4 * ms.size(), cudaMemcpyHostToDevice));
-    HM_CUDA_TRY(cudaMemcpy(d_l, lds.data(), 4 * lds.size(), cudaMemcpyHostToDevice));
+    HM_CUDA_TRY(h2d_sync(d_o, offs.data(), 8 * offs.size()));
+    HM_CUDA_TRY(h2d_sync(d_m, ms.data(), 4 * ms.size()));
+    HM_CUDA_TRY(h2d_sync(d_l, lds.data(), 4 * lds.size()));
     if (h->storage == HM_F64)
       shift_kernel<double><<<(unsigned)offs.size(), 128, 0, h->stream>>>(d_o, d_m, (int)offs.size(), d_l, (double*)h->d_dense, lam);
     else
@@ -1364,7 +1364,12 @@ int copy_handle(const hm_handle* h, hm_handle** out) {
   c->cl_depth = h->cl_depth; c->nodes = h->nodes; c->leaves = h->leaves; c->depth = h->depth;
   c->storage = h->storage; c->kmax = h->kmax; c->rk_bytes = h->rk_bytes; c->dense_bytes = h->dense_bytes;
   c->zlen = h->zlen;
-  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  c->tune = h->tune;                           // the same launch shapes: the same sums in the same order
+  // h's pending work lands before the copies read it (they run on the legacy
+  // stream, which the handles' non-blocking streams do not order with)
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) { delete c; return fail(HM_ERR_CUDA, cudaGetErrorString(e)); }
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete c; return fail(HM_ERR_CUDA, cudaGetErrorString(e)); }
   int s = HM_OK;
   auto chk = [&](int st) { if (s == HM_OK) s = st; };
@@ -1384,6 +1389,8 @@ int copy_handle(const hm_handle* h, hm_handle** out) {
   }
   if (s == HM_OK && h->lu) s = lu_copy(h, c);
   c->factorized = h->factorized;
+  // and the copies land before c's kernels read them
+  if (s == HM_OK && cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess) s = fail(HM_ERR_CUDA, "copy");
   if (s != HM_OK) {
     free_handle_data(c);
     cudaStreamDestroy(c->stream);

@@ -541,11 +541,11 @@ static int ensure_sorted_p1(MvPlan& P) {
   P.maxlen1 = maxlen;
   tk.push_back((uint32_t)v.size());
   HM_CUDA_TRY(cudaMalloc(&P.d_t1s, sizeof(uint32_t) * tk.size()));
-  HM_CUDA_TRY(cudaMemcpy(P.d_t1s, tk.data(), sizeof(uint32_t) * tk.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(h2d_sync(P.d_t1s, tk.data(), sizeof(uint32_t) * tk.size()));
   HM_CUDA_TRY(cudaMalloc(&P.d_p1s, sizeof(P1Desc) * v.size()));
-  HM_CUDA_TRY(cudaMemcpy(P.d_p1s, v.data(), sizeof(P1Desc) * v.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(h2d_sync(P.d_p1s, v.data(), sizeof(P1Desc) * v.size()));
   HM_CUDA_TRY(cudaMalloc(&P.d_g1s, sizeof(uint32_t) * g.size()));
-  HM_CUDA_TRY(cudaMemcpy(P.d_g1s, g.data(), sizeof(uint32_t) * g.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(h2d_sync(P.d_g1s, g.data(), sizeof(uint32_t) * g.size()));
   return HM_OK;
 }
 

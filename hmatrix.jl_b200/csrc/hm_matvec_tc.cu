@@ -1002,7 +1002,7 @@ static int upload_vec(V** d, const std::vector<V>& v) {
   if (v.empty()) return HM_OK;
   cudaError_t e = cudaMalloc((void**)d, sizeof(V) * v.size());
   if (e != cudaSuccess) return fail(HM_ERR_OOM, std::string("tensor-core matvec plan: ") + cudaGetErrorString(e));
-  HM_CUDA_TRY(cudaMemcpy(*d, v.data(), sizeof(V) * v.size(), cudaMemcpyHostToDevice));
+  HM_CUDA_TRY(h2d_sync(*d, v.data(), sizeof(V) * v.size()));
   return HM_OK;
 }
 
