@@ -38,11 +38,20 @@ static __device__ void cgs2_qr(TS* X, int len, int ld, int r, TS* Rm /* r x r, c
         xj[t] -= s;
       }
       if (threadIdx.x < j) Rm[threadIdx.x + j * r] += proj[threadIdx.x];
-      __syncthreads();
+      // after the second pass no barrier: the norm reads only this thread's
+      // rows, and proj is rewritten only after the norm's barrier
+      if (pass == 0) __syncthreads();
     }
     TS ss = 0;
     for (int t = threadIdx.x; t < len; t += blockDim.x) ss = fma(xj[t], xj[t], ss);
-    const TS nrm = sqrt((TS)block_sum((double)ss, red));
+    // block_sum without its leading barrier: red was last read before the
+    // previous column's closing barrier
+    double sd = warp_sum((double)ss);
+    if (lane == 0) red[w] = sd;
+    __syncthreads();
+    sd = 0.0;
+    for (int q = 0; q < ((blockDim.x + 31) >> 5); ++q) sd += red[q];
+    const TS nrm = sqrt((TS)sd);
     const TS inv = nrm > (TS)0 ? (TS)1 / nrm : (TS)0;
     for (int t = threadIdx.x; t < len; t += blockDim.x) xj[t] *= inv;
     if (threadIdx.x == 0) Rm[j + j * r] = nrm;
@@ -51,15 +60,20 @@ static __device__ void cgs2_qr(TS* X, int len, int ld, int r, TS* Rm /* r x r, c
 }
 
 static __device__ void zero_cols(double* X, int len, int64_t ld, int c0, int c1) {
-  for (int64_t e = threadIdx.x; e < (int64_t)len * (c1 - c0); e += blockDim.x)
-    X[(e % len) + (int64_t)(c0 + e / len) * ld] = 0.0;
+  for (int c = c0; c < c1; ++c)
+    for (int i = threadIdx.x; i < len; i += blockDim.x) X[i + (int64_t)c * ld] = 0.0;
 }
 
 // TS: the working precision (double; float for a loose truncation, where
 // FP32 Gram-Schmidt and Jacobi keep far more accuracy than the truncation
 // discards).  A, B: the tall factors (in TS), J's other fields as for
 // core_body; the new factors are written in FP64.
-template <typename TS>
+// JAC8 (the H-LU tile kernel): Jacobi rounds with 8 lanes per column pair, so
+// a round's pairs run at once instead of one after another per warp, and the
+// singular values ordered by a parallel rank count instead of one thread's
+// selection sort.  The rotations and the order are the same; only the order
+// of the sums in the dot products differs.
+template <typename TS, bool JAC8 = false>
 static __device__ void core_body_t(const CoreJob& J, TS* __restrict__ JA, TS* __restrict__ JB, int rmax,
                                    double eps_trunc, int* __restrict__ flags) {
   extern __shared__ double sm_raw[];
@@ -152,9 +166,55 @@ static __device__ void core_body_t(const CoreJob& J, TS* __restrict__ JA, TS* __
     if (threadIdx.x == 0) s_rot = 0;
     __syncthreads();
     for (int round = 0; round < rr - 1; ++round) {
+      // tournament pairing: position 0 fixed, others rotate
+      auto posv = [&](int q) { return q == 0 ? 0 : 1 + (q - 1 + round) % (rr - 1); };
+      if constexpr (JAC8) {
+        // 8 lanes per pair (4 pairs a warp at once, rows strided by 8): a
+        // round's pairs run concurrently instead of one after another per warp
+        const int sg = lane >> 3, sl = lane & 7;
+        for (int base = w * 4; base < rr / 2; base += nw * 4) {
+          const int pidx = base + sg;
+          int p = 0, q = 0;
+          bool act = pidx < rr / 2;
+          if (act) {
+            p = posv(pidx); q = posv(rr - 1 - pidx);
+            if (p > q) { int t = p; p = q; q = t; }
+            act = q < r;
+          }
+          TS* wp = b2 + p * r;
+          TS* wq = b2 + q * r;
+          TS al = 0, be = 0, ga = 0;
+          if (act)
+            for (int t = sl; t < r; t += 8) {
+              al = fma(wp[t], wp[t], al);
+              be = fma(wq[t], wq[t], be);
+              ga = fma(wp[t], wq[t], ga);
+            }
+#pragma unroll
+          for (int o = 4; o > 0; o >>= 1) {
+            al += __shfl_xor_sync(0xffffffffu, al, o);
+            be += __shfl_xor_sync(0xffffffffu, be, o);
+            ga += __shfl_xor_sync(0xffffffffu, ga, o);
+          }
+          if (act && ga != (TS)0 && fabs(ga) > thr * sqrt(al * be)) {
+            const TS zeta = (be - al) / ((TS)2 * ga);
+            const TS t = (zeta >= (TS)0 ? (TS)1 : (TS)-1) / (fabs(zeta) + sqrt((TS)1 + zeta * zeta));
+            const TS c = (TS)1 / sqrt((TS)1 + t * t), s = c * t;
+            TS* vp = b0 + p * r;
+            TS* vq = b0 + q * r;
+            for (int t2 = sl; t2 < r; t2 += 8) {
+              const TS x = wp[t2], y = wq[t2];
+              wp[t2] = c * x - s * y;
+              wq[t2] = s * x + c * y;
+              const TS u = vp[t2], v = vq[t2];
+              vp[t2] = c * u - s * v;
+              vq[t2] = s * u + c * v;
+            }
+            if (sl == 0) atomicAdd(&s_rot, 1);
+          }
+        }
+      } else {
       for (int pidx = w; pidx < rr / 2; pidx += nw) {
-        // tournament pairing: position 0 fixed, others rotate
-        auto posv = [&](int q) { return q == 0 ? 0 : 1 + (q - 1 + round) % (rr - 1); };
         int p = posv(pidx), q = posv(rr - 1 - pidx);
         if (p > q) { int t = p; p = q; q = t; }
         if (q >= r) continue;
@@ -184,6 +244,7 @@ static __device__ void core_body_t(const CoreJob& J, TS* __restrict__ JA, TS* __
           if (lane == 0) atomicAdd(&s_rot, 1);
         }
       }
+      }
       __syncthreads();
     }
     if (s_rot == 0) break;
@@ -197,7 +258,25 @@ static __device__ void core_body_t(const CoreJob& J, TS* __restrict__ JA, TS* __
     if (lane == 0) sig[j] = sqrt(s);
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if constexpr (JAC8) {
+    // the same stable descending order in parallel (r <= RCORE_MAX < 128
+    // threads): column j goes to the place of the values above it and of the
+    // equal values before it; ord starts as the identity, so every entry
+    // stays a valid column even if a non-finite value breaks the order.  k:
+    // on the sorted values the findlast below is the count of ratios > eps.
+    if ((int)threadIdx.x < r) ord[threadIdx.x] = threadIdx.x;
+    __syncthreads();
+    if ((int)threadIdx.x < r) {
+      const TS sj = sig[threadIdx.x];
+      int pos = 0;
+      for (int c = 0; c < r; ++c) pos += (sig[c] > sj) || (sig[c] == sj && c < (int)threadIdx.x);
+      if (pos < r) ord[pos] = threadIdx.x;
+    }
+    __syncthreads();
+    const double s1 = sig[ord[0]];
+    const int kc = __syncthreads_count((int)threadIdx.x < r && (double)sig[threadIdx.x] / s1 > eps_trunc);
+    if (threadIdx.x == 0) s_k = (s1 > 0.0) ? kc : 0;
+  } else if (threadIdx.x == 0) {
     for (int j = 0; j < r; ++j) ord[j] = j;
     for (int a = 0; a < r; ++a) {             // stable selection sort, descending
       int b = a;
@@ -235,18 +314,19 @@ static __device__ void core_body_t(const CoreJob& J, TS* __restrict__ JA, TS* __
     b2[e] = b0[j + o * r] * sig[o];
   }
   __syncthreads();
-  for (int64_t e = threadIdx.x; e < (int64_t)J.m * k; e += blockDim.x) {
-    const int i = (int)(e % J.m), c = (int)(e / J.m);
-    TS s = 0;
-    for (int j = 0; j < r; ++j) s = fma(JA[i + (int64_t)j * J.lda], b1[j + c * r], s);
-    J.outA[i + (int64_t)c * J.ldoa] = (double)s;
-  }
-  for (int64_t e = threadIdx.x; e < (int64_t)J.n * k; e += blockDim.x) {
-    const int i = (int)(e % J.n), c = (int)(e / J.n);
-    TS s = 0;
-    for (int j = 0; j < r; ++j) s = fma(JB[i + (int64_t)j * J.ldb], b2[j + c * r], s);
-    J.outB[i + (int64_t)c * J.ldob] = (double)s;
-  }
+  // (column, row) loops without a division per element; the same sums
+  for (int c = 0; c < k; ++c)
+    for (int i = threadIdx.x; i < J.m; i += blockDim.x) {
+      TS s = 0;
+      for (int j = 0; j < r; ++j) s = fma(JA[i + (int64_t)j * J.lda], b1[j + c * r], s);
+      J.outA[i + (int64_t)c * J.ldoa] = (double)s;
+    }
+  for (int c = 0; c < k; ++c)
+    for (int i = threadIdx.x; i < J.n; i += blockDim.x) {
+      TS s = 0;
+      for (int j = 0; j < r; ++j) s = fma(JB[i + (int64_t)j * J.ldb], b2[j + c * r], s);
+      J.outB[i + (int64_t)c * J.ldob] = (double)s;
+    }
   if (J.zero_fill && k < zlim) {
     zero_cols(J.outA, J.m, J.ldoa, k, zlim);
     zero_cols(J.outB, J.n, J.ldob, k, zlim);

@@ -296,9 +296,13 @@ int launch_aca_fp_one(const AcaFpJob& J, cudaStream_t st) {
   return HM_OK;
 }
 
+// JAC8: the H-LU's recompressions (8 lanes per Jacobi pair, parallel ordering);
+// construction and H + H keep the block-wide rounds
+template <bool JAC8>
 __global__ void __launch_bounds__(256) core_recompress_kernel(const CoreJob* __restrict__ jobs, int rmax,
                                                               double eps_trunc, int* __restrict__ flags) {
-  core_body(jobs[blockIdx.x], rmax, eps_trunc, flags);
+  const CoreJob& J = jobs[blockIdx.x];
+  core_body_t<double, JAC8>(J, J.A, J.B, rmax, eps_trunc, flags);
 }
 
 __global__ void __launch_bounds__(256) core_recompress_one_kernel(CoreJob J, int rmax, double eps_trunc,
@@ -315,14 +319,17 @@ int launch_core_one(const CoreJob& J, double eps_trunc, int* d_flags, cudaStream
 }
 
 int launch_core_recompress(const CoreJob* d_jobs, int njobs, int rmax, double eps_trunc, int* d_flags,
-                           cudaStream_t st) {
+                           cudaStream_t st, bool jac8) {
   if (njobs == 0) return HM_OK;
   if (rmax > RCORE_MAX) return fail(HM_ERR_UNSUPPORTED, "recompression core above " + std::to_string(RCORE_MAX));
   rmax = std::max(rmax, 1);
   size_t smem = (size_t)3 * rmax * rmax * sizeof(double);
-  HM_CUDA_TRY(smem_attr((const void*)core_recompress_kernel, (int)((size_t)3 * RCORE_MAX * RCORE_MAX * sizeof(double))));
+  const void* kfn = jac8 ? (const void*)core_recompress_kernel<true> : (const void*)core_recompress_kernel<false>;
+  HM_CUDA_TRY(smem_attr(kfn, (int)((size_t)3 * RCORE_MAX * RCORE_MAX * sizeof(double))));
   // small cores: 2 warps per job, so that many jobs share an SM
-  core_recompress_kernel<<<njobs, rmax <= 32 ? 64 : 256, smem, st>>>(d_jobs, rmax, eps_trunc, d_flags);
+  const int nt = rmax <= 32 ? 64 : 256;
+  if (jac8) core_recompress_kernel<true><<<njobs, nt, smem, st>>>(d_jobs, rmax, eps_trunc, d_flags);
+  else core_recompress_kernel<false><<<njobs, nt, smem, st>>>(d_jobs, rmax, eps_trunc, d_flags);
   HM_CUDA_TRY(cudaGetLastError());
   return HM_OK;
 }

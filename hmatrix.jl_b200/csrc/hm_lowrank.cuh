@@ -116,7 +116,8 @@ int launch_aca_fp(const AcaFpJob* d_jobs, int njobs, cudaStream_t st);   // one 
 int launch_core_one(const CoreJob& J, double eps_trunc, int* d_flags, cudaStream_t st);
 // launch the batched recompression; status of rank overflow/nonfinite is
 // OR-ed into *d_flags (bit 0: rank > kcap, bit 1: non-finite).
+// jac8: the Jacobi rounds and ordering of the H-LU's recompressions (core_body_t)
 int launch_core_recompress(const CoreJob* d_jobs, int njobs, int rmax, double eps_trunc,
-                           int* d_flags, cudaStream_t st);
+                           int* d_flags, cudaStream_t st, bool jac8 = false);
 
 }  // namespace hm

@@ -1289,7 +1289,7 @@ static void recompress_batch(Ctx& c, const std::vector<RcReq>& reqs, int rmax, b
         throw LuError(HM_ERR_CUDA, "core size read-back");
       rlaunch = std::min(rmax, std::max(8, (hmax + 7) / 8 * 8));
     }
-    int s = launch_core_recompress(dc, (int)(e - b), rlaunch, c.eps_trunc, c.flags, c.st);
+    int s = launch_core_recompress(dc, (int)(e - b), rlaunch, c.eps_trunc, c.flags, c.st, true);
     if (s != HM_OK) throw LuError(s, "batched recompression launch");
     b = e;
   }
@@ -1545,14 +1545,12 @@ __global__ void __launch_bounds__(128) lu_tile_core_kernel(TileJobArgs a, int rl
   }
   TS* XA = sm + 3 * rl * rl;
   TS* XB = XA + (int64_t)smax * rl;
-  for (int e = threadIdx.x; e < mi * r; e += blockDim.x) {
-    const int t = e % mi, q = e / mi;
-    XA[e] = (TS)(q < k1 ? Aij[t + (int64_t)q * mi] : -Qij[t + (int64_t)(q - k1) * mi]);
-  }
-  for (int e = threadIdx.x; e < nj * r; e += blockDim.x) {
-    const int t = e % nj, q = e / nj;
-    XB[e] = (TS)(q < k1 ? Bij[t + (int64_t)q * nj] : Bkj[t + (int64_t)(q - k1) * nj]);
-  }
+  for (int q = 0; q < r; ++q)
+    for (int t = threadIdx.x; t < mi; t += blockDim.x)
+      XA[t + q * mi] = (TS)(q < k1 ? Aij[t + (int64_t)q * mi] : -Qij[t + (int64_t)(q - k1) * mi]);
+  for (int q = 0; q < r; ++q)
+    for (int t = threadIdx.x; t < nj; t += blockDim.x)
+      XB[t + q * nj] = (TS)(q < k1 ? Bij[t + (int64_t)q * nj] : Bkj[t + (int64_t)(q - k1) * nj]);
   __syncthreads();
   CoreJob J{};
   J.outA = Aij; J.outB = Bij;
@@ -1565,7 +1563,7 @@ __global__ void __launch_bounds__(128) lu_tile_core_kernel(TileJobArgs a, int rl
   // from step 1 on, every trailing tile (and tile (k, j)) is a previous step's
   // core output: A_ij orthonormal, B_ij and B_kj with orthogonal columns
   J.ortho_k = a.k >= 1 ? k1 : 0;
-  core_body_t<TS>(J, XA, XB, rl, eps_trunc, a.flags);
+  core_body_t<TS, true>(J, XA, XB, rl, eps_trunc, a.flags);
 }
 
 // an upper bound of rank(A_ij) + rank(B_kj) over the trailing pairs of step k
@@ -1659,7 +1657,7 @@ static void recompress_tile_pairs(Ctx& c, const TileLU& TL, int k, int64_t R, co
         cudaStreamSynchronize(c.st) != cudaSuccess)
       throw LuError(HM_ERR_CUDA, "core size read-back");
     const int rlaunch = std::min(rmax, std::max(8, (hmax + 7) / 8 * 8));
-    int st = launch_core_recompress(cj, (int)nb, rlaunch, c.eps_trunc, c.flags, c.st);
+    int st = launch_core_recompress(cj, (int)nb, rlaunch, c.eps_trunc, c.flags, c.st, true);
     if (st != HM_OK) throw LuError(st, "batched recompression launch");
   }
 }
