@@ -488,6 +488,67 @@ def batched_problems(count, seed=3, nmin=2 ** 10, nmax=2 ** 16):
     return out
 
 
+def oracle_batch_sample(count, budget_s=15.0, nmax=8192):
+    """The oracle's FP64 lu! + \\ (src/hlu.jl:465-562, numpy BLAS on every host
+    thread) on a bounded sample of the batched problems: in problem order, those
+    of n <= nmax, until budget_s of CPU time is spent; per-problem times, no
+    refinement."""
+    import os
+    from oracle import hm_oracle as O
+    rows = []
+    spent = 0.0
+    for i, (x, ell, y) in enumerate(batched_problems(count)):
+        if len(x) > nmax:
+            continue
+        prm = O.Params(Geom=x, Kernel=O.kernel_cauchy(ell), MaxBlock=256, MinBlock=32, MaxRank=12,
+                       ConsMethod="aca2", εComp=1e-10, Tree="bisect")
+        _, H = O.NewHmat(prm)
+        H = O.add_identity(H, 1.0)
+        t0 = time.perf_counter()
+        L = O.lu(H, prm)
+        xs = O.solve(L, y)
+        dt = time.perf_counter() - t0
+        rr = float(np.linalg.norm(O.matvec(H, xs) - y) / np.linalg.norm(y))
+        rows.append({"problem": i, "n": len(x), "s": dt, "relres": rr})
+        spent += dt
+        if spent >= budget_s:
+            break
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except Exception:
+        cores = os.cpu_count() or 1
+    return rows, cores
+
+
+def batch_cpu_beside_gpu(count, torch):
+    """The CPU sample of oracle_batch_sample next to the GPU's FP64 lu(H) + H\\y of
+    the same problems, one at a time (no refinement on either side)."""
+    import hmatrix as hm
+    rows, cores = oracle_batch_sample(count)
+    probs = batched_problems(count)
+    gpu_total = 0.0
+    for r in rows:
+        x, ell, y = probs[r["problem"]]
+        prm = hm.Params(Geom=x, Kernel=hm.Cauchy(ell), MaxBlock=256, MinBlock=32, MaxRank=12,
+                        ConsMethod="aca2", εComp=1e-10, Tree="bisect", Shift=1.0,
+                        Device=torch.cuda.current_device())
+        _, H = hm.NewHmat(prm)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L = hm.lu(H)
+        xs = L.solve(y)
+        dt = time.perf_counter() - t0
+        r["gpu_s"] = dt
+        r["gpu_relres"] = float(np.linalg.norm(H * xs - y) / np.linalg.norm(y))
+        gpu_total += dt
+        del L, H
+    cpu_total = sum(r["s"] for r in rows)
+    return {"kind": "port", "cores": cores, "problems": rows, "cpu_total_s": cpu_total, "gpu_total_s": gpu_total,
+            "gpu_speedup": cpu_total / gpu_total if gpu_total > 0 else None,
+            "sample": "lu! + \\ of the FP64 oracle (numpy/BLAS) on the first %d batched problems of n <= 8192 "
+                      "(about 15 s of host time), beside the GPU's FP64 lu(H) + H\\y of the same problems" % len(rows)}
+
+
 def batch_leg(count, torch, nthreads=0, budget_gb=90.0, rank=0, world=1, dist=None):
     """All problems factored (lu!) and solved with FP64 refinement to a
     relative residual <= 1e-10 through the batched entry points, in waves
@@ -781,6 +842,12 @@ def run_ours(a):
         H = None
         torch.cuda.empty_cache()
         batch = batch_leg(a.batch, torch, a.batch_nthreads, rank=rank, world=world, dist=dist)
+        if not a.no_cpu and world == 1:
+            try:
+                batch["cpu_baseline"] = batch_cpu_beside_gpu(a.batch, torch)
+            except Exception as e:          # the CPU sample never costs the bench line
+                batch["cpu_baseline"] = {"error": repr(e)[:300]}
+            torch.cuda.empty_cache()
     c5 = None
     if a.c5 and world == 1:
         H = None
