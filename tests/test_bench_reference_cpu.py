@@ -43,3 +43,18 @@ def test_oracle_lu_sample_contract():
     d = bench.oracle_lu_sample(2048)
     assert d["n"] == 2048 and d["kind"] == "port" and d["cores"] >= 1
     assert d["lu_s"] > 0 and d["total_s"] >= d["lu_s"] and d["relres"] < 1e-8
+
+
+def test_oracle_batch_sample_contract():
+    # the CPU sample of the batched configuration set beside the GPU's
+    sys.path.insert(0, ROOT)
+    import bench
+    rows, cores = bench.oracle_batch_sample(256, budget_s=0.2, nmax=2048)
+    assert cores >= 1 and len(rows) >= 1
+    probs = bench.batched_problems(256)
+    for r in rows:
+        assert r["n"] == len(probs[r["problem"]][0]) <= 2048
+        assert r["s"] > 0 and r["relres"] < 1e-8
+    # problem order, and the budget ends the sample after the problem that crosses it
+    assert [r["problem"] for r in rows] == sorted(r["problem"] for r in rows)
+    assert sum(r["s"] for r in rows[:-1]) < 0.2
